@@ -1,0 +1,432 @@
+#!/usr/bin/env python
+"""Benchmark of Catmull-Clark halfedge refinement on B200.
+
+Workload (one "step"): ``ccs_Refine_Scatter`` of the mixed-crease torus cage
+(64x64 grid-torus with triangles, pentagons, a boundary strip, crease chains
+and UVs; H0 = 17,416 halfedges) to depth 6: topology, creases, UVs and FP32
+points of every level, 95.1M refined halfedges per step.
+
+Metric: refined halfedges per second (sum of H_d over depths 1..6 per step).
+
+* ``value``   device time of the refine call with its inputs resident in HBM,
+              CUDA events on the subd's stream, L2 flushed (256 MB write)
+              between timed steps, outside the events.
+* ``e2e``     the same call through the C ABI with host buffers: upload of
+              the cage points from pinned host memory, refine, download of
+              every level's halfedges, creases and points to the host.
+* ``roofline`` the kernel with the largest share of device time (per-launch
+              CUDA events inside the library), its algorithmic bytes per
+              launch over its mean duration, against MEASURED_PEAKS.json.
+* ``cpu_baseline`` the reference's own ccs_Refine_Scatter (compiled from its
+              sources into oracle/_ref, OpenMP on all host cores) on the same
+              cage and depth, a bounded sample of runs.
+
+``--impl reference`` times only the reference CPU path (rank 0).
+Multi-GPU (torchrun): every rank refines its own replica of the cage (the
+single-mesh path does not shard); value = all ranks' halfedges / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "refined halfedges/s"
+UNIT = "halfedges/s"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--depth", type=int, default=6)
+    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--e2e-steps", type=int, default=5)
+    p.add_argument("--deterministic", action="store_true")
+    return p.parse_args()
+
+
+def workload(depth):
+    from halfedgecatmullclark_b200 import configs
+    return configs.mixed_torus(depth=depth)
+
+
+def config_dict(w, extra=None):
+    c = {"workload": "mixed_torus_64x64_depth%d" % w.depth, "cage_halfedges": w.cage.H,
+         "cage_faces": w.cage.F, "depth": w.depth, "uv": w.cage.U > 0,
+         "crease_edges": w.notes.get("crease_edges"), "l2": "flushed (256 MB write) between timed steps"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid=None):
+        self.uuid = uuid
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.QUERY,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        rows = []
+        with open(self.path) as fh:
+            for line in fh:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 10:
+                    continue
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        if self.uuid:
+            mine = [r for r in rows if r[1].lower().endswith(self.uuid.lower()[-12:])]
+            rows = mine or rows
+        # keep the GPU that drew the most power (the one under load)
+        by_idx = {}
+        for r in rows:
+            by_idx.setdefault(r[0], []).append(r)
+
+        def pw(rs):
+            try:
+                return max(float(r[4]) for r in rs)
+            except ValueError:
+                return 0.0
+        rs = max(by_idx.values(), key=pw)
+        sm = [float(r[2]) for r in rs if r[2].replace(".", "").isdigit()]
+        smax = [float(r[3]) for r in rs if r[3].replace(".", "").isdigit()]
+        pmax = pw(rs)
+        load = [s for s, r in zip(sm, rs) if float(r[4] or 0) > 0.35 * pmax] or sm
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rs for k in range(4) if "Active" in r[6 + k] and "Not" not in r[6 + k]})
+        return {"sm_mhz": statistics.median(load) if load else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": reasons,
+                "samples": len(rs), "power_w_max": pmax}
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_table():
+    """dram bytes per launch from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as fh:
+            return json.load(fh)
+    except Exception:
+        return {}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference compiled from its sources (oracle/_ref)
+# ---------------------------------------------------------------------------
+def cpu_reference(w, seconds, max_runs=20, min_runs=2):
+    from oracle import refimpl
+    from halfedgecatmullclark_b200 import metrics
+    from halfedgecatmullclark_b200.subd import level_counts
+    sh = metrics.total_halfedges(level_counts(w.cage, w.depth))
+    cores = os.cpu_count() or 1
+    if refimpl.available():
+        refimpl.set_threads(cores)
+        s = refimpl.RefSubd(w.cage, w.depth)
+        times = []
+        t_end = time.perf_counter() + seconds
+        try:
+            while len(times) < max_runs and (len(times) < min_runs or time.perf_counter() < t_end):
+                t0 = time.perf_counter()
+                s.refine("scatter")
+                times.append(time.perf_counter() - t0)
+        finally:
+            s.close()
+        med = statistics.median(times)
+        return {"value": sh / med, "unit": UNIT, "cores": cores, "kind": "reference",
+                "sample": "%d runs of the reference ccs_Refine_Scatter on the full workload "
+                          "(OpenMP %d threads), median %.1f ms" % (len(times), cores, med * 1e3),
+                "ms_per_step": med * 1e3}
+    # the oracle port, single-threaded, on a smaller depth of the same cage
+    from oracle import oracle
+    d = max(1, w.depth - 2)
+    sh_d = metrics.total_halfedges(level_counts(w.cage, d))
+    times = []
+    t_end = time.perf_counter() + seconds
+    while len(times) < max_runs and (len(times) < min_runs or time.perf_counter() < t_end):
+        t0 = time.perf_counter()
+        oracle.refine(w.cage, d, "scatter")
+        times.append(time.perf_counter() - t0)
+    med = statistics.median(times)
+    return {"value": sh_d / med, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": "%d runs of the single-threaded oracle at depth %d of the same cage" % (len(times), d),
+            "ms_per_step": med * 1e3}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    w = workload(args.depth)
+    from oracle import refimpl
+    from halfedgecatmullclark_b200 import metrics
+    from halfedgecatmullclark_b200.subd import level_counts
+    sh = metrics.total_halfedges(level_counts(w.cage, w.depth))
+    cores = os.cpu_count() or 1
+    if not refimpl.available():
+        base = cpu_reference(w, args.cpu_seconds)
+        line = {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": UNIT,
+                "n_gpus": args.gpus, "steps": 0, "warmup": 0, "ms_per_step": base["ms_per_step"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic", "config": config_dict(w), "cpu_baseline": base,
+                "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+    refimpl.set_threads(cores)
+    s = refimpl.RefSubd(w.cage, w.depth)
+    try:
+        for _ in range(args.warmup):
+            s.refine("scatter")
+        times = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            s.refine("scatter")
+            times.append(time.perf_counter() - t0)
+    finally:
+        s.close()
+    total = sum(times)
+    value = sh * args.steps / total
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": config_dict(w),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                             "sample": "%d timed runs of the reference ccs_Refine_Scatter on the full "
+                                       "workload, OpenMP %d threads" % (args.steps, cores)},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def dist_init():
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return rank, world
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    from halfedgecatmullclark_b200 import _native as N
+    from halfedgecatmullclark_b200 import metrics
+    from halfedgecatmullclark_b200.subd import Subd
+
+    rank, world = dist_init()
+    w = workload(args.depth)
+    flags = N.FLAG_DETERMINISTIC if args.deterministic else 0
+    subd = Subd(w.cage, w.depth, flags)
+    stream = torch.cuda.Stream()
+    subd.set_stream(stream)
+    levels = subd.levels
+    SH = metrics.total_halfedges(levels)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    uuid = None
+    try:
+        uuid = str(torch.cuda.get_device_properties(torch.cuda.current_device()).uuid)
+    except Exception:
+        pass
+
+    with torch.cuda.stream(stream):
+        for _ in range(max(3, args.warmup)):
+            subd.refine_scatter()
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler(uuid)
+    sampler.start()
+    t_wall = time.perf_counter()
+    evs = []
+    with torch.cuda.stream(stream):
+        for _ in range(args.steps):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            subd.refine_scatter()
+            b.record(stream)
+            evs.append((a, b))
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t_wall
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    total_ms = max_over_ranks(sum(step_ms), world)
+
+    # per-kernel CUDA events (same workload, profiling launches one by one)
+    subd.set_profiling(True)
+    with torch.cuda.stream(stream):
+        for _ in range(args.steps):
+            flush.zero_()
+            subd.refine_scatter()
+    recs = subd.read_profile(1 << 16)
+    subd.set_profiling(False)
+    clocks = sampler.stop()
+
+    value = world * SH * args.steps / (total_ms / 1e3)
+    rec_bytes = 16 if subd.record_words == 4 else 12
+
+    # roofline of the dominant kernel
+    by = {}
+    for r in recs:
+        by.setdefault((r["kernel"], r["level"]), []).append(r["ms"])
+    total_prof = sum(sum(v) for v in by.values())
+    dom_key = max(by, key=lambda k: sum(by[k]))
+    dom_ms = statistics.mean(by[dom_key])
+    dom_bytes = metrics.kernel_bytes(dom_key[0], levels[dom_key[1]], rec_bytes)
+    peak, peak_kind = measured_peak()
+    achieved = dom_bytes / (dom_ms / 1e3) / 1e9
+    traffic = traffic_table().get("%s@%d" % dom_key)
+    kernels = sorted(({"kernel": k[0], "level": k[1], "mean_ms": statistics.mean(v),
+                       "share": sum(v) / total_prof,
+                       "gbs": metrics.kernel_bytes(k[0], levels[k[1]], rec_bytes) / (statistics.mean(v) / 1e3) / 1e9}
+                      for k, v in by.items()), key=lambda x: -x["share"])
+    per_depth = []
+    for d in range(w.depth):
+        ms = sum(statistics.mean(v) for k, v in by.items() if k[1] == d)
+        nb = metrics.level_bytes(levels[d], levels[d + 1], rec_bytes, subd.record_words == 4, d == 0, w.cage.U)
+        per_depth.append({"depth": d + 1, "ms": ms, "refined_halfedges": levels[d + 1]["H"],
+                          "halfedges_per_s": levels[d + 1]["H"] / (ms / 1e3), "alg_bytes": nb,
+                          "gbs": nb / (ms / 1e3) / 1e9, "frac_of_peak": nb / (ms / 1e3) / 1e9 / peak})
+
+    # end to end through the C ABI with host buffers
+    host_pts = torch.from_numpy(w.cage.vertex_points.copy()).pin_memory()
+    e2e_ms = []
+    torch.cuda.synchronize()
+    for _ in range(args.e2e_steps):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        subd.upload_cage_points(host_pts.numpy())
+        subd.refine_scatter()
+        subd.download()
+        b.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms.append(a.elapsed_time(b))
+    e2e_total = max_over_ranks(sum(e2e_ms), world)
+    h2d = 12 * w.cage.V
+    d2h = 4 * subd.record_words * subd.cumH + 12 * subd.cumC + 12 * subd.cumV
+    launches = len([r for r in recs if r["kernel"] != "clear"]) // max(1, args.steps)
+
+    base = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            base = cpu_reference(w, args.cpu_seconds)
+        except Exception as exc:  # a missing baseline must not hide the GPU number
+            base = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "unavailable",
+                    "sample": "error: %s" % exc}
+    subd.close()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config_dict(w, {"parallelism": "replicas x%d" % world,
+                                      "deterministic": bool(args.deterministic),
+                                      "refined_halfedges_per_step": SH}),
+            "e2e": {"value": world * SH * args.e2e_steps / (e2e_total / 1e3), "unit": UNIT,
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "ms_per_step": e2e_total / args.e2e_steps},
+            "gpu_launches": launches * args.steps,
+            "roofline": {"bound": "hbm", "kernel": "%s@depth%d" % (dom_key[0], dom_key[1]),
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": peak_kind, "alg_bytes_per_launch": dom_bytes,
+                         "launch_ms": dom_ms,
+                         "traffic": traffic},
+            "per_depth": per_depth,
+            "kernels": kernels[:12],
+            "clocks": clocks,
+            "wall_s": wall,
+        }
+        if base is not None:
+            line["cpu_baseline"] = base
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,620 @@
+// ccs_capi.cu -- the extern "C" boundary (include/ccs_cuda.h).
+//
+// A subd created here is the reference's cc_Subd (CatmullClark.h:136-142)
+// plus a device mirror kept in a side table keyed by the cc_Subd address, so
+// the public struct layout is unchanged.  The cage is validated on upload:
+// every index the kernels follow is checked once on the host, which makes
+// the refined levels in-range by construction (the refinement rules map
+// valid indices to valid indices), so no kernel can read out of bounds.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <new>
+#include <unordered_map>
+#include <vector>
+
+#include "ccs_host.h"
+
+namespace ccs {
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local int g_last = CCS_OK;
+static int ret(int s) {
+    g_last = s;
+    return s;
+}
+
+// ---------------------------------------------------------------------------
+// counts (CatmullClark.h:465-585, :815-936) with int32 overflow detection
+// ---------------------------------------------------------------------------
+static bool fits(long double x) { return x >= -2147483648.0L && x <= 2147483647.0L; }
+
+static int level_counts(const cc_Mesh* cage, int32_t D, std::vector<Level>* out) {
+    if (!cage || D < 1 || D > 15) return CCS_ERR_ARG;
+    const long double V0 = cage->vertexCount, F0 = cage->faceCount, E0 = cage->edgeCount, H0 = cage->halfedgeCount;
+    std::vector<Level> lv(D + 1);
+    long double cumH = 0, cumC = 0, cumV = 0;
+    for (int d = 0; d <= D; ++d) {
+        const long double p4 = powl(4.0L, d), p2 = powl(2.0L, d);
+        const long double H = H0 * p4;
+        const long double F = d == 0 ? F0 : H0 * powl(4.0L, d - 1);
+        const long double E = d == 0 ? E0 : powl(2.0L, d - 1) * (2 * E0 + (p2 - 1) * H0);
+        const long double t = d == 0 ? 0 : powl(2.0L, d - 1) - 1;
+        const long double V = d == 0 ? V0 : (V0 + E0 + F0) + t * ((2 * E0 + H0) + t * H0);
+        const long double C = E0 * p2;
+        // the reference's cumulative formulas multiply before dividing
+        const long double H1xA = 4 * H0 * (p4 - 1);
+        const long double Ae = p2 - 1, E1 = 2 * E0 + H0, H1 = 4 * H0;
+        const long double cumEraw = Ae * (6 * E1 + Ae * H1 - H1);
+        if (!fits(H) || !fits(F) || !fits(E) || !fits(V) || !fits(C) || !fits(H1xA) || !fits(cumEraw) ||
+            !fits(2 * E + H) || !fits(V + F + E))
+            return CCS_ERR_OVERFLOW;
+        lv[d].d = d;
+        lv[d].H = (int32_t)H; lv[d].F = (int32_t)F; lv[d].E = (int32_t)E;
+        lv[d].V = (int32_t)V; lv[d].C = (int32_t)C;
+        // depth-d arrays start after depths 1..d-1
+        lv[d].heOff = d == 0 ? 0 : (int64_t)cumH;
+        lv[d].crOff = d == 0 ? 0 : (int64_t)cumC;
+        lv[d].ptOff = d == 0 ? 0 : (int64_t)cumV;
+        if (d >= 1) {
+            cumH += H; cumC += C; cumV += V;
+            if (!fits(cumH) || !fits(cumC) || !fits(cumV)) return CCS_ERR_OVERFLOW;
+        }
+    }
+    *out = lv;
+    return CCS_OK;
+}
+
+static int64_t cum_of(const std::vector<Level>& lv, char what) {
+    const Level& last = lv.back();
+    switch (what) {
+        case 'H': return last.heOff + last.H;
+        case 'C': return last.crOff + last.C;
+        default: return last.ptOff + last.V;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// cage validation: every index a kernel follows must be in range
+// ---------------------------------------------------------------------------
+static int validate_cage(const cc_Mesh* m) {
+    if (!m) return CCS_ERR_ARG;
+    const int32_t V = m->vertexCount, U = m->uvCount, H = m->halfedgeCount, E = m->edgeCount, F = m->faceCount;
+    if (V <= 0 || H <= 0 || E <= 0 || F <= 0 || U < 0) return CCS_ERR_ARG;
+    if (!m->halfedges || !m->creases || !m->vertexPoints || !m->vertexToHalfedgeIDs ||
+        !m->edgeToHalfedgeIDs || !m->faceToHalfedgeIDs || (U > 0 && !m->uvs))
+        return CCS_ERR_ARG;
+    const cc_Halfedge* he = m->halfedges;
+    for (int32_t h = 0; h < H; ++h) {
+        const cc_Halfedge& r = he[h];
+        if (r.twinID < -1 || r.twinID >= H) return CCS_ERR_ARG;
+        if (r.nextID < 0 || r.nextID >= H || r.prevID < 0 || r.prevID >= H) return CCS_ERR_ARG;
+        if (r.faceID < 0 || r.faceID >= F || r.edgeID < 0 || r.edgeID >= E) return CCS_ERR_ARG;
+        if (r.vertexID < 0 || r.vertexID >= V) return CCS_ERR_ARG;
+        if (U > 0 && (r.uvID < 0 || r.uvID >= U)) return CCS_ERR_ARG;
+    }
+    for (int32_t h = 0; h < H; ++h) {
+        const cc_Halfedge& r = he[h];
+        if (he[r.nextID].prevID != h || he[r.prevID].nextID != h) return CCS_ERR_ARG;
+        if (r.twinID >= 0 && (he[r.twinID].twinID != h || he[r.twinID].edgeID != r.edgeID)) return CCS_ERR_ARG;
+        if (he[r.nextID].faceID != r.faceID) return CCS_ERR_ARG;
+    }
+    for (int32_t e = 0; e < E; ++e) {
+        const cc_Crease& c = m->creases[e];
+        if (c.nextID < 0 || c.nextID >= E || c.prevID < 0 || c.prevID >= E) return CCS_ERR_ARG;
+        const int32_t h = m->edgeToHalfedgeIDs[e];
+        if (h < 0 || h >= H) return CCS_ERR_ARG;
+    }
+    for (int32_t v = 0; v < V; ++v) {
+        const int32_t h = m->vertexToHalfedgeIDs[v];
+        if (h < 0 || h >= H) return CCS_ERR_ARG;
+    }
+    for (int32_t f = 0; f < F; ++f) {
+        const int32_t h = m->faceToHalfedgeIDs[f];
+        if (h < 0 || h >= H || he[h].faceID != f) return CCS_ERR_ARG;
+    }
+    return CCS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// profiling
+// ---------------------------------------------------------------------------
+void Profiler::begin(cudaStream_t s, int kernel, int level, int64_t units) {
+    if (!on) return;
+    TimedLaunch t{kernel, level, units, nullptr, nullptr};
+    cudaEventCreate(&t.a);
+    cudaEventCreate(&t.b);
+    cudaEventRecord(t.a, s);
+    pending.push_back(t);
+}
+void Profiler::end(cudaStream_t s) {
+    if (!on || pending.empty()) return;
+    cudaEventRecord(pending.back().b, s);
+}
+
+// ---------------------------------------------------------------------------
+// the device mirror of one subd
+// ---------------------------------------------------------------------------
+struct SubdImpl {
+    cc_Subd* host = nullptr;
+    const cc_Mesh* cage = nullptr;
+    int device = 0;
+    int32_t D = 0, rw = 4;
+    uint32_t flags = 0;
+    std::vector<Level> lv;
+    int64_t cumH = 0, cumC = 0, cumV = 0;
+    DevCage dc;
+    int32_t* he = nullptr;
+    cc_Crease* cr = nullptr;
+    float* pts = nullptr;
+    float* work = nullptr;         // adjoint scratch (cumV x 3)
+    int* err = nullptr;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    bool pinned = true;
+    bool topo_ready = false, creases_ready = false;
+    Profiler prof;
+    std::map<int, cudaGraphExec_t> graphs;
+
+    Ctx ctx(cudaStream_t s) {
+        Ctx c;
+        c.cage = &dc; c.rw = rw; c.D = D; c.lv = lv.data(); c.he = he; c.cr = cr;
+        c.stream = s; c.prof = &prof; c.err = err;
+        return c;
+    }
+};
+
+static std::mutex g_mu;
+static std::unordered_map<const cc_Subd*, SubdImpl*> g_reg;
+
+static SubdImpl* find(const cc_Subd* s) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    auto it = g_reg.find(s);
+    return it == g_reg.end() ? nullptr : it->second;
+}
+
+// RAII: make the subd's device current, restore the caller's afterwards.
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+static void free_impl(SubdImpl* s) {
+    if (!s) return;
+    for (auto& kv : s->graphs) cudaGraphExecDestroy(kv.second);
+    s->graphs.clear();
+    for (auto& t : s->prof.pending) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
+    cudaFree(s->dc.he); cudaFree(s->dc.cr); cudaFree(s->dc.pts); cudaFree(s->dc.uvs);
+    cudaFree(s->dc.v2h); cudaFree(s->dc.e2h); cudaFree(s->dc.f2h);
+    cudaFree(s->he); cudaFree(s->cr); cudaFree(s->pts); cudaFree(s->work); cudaFree(s->err);
+    if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+    if (s->host) {
+        if (s->pinned) {
+            cudaFreeHost(s->host->halfedges); cudaFreeHost(s->host->creases); cudaFreeHost(s->host->vertexPoints);
+        } else {
+            free(s->host->halfedges); free(s->host->creases); free(s->host->vertexPoints);
+        }
+        free(s->host);
+    }
+    delete s;
+}
+
+template <class T>
+static cudaError_t dmalloc(T** p, size_t bytes) {
+    return cudaMalloc((void**)p, bytes ? bytes : 16);
+}
+
+static int upload_cage(SubdImpl* s, const cc_Mesh* m) {
+    DevCage& d = s->dc;
+    d.V = m->vertexCount; d.U = m->uvCount; d.H = m->halfedgeCount; d.E = m->edgeCount; d.F = m->faceCount;
+    if (dmalloc(&d.he, sizeof(cc_Halfedge) * (size_t)d.H) || dmalloc(&d.cr, sizeof(cc_Crease) * (size_t)d.E) ||
+        dmalloc(&d.pts, sizeof(float) * 3 * (size_t)d.V) || dmalloc(&d.uvs, sizeof(float) * 2 * (size_t)d.U) ||
+        dmalloc(&d.v2h, sizeof(int32_t) * (size_t)d.V) || dmalloc(&d.e2h, sizeof(int32_t) * (size_t)d.E) ||
+        dmalloc(&d.f2h, sizeof(int32_t) * (size_t)d.F))
+        return CCS_ERR_ALLOC;
+    cudaStream_t st = s->stream;
+    if (cudaMemcpyAsync(d.he, m->halfedges, sizeof(cc_Halfedge) * (size_t)d.H, cudaMemcpyHostToDevice, st) ||
+        cudaMemcpyAsync(d.cr, m->creases, sizeof(cc_Crease) * (size_t)d.E, cudaMemcpyHostToDevice, st) ||
+        cudaMemcpyAsync(d.pts, m->vertexPoints, sizeof(float) * 3 * (size_t)d.V, cudaMemcpyHostToDevice, st) ||
+        (d.U > 0 && cudaMemcpyAsync(d.uvs, m->uvs, sizeof(float) * 2 * (size_t)d.U, cudaMemcpyHostToDevice, st)) ||
+        cudaMemcpyAsync(d.v2h, m->vertexToHalfedgeIDs, sizeof(int32_t) * (size_t)d.V, cudaMemcpyHostToDevice, st) ||
+        cudaMemcpyAsync(d.e2h, m->edgeToHalfedgeIDs, sizeof(int32_t) * (size_t)d.E, cudaMemcpyHostToDevice, st) ||
+        cudaMemcpyAsync(d.f2h, m->faceToHalfedgeIDs, sizeof(int32_t) * (size_t)d.F, cudaMemcpyHostToDevice, st))
+        return CCS_ERR_CUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return CCS_ERR_CUDA;
+    return CCS_OK;
+}
+
+static int create(const cc_Mesh* cage, int32_t D, uint32_t flags, cc_Subd** out) {
+    if (!out) return CCS_ERR_ARG;
+    *out = nullptr;
+    int st = validate_cage(cage);
+    if (st != CCS_OK) return st;
+    std::vector<Level> lv;
+    st = level_counts(cage, D, &lv);
+    if (st != CCS_OK) return st;
+    SubdImpl* s = new (std::nothrow) SubdImpl();
+    if (!s) return CCS_ERR_ALLOC;
+    s->cage = cage;
+    s->D = D;
+    s->flags = flags;
+    s->rw = (flags & CCS_FLAG_NO_UV) ? 3 : 4;
+    s->lv = lv;
+    s->cumH = cum_of(lv, 'H');
+    s->cumC = cum_of(lv, 'C');
+    s->cumV = cum_of(lv, 'V');
+    s->pinned = !(flags & CCS_FLAG_PAGEABLE_HOST);
+    if (cudaGetDevice(&s->device) != cudaSuccess) { delete s; return CCS_ERR_CUDA; }
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) { delete s; return CCS_ERR_CUDA; }
+    s->own_stream = true;
+
+    const size_t heBytes = sizeof(int32_t) * (size_t)s->rw * (size_t)s->cumH;
+    const size_t crBytes = sizeof(cc_Crease) * (size_t)s->cumC;
+    const size_t ptBytes = sizeof(float) * 3 * (size_t)s->cumV;
+    s->host = (cc_Subd*)calloc(1, sizeof(cc_Subd));
+    if (!s->host) { free_impl(s); return CCS_ERR_ALLOC; }
+    s->host->cage = cage;
+    s->host->maxDepth = D;
+    void *hh = nullptr, *hc = nullptr, *hp = nullptr;
+    if (s->pinned) {
+        if (cudaMallocHost(&hh, heBytes) || cudaMallocHost(&hc, crBytes ? crBytes : 16) ||
+            cudaMallocHost(&hp, ptBytes)) {
+            s->host->halfedges = (cc_Halfedge_SemiRegular*)hh; s->host->creases = (cc_Crease*)hc;
+            s->host->vertexPoints = (cc_VertexPoint*)hp;
+            free_impl(s);
+            return CCS_ERR_ALLOC;
+        }
+    } else {
+        hh = malloc(heBytes); hc = malloc(crBytes ? crBytes : 16); hp = malloc(ptBytes);
+    }
+    s->host->halfedges = (cc_Halfedge_SemiRegular*)hh;
+    s->host->creases = (cc_Crease*)hc;
+    s->host->vertexPoints = (cc_VertexPoint*)hp;
+    if (!hh || !hc || !hp) { free_impl(s); return CCS_ERR_ALLOC; }
+    if (dmalloc(&s->he, heBytes) || dmalloc(&s->cr, crBytes) || dmalloc(&s->pts, ptBytes) ||
+        dmalloc(&s->err, sizeof(int))) {
+        free_impl(s);
+        return CCS_ERR_ALLOC;
+    }
+    st = upload_cage(s, cage);
+    if (st != CCS_OK) { free_impl(s); return st; }
+    {
+        std::lock_guard<std::mutex> lock(g_mu);
+        g_reg[s->host] = s;
+    }
+    *out = s->host;
+    return CCS_OK;
+}
+
+// Operation identifiers (graph cache keys).
+enum Op {
+    OP_HALFEDGES = 1, OP_CREASES, OP_UVS,
+    OP_POINTS_BASE = 16,        // + mode * 2 + det
+    OP_REFINE_BASE = 64,        // + mode * 2 + det
+};
+
+// Enqueue the launches of one operation on `st`.
+static cudaError_t enqueue(SubdImpl* s, int op, cudaStream_t st) {
+    Ctx c = s->ctx(st);
+    const bool det = (s->flags & CCS_FLAG_DETERMINISTIC) != 0;
+    (void)det;
+    const bool uv = s->dc.U > 0 && s->rw == 4;
+    cudaError_t e = cudaSuccess;
+    if (op == OP_HALFEDGES) return run_topology(c, true, false);
+    if (op == OP_CREASES) return run_creases(c);
+    if (op == OP_UVS) return uv ? run_topology(c, false, true) : cudaSuccess;
+    if (op >= OP_REFINE_BASE) {
+        const int k = op - OP_REFINE_BASE;
+        e = run_topology(c, true, uv);
+        if (e == cudaSuccess) e = run_creases(c);
+        if (e == cudaSuccess) e = run_points(c, s->dc.pts, s->pts, k >> 1, (k & 1) != 0);
+        return e;
+    }
+    if (op >= OP_POINTS_BASE) {
+        const int k = op - OP_POINTS_BASE;
+        return run_points(c, s->dc.pts, s->pts, k >> 1, (k & 1) != 0);
+    }
+    return cudaErrorInvalidValue;
+}
+
+// Run an operation: replay its CUDA graph when allowed, else launch directly.
+static int execute(SubdImpl* s, int op) {
+    DeviceGuard g(s->device);
+    cudaStream_t st = s->stream;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (st) cudaStreamIsCapturing(st, &cap);
+    const bool use_graph = st && !s->prof.on && !(s->flags & CCS_FLAG_NO_GRAPH) &&
+                           cap == cudaStreamCaptureStatusNone;
+    if (!use_graph) {
+        cudaError_t e = enqueue(s, op, st);
+        return e == cudaSuccess ? CCS_OK : CCS_ERR_CUDA;
+    }
+    auto it = s->graphs.find(op);
+    if (it == s->graphs.end()) {
+        cudaGraph_t graph = nullptr;
+        if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return CCS_ERR_CUDA;
+        cudaError_t e = enqueue(s, op, st);
+        cudaError_t e2 = cudaStreamEndCapture(st, &graph);
+        if (e != cudaSuccess || e2 != cudaSuccess || !graph) {
+            if (graph) cudaGraphDestroy(graph);
+            cudaGetLastError();
+            return CCS_ERR_CUDA;
+        }
+        cudaGraphExec_t exec = nullptr;
+        e = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) return CCS_ERR_CUDA;
+        it = s->graphs.emplace(op, exec).first;
+    }
+    return cudaGraphLaunch(it->second, st) == cudaSuccess ? CCS_OK : CCS_ERR_CUDA;
+}
+
+static int refine_points_op(cc_Subd* subd, int mode) {
+    SubdImpl* s = find(subd);
+    if (!s) return ret(CCS_ERR_ARG);
+    if (!s->topo_ready || !s->creases_ready) return ret(CCS_ERR_STATE);
+    const int det = (s->flags & CCS_FLAG_DETERMINISTIC) ? 1 : 0;
+    return ret(execute(s, OP_POINTS_BASE + mode * 2 + det));
+}
+
+static int refine_op(cc_Subd* subd, int mode) {
+    SubdImpl* s = find(subd);
+    if (!s) return ret(CCS_ERR_ARG);
+    const int det = (s->flags & CCS_FLAG_DETERMINISTIC) ? 1 : 0;
+    const int st = execute(s, OP_REFINE_BASE + mode * 2 + det);
+    if (st == CCS_OK) s->topo_ready = s->creases_ready = true;
+    return ret(st);
+}
+
+}  // namespace ccs
+
+using namespace ccs;
+
+extern "C" {
+
+cc_Subd* ccs_Create_cuda(const cc_Mesh* cage, int32_t maxDepth) {
+    cc_Subd* out = nullptr;
+    ret(create(cage, maxDepth, 0u, &out));
+    return out;
+}
+
+int ccs_CreateEx_cuda(const cc_Mesh* cage, int32_t maxDepth, uint32_t flags, cc_Subd** out) {
+    return ret(create(cage, maxDepth, flags, out));
+}
+
+void ccs_Release_cuda(cc_Subd* subd) {
+    if (!subd) return;
+    SubdImpl* s = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_mu);
+        auto it = g_reg.find(subd);
+        if (it == g_reg.end()) { g_last = CCS_ERR_ARG; return; }
+        s = it->second;
+        g_reg.erase(it);
+    }
+    DeviceGuard g(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    free_impl(s);
+    g_last = CCS_OK;
+}
+
+int ccs_Refine_Scatter_cuda(cc_Subd* subd) { return refine_op(subd, CCS_POINTS_SCATTER); }
+int ccs_Refine_Gather_cuda(cc_Subd* subd) { return refine_op(subd, CCS_POINTS_GATHER); }
+int ccs_Refine_NoCreases_Scatter_cuda(cc_Subd* subd) { return refine_op(subd, CCS_POINTS_NOCREASES_SCATTER); }
+int ccs_Refine_NoCreases_Gather_cuda(cc_Subd* subd) { return refine_op(subd, CCS_POINTS_NOCREASES_GATHER); }
+int ccs_RefineVertexPoints_Scatter_cuda(cc_Subd* subd) { return refine_points_op(subd, CCS_POINTS_SCATTER); }
+int ccs_RefineVertexPoints_Gather_cuda(cc_Subd* subd) { return refine_points_op(subd, CCS_POINTS_GATHER); }
+int ccs_RefineVertexPoints_NoCreases_Scatter_cuda(cc_Subd* subd) {
+    return refine_points_op(subd, CCS_POINTS_NOCREASES_SCATTER);
+}
+int ccs_RefineVertexPoints_NoCreases_Gather_cuda(cc_Subd* subd) {
+    return refine_points_op(subd, CCS_POINTS_NOCREASES_GATHER);
+}
+
+int ccs_RefineHalfedges_cuda(cc_Subd* subd) {
+    SubdImpl* s = find(subd);
+    if (!s) return ret(CCS_ERR_ARG);
+    const int st = execute(s, OP_HALFEDGES);
+    if (st == CCS_OK) s->topo_ready = true;
+    return ret(st);
+}
+
+int ccs_RefineCreases_cuda(cc_Subd* subd) {
+    SubdImpl* s = find(subd);
+    if (!s) return ret(CCS_ERR_ARG);
+    const int st = execute(s, OP_CREASES);
+    if (st == CCS_OK) s->creases_ready = true;
+    return ret(st);
+}
+
+int ccs_RefineVertexUvs_cuda(cc_Subd* subd) {
+    SubdImpl* s = find(subd);
+    if (!s) return ret(CCS_ERR_ARG);
+    if (s->dc.U <= 0) return ret(CCS_OK);        // CatmullClark.h:2930
+    if (s->rw != 4) return ret(CCS_ERR_UNSUPPORTED);
+    return ret(execute(s, OP_UVS));
+}
+
+int ccs_Download_cuda(cc_Subd* subd) {
+    SubdImpl* s = find(subd);
+    if (!s) return ret(CCS_ERR_ARG);
+    DeviceGuard g(s->device);
+    cudaStream_t st = s->stream;
+    const size_t heBytes = sizeof(int32_t) * (size_t)s->rw * (size_t)s->cumH;
+    if (cudaMemcpyAsync(subd->halfedges, s->he, heBytes, cudaMemcpyDeviceToHost, st) ||
+        cudaMemcpyAsync(subd->creases, s->cr, sizeof(cc_Crease) * (size_t)s->cumC, cudaMemcpyDeviceToHost, st) ||
+        cudaMemcpyAsync(subd->vertexPoints, s->pts, sizeof(float) * 3 * (size_t)s->cumV, cudaMemcpyDeviceToHost, st))
+        return ret(CCS_ERR_CUDA);
+    return ret(cudaStreamSynchronize(st) == cudaSuccess ? CCS_OK : CCS_ERR_CUDA);
+}
+
+int ccs_UploadCagePoints_cuda(cc_Subd* subd, const cc_VertexPoint* points) {
+    SubdImpl* s = find(subd);
+    if (!s) return ret(CCS_ERR_ARG);
+    const cc_VertexPoint* src = points ? points : s->cage->vertexPoints;
+    if (!src) return ret(CCS_ERR_ARG);
+    DeviceGuard g(s->device);
+    return ret(cudaMemcpyAsync(s->dc.pts, src, sizeof(float) * 3 * (size_t)s->dc.V, cudaMemcpyHostToDevice,
+                               s->stream) == cudaSuccess ? CCS_OK : CCS_ERR_CUDA);
+}
+
+int ccs_SetStream_cuda(cc_Subd* subd, void* stream) {
+    SubdImpl* s = find(subd);
+    if (!s) return ret(CCS_ERR_ARG);
+    DeviceGuard g(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+    s->stream = (cudaStream_t)stream;
+    s->own_stream = false;
+    return ret(CCS_OK);
+}
+
+void* ccs_GetStream_cuda(const cc_Subd* subd) {
+    SubdImpl* s = find(subd);
+    return s ? (void*)s->stream : nullptr;
+}
+
+int ccs_Synchronize_cuda(cc_Subd* subd) {
+    SubdImpl* s = find(subd);
+    if (!s) return ret(CCS_ERR_ARG);
+    DeviceGuard g(s->device);
+    return ret(cudaStreamSynchronize(s->stream) == cudaSuccess ? CCS_OK : CCS_ERR_CUDA);
+}
+
+int ccs_SetFlags_cuda(cc_Subd* subd, uint32_t flags) {
+    SubdImpl* s = find(subd);
+    if (!s) return ret(CCS_ERR_ARG);
+    const uint32_t fixed = CCS_FLAG_NO_UV | CCS_FLAG_PAGEABLE_HOST;
+    if ((flags & fixed) != (s->flags & fixed)) return ret(CCS_ERR_UNSUPPORTED);
+    s->flags = flags;
+    return ret(CCS_OK);
+}
+
+uint32_t ccs_GetFlags_cuda(const cc_Subd* subd) {
+    SubdImpl* s = find(subd);
+    return s ? s->flags : 0u;
+}
+
+int ccs_GetDeviceArrays_cuda(const cc_Subd* subd, ccs_DeviceArrays* out) {
+    SubdImpl* s = find(subd);
+    if (!s || !out) return ret(CCS_ERR_ARG);
+    out->halfedges = s->he;
+    out->creases = s->cr;
+    out->vertexPoints = s->pts;
+    out->cagePoints = s->dc.pts;
+    out->halfedgeCount = s->cumH;
+    out->creaseCount = s->cumC;
+    out->vertexCount = s->cumV;
+    out->recordBytes = 4 * s->rw;
+    return ret(CCS_OK);
+}
+
+int ccs_RefinePointsDevice_cuda(cc_Subd* subd, const float* cagePoints, float* points, int mode, void* stream) {
+    SubdImpl* s = find(subd);
+    if (!s || !cagePoints || !points || mode < 0 || mode > 3) return ret(CCS_ERR_ARG);
+    if (!s->topo_ready || !s->creases_ready) return ret(CCS_ERR_STATE);
+    DeviceGuard g(s->device);
+    Ctx c = s->ctx((cudaStream_t)stream);
+    const bool det = (s->flags & CCS_FLAG_DETERMINISTIC) != 0;
+    return ret(run_points(c, cagePoints, points, mode, det) == cudaSuccess ? CCS_OK : CCS_ERR_CUDA);
+}
+
+int ccs_AdjointPointsDevice_cuda(cc_Subd* subd, const float* gradPoints, float* gradCage, void* stream) {
+    SubdImpl* s = find(subd);
+    if (!s || !gradPoints || !gradCage) return ret(CCS_ERR_ARG);
+    if (!s->topo_ready || !s->creases_ready) return ret(CCS_ERR_STATE);
+    DeviceGuard g(s->device);
+    if (!s->work && dmalloc(&s->work, sizeof(float) * 3 * (size_t)s->cumV)) return ret(CCS_ERR_ALLOC);
+    Ctx c = s->ctx((cudaStream_t)stream);
+    return ret(run_adjoint(c, gradPoints, s->work, gradCage, s->cumV) == cudaSuccess ? CCS_OK : CCS_ERR_CUDA);
+}
+
+int ccs_LevelCounts_cuda(const cc_Mesh* cage, int32_t maxDepth, ccs_LevelCounts* out) {
+    if (!cage || !out) return ret(CCS_ERR_ARG);
+    std::vector<Level> lv;
+    const int st = level_counts(cage, maxDepth, &lv);
+    if (st != CCS_OK) return ret(st);
+    for (int d = 0; d <= maxDepth; ++d) {
+        out[d].H = lv[d].H; out[d].F = lv[d].F; out[d].E = lv[d].E; out[d].V = lv[d].V; out[d].C = lv[d].C;
+        out[d].cumH = lv[d].heOff; out[d].cumC = lv[d].crOff; out[d].cumV = lv[d].ptOff;
+    }
+    return ret(CCS_OK);
+}
+
+int32_t ccs_MaxSupportedDepth_cuda(const cc_Mesh* cage) {
+    std::vector<Level> lv;
+    int32_t best = 0;
+    for (int32_t d = 1; d <= 15; ++d) {
+        if (level_counts(cage, d, &lv) != CCS_OK) break;
+        best = d;
+    }
+    return best;
+}
+
+int ccs_SetProfiling_cuda(cc_Subd* subd, int enable) {
+    SubdImpl* s = find(subd);
+    if (!s) return ret(CCS_ERR_ARG);
+    s->prof.on = enable != 0;
+    return ret(CCS_OK);
+}
+
+int ccs_ReadProfile_cuda(cc_Subd* subd, ccs_KernelTime* out, int cap) {
+    SubdImpl* s = find(subd);
+    if (!s || (cap > 0 && !out)) return ret(CCS_ERR_ARG);
+    DeviceGuard g(s->device);
+    if (cudaStreamSynchronize(s->stream) != cudaSuccess) return ret(CCS_ERR_CUDA);
+    int n = 0;
+    for (auto& t : s->prof.pending) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, t.a, t.b);
+        if (n < cap) {
+            out[n].kernel = t.kernel;
+            out[n].level = t.level;
+            out[n].ms = ms;
+            out[n].units = t.units;
+        }
+        ++n;
+        cudaEventDestroy(t.a);
+        cudaEventDestroy(t.b);
+    }
+    s->prof.pending.clear();
+    g_last = CCS_OK;
+    return n < cap ? n : cap;
+}
+
+const char* ccs_KernelName_cuda(int kernel) {
+    static const char* names[] = {"topology", "creases", "face_points", "edge_points", "vertex_points",
+                                  "clear", "level_fused", "adjoint", "uvs"};
+    return (kernel >= 0 && kernel < CCS_K_COUNT) ? names[kernel] : "unknown";
+}
+
+int ccs_LastError_cuda(void) { return g_last; }
+
+const char* ccs_ErrorString_cuda(int status) {
+    switch (status) {
+        case CCS_OK: return "ok";
+        case CCS_ERR_ARG: return "invalid argument or cage";
+        case CCS_ERR_ALLOC: return "allocation failed";
+        case CCS_ERR_OVERFLOW: return "depth overflows the int32 counts of the cc_Subd layout";
+        case CCS_ERR_CUDA: return "CUDA error";
+        case CCS_ERR_TIMEOUT: return "bounded device wait timed out";
+        case CCS_ERR_STATE: return "topology not refined yet";
+        case CCS_ERR_UNSUPPORTED: return "unsupported for this subd layout";
+        default: return "unknown status";
+    }
+}
+
+const char* ccs_Version_cuda(void) { return "ccs_cuda 0.1 (sm_100a)"; }
+
+}  // extern "C"

@@ -1,0 +1,71 @@
+// ccs_host.h -- host-side structures shared by the CUDA translation units.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+#include <cuda_runtime.h>
+
+#include "ccs_cuda.h"
+
+namespace ccs {
+
+struct CageCountsH {
+    int32_t V, F, E, H;
+};
+
+// Device copy of a cage (cc_Mesh arrays, same layouts).
+struct DevCage {
+    int32_t* he = nullptr;      // H x 7 words
+    cc_Crease* cr = nullptr;    // E
+    float* pts = nullptr;       // V x 3
+    float* uvs = nullptr;       // U x 2
+    int32_t* v2h = nullptr;
+    int32_t* e2h = nullptr;
+    int32_t* f2h = nullptr;
+    int32_t V = 0, U = 0, H = 0, E = 0, F = 0;
+};
+
+// Counts of one depth and the offsets of its arrays in the packed hierarchy.
+struct Level {
+    int32_t d;
+    int32_t V, F, E, H, C;        // counts at depth d
+    int64_t heOff, crOff, ptOff;  // offset of depth-d records (d >= 1)
+};
+
+// One timed launch (profiling mode).
+struct TimedLaunch {
+    int kernel, level;
+    int64_t units;
+    cudaEvent_t a, b;
+};
+
+struct Profiler {
+    bool on = false;
+    std::vector<TimedLaunch> pending;
+    void begin(cudaStream_t s, int kernel, int level, int64_t units);
+    void end(cudaStream_t s);
+};
+
+// Launch context: everything a refine pass needs.
+struct Ctx {
+    const DevCage* cage;
+    int32_t rw;                  // 4 or 3 words per refined halfedge record
+    int32_t D;
+    const Level* lv;             // D + 1 entries
+    int32_t* he;                 // refined halfedges (cumH records)
+    cc_Crease* cr;               // refined creases
+    cudaStream_t stream;
+    Profiler* prof;
+    int* err;                    // device error word
+};
+
+// Forward passes (ccs_forward.cu).  All return cudaError_t of the launches.
+cudaError_t run_topology(const Ctx& c, bool topo, bool uv);
+cudaError_t run_creases(const Ctx& c);
+// mode: CCS_POINTS_*; deterministic selects the fixed-order scatter sum.
+cudaError_t run_points(const Ctx& c, const float* cagePts, float* pts, int mode, bool deterministic);
+
+// Adjoint (ccs_adjoint.cu).  `work` holds cumV x 3 floats.
+cudaError_t run_adjoint(const Ctx& c, const float* gradPts, float* work, float* gradCage, int64_t cumV);
+
+}  // namespace ccs

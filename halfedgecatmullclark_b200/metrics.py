@@ -1,0 +1,51 @@
+"""Algorithmic byte counts of the refinement kernels (the roofline numerators).
+
+Every figure counts each unique input read once and each output written
+once, in the packed layout (16-byte halfedge records, or 12 with
+CCS_FLAG_NO_UV; 12-byte creases; 12-byte points).  ``level_bytes`` is the
+minimum for a whole refinement step d -> d+1 when the point passes read the
+halfedges once more (the per-depth GB/s figure); ``kernel_bytes`` is the
+per-launch figure of one kernel, which defines its achieved bandwidth.
+"""
+from __future__ import annotations
+
+
+def level_bytes(lv: dict, nxt: dict, rec: int = 16, uv: bool = True, cage: bool = False,
+                cage_uvs: int = 0) -> int:
+    """Minimum HBM bytes of one full refinement step (topology, creases, points)."""
+    H, V, C = lv["H"], lv["V"], lv["C"]
+    Vn = nxt["V"]
+    if cage:
+        topo = 28 * H + 4 * rec * H + 8 * cage_uvs
+    else:
+        topo = rec * H + 4 * rec * H
+    creases = 12 * C + 24 * C
+    points = 12 * V + 12 * Vn + 4 * C + rec * H
+    return int(topo + creases + points)
+
+
+def kernel_bytes(kernel: str, lv: dict, rec: int = 16) -> int:
+    """Per-launch algorithmic bytes of one kernel at parent depth `lv`."""
+    H, V, F, E, C = lv["H"], lv["V"], lv["F"], lv["E"], lv["C"]
+    if kernel in ("topology", "uvs"):
+        return int(rec * H + 4 * rec * H)
+    if kernel == "creases":
+        return int(36 * C)
+    if kernel == "face_points":
+        return int(rec * H + 12 * V + 12 * F)
+    if kernel == "edge_points":
+        return int(rec * H + 12 * V + 12 * F + 12 * C + 12 * E)
+    if kernel == "vertex_points":
+        return int(rec * H + 12 * V + 12 * F + 12 * E + 12 * C + 12 * V)
+    if kernel == "clear":
+        return int(12 * V)
+    if kernel == "level_fused":
+        return int(rec * H + 4 * rec * H + 36 * C + 12 * V + 12 * (V + F + E))
+    if kernel == "adjoint":
+        return int(rec * H + 12 * C + 12 * (V + F + E) + 12 * V)
+    return 0
+
+
+def total_halfedges(levels: list[dict]) -> int:
+    """Refined halfedges of depths 1..D (the unit of the headline metric)."""
+    return int(sum(lv["H"] for lv in levels[1:]))

@@ -1,0 +1,237 @@
+/*
+ * ccs_cuda.h -- C ABI of the B200 (sm_100a) Catmull-Clark refinement library.
+ *
+ * Drop-in for the refinement entry points of jdupuy/HalfedgeCatmullClark's
+ * CatmullClark.h.  The library keeps the reference's data layout: a
+ * `cc_Mesh` cage goes in, a `cc_Subd` with the packed level-by-level
+ * halfedge / crease / vertex-point arrays comes out, byte-compatible with
+ * the reference's accessors (ccs_HalfedgeTwinID, ccs_VertexPoint, ...).
+ * Each `_cuda` function replaces the reference function of the same name
+ * without the suffix; the work runs as CUDA kernels on the GPU that is
+ * current when `ccs_Create_cuda` is called, and results reach the host
+ * arrays of the `cc_Subd` by `ccs_Download_cuda`.
+ *
+ * Differences from the reference, all deliberate:
+ *   - functions return a status (CCS_OK = 0) instead of void / aborting;
+ *     C code that ignores the result still compiles unchanged;
+ *   - a subd made by ccs_Create_cuda must be released by ccs_Release_cuda;
+ *   - the host arrays of such a subd are written only by ccs_Download_cuda.
+ *
+ * Thread safety: calls on one subd must not overlap; distinct subds are
+ * independent.  Each subd owns one CUDA stream (replaceable with
+ * ccs_SetStream_cuda); every call is stream-ordered on it and the refine
+ * calls return without waiting for the GPU.
+ *
+ * Include CatmullClark.h before this header to share its type definitions;
+ * otherwise this header defines the same types with the same layout.
+ */
+#ifndef CCS_CUDA_H
+#define CCS_CUDA_H
+
+#include <stdint.h>
+#include <stddef.h>
+#include <stdbool.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#ifndef CC_INCLUDE_CC_H
+#define CC_INCLUDE_CC_H
+/* Types of CatmullClark.h:17-71 and :136-142, same members and layout. */
+typedef union { struct { float x, y, z; }; float array[3]; } cc_VertexPoint;
+typedef union { struct { float u, v; }; float array[2]; } cc_VertexUv;
+typedef struct { int32_t nextID; int32_t prevID; float sharpness; } cc_Crease;
+typedef struct {
+    int32_t twinID, nextID, prevID, faceID, edgeID, vertexID, uvID;
+} cc_Halfedge;
+typedef struct {
+    int32_t twinID;
+    int32_t edgeID;
+    int32_t vertexID;
+#ifndef CC_DISABLE_UV
+    int32_t uvID;
+#endif
+} cc_Halfedge_SemiRegular;
+typedef struct {
+    int32_t vertexCount;
+    int32_t uvCount;
+    int32_t halfedgeCount;
+    int32_t edgeCount;
+    int32_t faceCount;
+    int32_t *vertexToHalfedgeIDs;
+    int32_t *edgeToHalfedgeIDs;
+    int32_t *faceToHalfedgeIDs;
+    cc_VertexPoint *vertexPoints;
+    cc_VertexUv *uvs;
+    cc_Halfedge *halfedges;
+    cc_Crease *creases;
+} cc_Mesh;
+typedef struct {
+    const cc_Mesh *cage;
+    cc_VertexPoint *vertexPoints;
+    cc_Halfedge_SemiRegular *halfedges;
+    cc_Crease *creases;
+    int32_t maxDepth;
+} cc_Subd;
+#endif /* CC_INCLUDE_CC_H */
+
+/* Status codes.  The reference aborts through CC_ASSERT (CatmullClark.h:
+ * 227-230) or returns NULL; this library returns one of these instead. */
+enum {
+    CCS_OK = 0,
+    CCS_ERR_ARG = -1,          /* NULL / inconsistent argument            */
+    CCS_ERR_ALLOC = -2,        /* host or device allocation failed        */
+    CCS_ERR_OVERFLOW = -3,     /* a count at this depth exceeds int32     */
+    CCS_ERR_CUDA = -4,         /* a CUDA call failed                      */
+    CCS_ERR_TIMEOUT = -5,      /* a bounded device wait gave up           */
+    CCS_ERR_STATE = -6,        /* call order (e.g. points before topology) */
+    CCS_ERR_UNSUPPORTED = -7   /* option not available for this layout     */
+};
+
+/* Flags for ccs_CreateEx_cuda / ccs_SetFlags_cuda. */
+enum {
+    CCS_FLAG_NO_UV = 1u << 0,          /* 12-byte halfedge records (the
+                                          CC_DISABLE_UV build of the record) */
+    CCS_FLAG_PAGEABLE_HOST = 1u << 1,  /* host arrays from malloc, not pinned */
+    CCS_FLAG_DETERMINISTIC = 1u << 2,  /* scatter rule summed per vertex in a
+                                          fixed order instead of atomics      */
+    CCS_FLAG_NO_GRAPH = 1u << 3,       /* launch kernels one by one instead
+                                          of replaying a captured CUDA graph  */
+    CCS_FLAG_SEPARATE_PASSES = 1u << 4 /* run the reference's pass structure
+                                          (no per-level kernel fusion)        */
+};
+
+/* ---------------------------------------------------------------------- */
+/* Construction / destruction                                              */
+/* ---------------------------------------------------------------------- */
+
+/* Replaces ccs_Create (CatmullClark.h:145, :953-970).  Allocates the host
+ * arrays of the returned subd (pinned) and their device mirrors, uploads the
+ * cage.  The cage is borrowed and must outlive the subd.  Returns NULL on
+ * failure; ccs_LastError_cuda() tells why.  16-byte records (with uvID). */
+cc_Subd *ccs_Create_cuda(const cc_Mesh *cage, int32_t maxDepth);
+
+/* ccs_Create_cuda with CCS_FLAG_* options; *out receives the subd. */
+int ccs_CreateEx_cuda(const cc_Mesh *cage, int32_t maxDepth, uint32_t flags, cc_Subd **out);
+
+/* Replaces ccs_Release (CatmullClark.h:146, :977-983). NULL is a no-op. */
+void ccs_Release_cuda(cc_Subd *subd);
+
+/* ---------------------------------------------------------------------- */
+/* Refinement (CatmullClark.h:197-212)                                     */
+/* ---------------------------------------------------------------------- */
+int ccs_Refine_Scatter_cuda(cc_Subd *subd);                   /* :198, :3060 */
+int ccs_Refine_Gather_cuda(cc_Subd *subd);                    /* :199, :3066 */
+int ccs_RefineVertexPoints_Gather_cuda(cc_Subd *subd);        /* :200, :2659 */
+int ccs_RefineVertexPoints_Scatter_cuda(cc_Subd *subd);       /* :201, :2631 */
+int ccs_RefineHalfedges_cuda(cc_Subd *subd);                  /* :202, :2803 */
+int ccs_RefineCreases_cuda(cc_Subd *subd);                    /* :203, :3033 */
+int ccs_RefineVertexUvs_cuda(cc_Subd *subd);                  /* :205, :2928 */
+int ccs_Refine_NoCreases_Gather_cuda(cc_Subd *subd);          /* :209, :3078 */
+int ccs_Refine_NoCreases_Scatter_cuda(cc_Subd *subd);         /* :210, :3072 */
+int ccs_RefineVertexPoints_NoCreases_Gather_cuda(cc_Subd *subd);   /* :211, :2672 */
+int ccs_RefineVertexPoints_NoCreases_Scatter_cuda(cc_Subd *subd);  /* :212, :2645 */
+
+/* ---------------------------------------------------------------------- */
+/* Host <-> device                                                         */
+/* ---------------------------------------------------------------------- */
+
+/* Copies the device halfedges, creases and points into subd->halfedges,
+ * subd->creases and subd->vertexPoints, then waits for the copy.  After it
+ * the reference's accessors (CatmullClark.h:986-1395) read the results. */
+int ccs_Download_cuda(cc_Subd *subd);
+
+/* Uploads new cage points (V0 records) -- NULL re-reads subd->cage. */
+int ccs_UploadCagePoints_cuda(cc_Subd *subd, const cc_VertexPoint *points);
+
+/* Stream control.  `stream` is a cudaStream_t (NULL = the legacy default
+ * stream).  The subd does not take ownership of a stream set this way. */
+int ccs_SetStream_cuda(cc_Subd *subd, void *stream);
+void *ccs_GetStream_cuda(const cc_Subd *subd);
+int ccs_Synchronize_cuda(cc_Subd *subd);
+int ccs_SetFlags_cuda(cc_Subd *subd, uint32_t flags);
+uint32_t ccs_GetFlags_cuda(const cc_Subd *subd);
+
+/* Device addresses of the subd's arrays (same layout as the host arrays). */
+typedef struct {
+    void *halfedges;          /* cumH records of 16 (or 12) bytes            */
+    cc_Crease *creases;       /* cumC records                                */
+    float *vertexPoints;      /* cumV x 3 floats                             */
+    float *cagePoints;        /* V0 x 3 floats                               */
+    int64_t halfedgeCount, creaseCount, vertexCount;
+    int32_t recordBytes;      /* 16, or 12 with CCS_FLAG_NO_UV               */
+} ccs_DeviceArrays;
+int ccs_GetDeviceArrays_cuda(const cc_Subd *subd, ccs_DeviceArrays *out);
+
+/* ---------------------------------------------------------------------- */
+/* Points from caller-owned device buffers (no reference counterpart: the   */
+/* building blocks of the PyTorch extension's autograd function).           */
+/* ---------------------------------------------------------------------- */
+
+/* Point modes. */
+enum { CCS_POINTS_SCATTER = 0, CCS_POINTS_GATHER = 1,
+       CCS_POINTS_NOCREASES_SCATTER = 2, CCS_POINTS_NOCREASES_GATHER = 3 };
+
+/* Refines `cagePoints` (V0 x 3 floats, device) through the subd's device
+ * topology into `points` (cumV x 3 floats, device) on `stream`.  The
+ * topology must have been refined (ccs_RefineHalfedges_cuda and
+ * ccs_RefineCreases_cuda, or a ccs_Refine_* call). */
+int ccs_RefinePointsDevice_cuda(cc_Subd *subd, const float *cagePoints, float *points,
+                                int mode, void *stream);
+
+/* Adjoint of the scatter point rule: given dL/dpoints (cumV x 3, device),
+ * writes dL/dcagePoints (V0 x 3, device).  Runs the transposed face, edge
+ * and vertex rules as gathers, deepest level first.  Uses a scratch buffer
+ * of cumV x 3 floats that the library allocates on first use and keeps. */
+int ccs_AdjointPointsDevice_cuda(cc_Subd *subd, const float *gradPoints, float *gradCage,
+                                 void *stream);
+
+/* ---------------------------------------------------------------------- */
+/* Counts (int64, with the int32 overflow check the library applies)       */
+/* ---------------------------------------------------------------------- */
+typedef struct {
+    int64_t H, F, E, V, C;            /* counts at one depth                */
+    int64_t cumH, cumC, cumV;         /* offset of this depth's arrays      */
+} ccs_LevelCounts;
+/* Level counts of depth 0..maxDepth (maxDepth+1 entries).  Returns
+ * CCS_ERR_OVERFLOW when a count the reference stores in int32 would
+ * overflow at that depth. */
+int ccs_LevelCounts_cuda(const cc_Mesh *cage, int32_t maxDepth, ccs_LevelCounts *out);
+/* Largest depth whose counts all fit the reference's int32 arithmetic. */
+int32_t ccs_MaxSupportedDepth_cuda(const cc_Mesh *cage);
+
+/* ---------------------------------------------------------------------- */
+/* Kernel timing (profiling aid)                                           */
+/* ---------------------------------------------------------------------- */
+typedef struct {
+    int32_t kernel;           /* CCS_K_* identifier                          */
+    int32_t level;            /* parent depth the launch refines             */
+    float ms;                 /* device time between CUDA events             */
+    int64_t units;            /* parent halfedges / creases processed        */
+} ccs_KernelTime;
+enum {
+    CCS_K_TOPOLOGY = 0, CCS_K_CREASES = 1, CCS_K_FACE_POINTS = 2, CCS_K_EDGE_POINTS = 3,
+    CCS_K_VERTEX_POINTS = 4, CCS_K_CLEAR = 5, CCS_K_LEVEL_FUSED = 6, CCS_K_ADJOINT = 7,
+    CCS_K_UVS = 8, CCS_K_COUNT = 9
+};
+/* When enabled, every launch of the subd is bracketed by CUDA events on its
+ * stream (and CUDA graphs are not used). */
+int ccs_SetProfiling_cuda(cc_Subd *subd, int enable);
+/* Copies up to `cap` records of the launches since the last call (waits for
+ * the stream); returns the number of records, or a negative status. */
+int ccs_ReadProfile_cuda(cc_Subd *subd, ccs_KernelTime *out, int cap);
+const char *ccs_KernelName_cuda(int kernel);
+
+/* ---------------------------------------------------------------------- */
+/* Errors                                                                  */
+/* ---------------------------------------------------------------------- */
+int ccs_LastError_cuda(void);                 /* last status of this thread */
+const char *ccs_ErrorString_cuda(int status);
+const char *ccs_Version_cuda(void);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* CCS_CUDA_H */

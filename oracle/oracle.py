@@ -102,11 +102,13 @@ def counts(cage, depth: int) -> dict:
 
 
 def edge_to_halfedge(cage, edge: int, depth: int) -> int:
-    return int(_lib(np.float32).or_edge_to_halfedge(_CageRef(cage).addr, edge, depth))
+    c = _CageRef(cage)
+    return int(_lib(np.float32).or_edge_to_halfedge(c.addr, edge, depth))
 
 
 def vertex_to_halfedge(cage, vertex: int, depth: int) -> int:
-    return int(_lib(np.float32).or_vertex_to_halfedge(_CageRef(cage).addr, vertex, depth))
+    c = _CageRef(cage)
+    return int(_lib(np.float32).or_vertex_to_halfedge(c.addr, vertex, depth))
 
 
 _POINT_FNS = {

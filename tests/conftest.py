@@ -1,0 +1,65 @@
+"""Shared test setup.
+
+Markers: ``gpu`` tests need a CUDA device and the built library; everything
+else runs on the CPU.  The checker (``oracle/``) is built on demand from its
+committed sources with gcc.
+"""
+import glob
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+REFERENCE_MESHES = "/root/reference/examples/meshes"
+LOCAL_MESHES = os.path.join(ROOT, "tests", "golden", "_ccm")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200) and lib/libccs_cuda.so")
+    config.addinivalue_line("markers", "slow: larger workloads")
+
+
+def ccm_paths():
+    """Cage fixtures: the reference's sample .ccm files when present.
+
+    They are read from the reference checkout, or from the untracked copy
+    under tests/golden/_ccm that tests/golden/make_golden.py makes so that
+    they travel with the working tree to a GPU machine.
+    """
+    for d in (REFERENCE_MESHES, LOCAL_MESHES):
+        paths = sorted(glob.glob(os.path.join(d, "*.ccm")))
+        if paths:
+            return paths
+    return []
+
+
+@pytest.fixture(scope="session")
+def small_workloads():
+    from halfedgecatmullclark_b200 import configs
+    return [
+        configs.torus_quads(depth=3),
+        configs.mixed_torus(nu=16, nv=12, strip=6, depth=3, seed=1),
+        configs.mixed_torus(nu=10, nv=9, strip=4, depth=4, seed=2, with_uv=True),
+        configs.height_grid(n=12, depth=3, seed=3),
+        configs.fitting_cage(nu=12, nv=10, depth=3, seed=4),
+    ]
+
+
+def gpu_available():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+def rel_err(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    den = np.abs(b).max()
+    return float(np.abs(a - b).max() / (den if den > 0 else 1.0))

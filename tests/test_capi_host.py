@@ -1,0 +1,125 @@
+"""The C ABI library without a GPU: it loads, exports every declared symbol,
+and its host-side validation returns the documented status codes."""
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, gpu_available
+
+HEADER = os.path.join(ROOT, "include", "ccs_cuda.h")
+
+
+def declared_symbols():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(ccs_\w+_cuda)\s*\(", text)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from halfedgecatmullclark_b200 import _native
+    if not os.path.exists(_native.LIB_PATH):
+        from halfedgecatmullclark_b200 import build
+        build.build()
+    return _native.lib()
+
+
+def test_every_declared_symbol_is_exported(lib):
+    from halfedgecatmullclark_b200 import _native
+    syms = declared_symbols()
+    assert len(syms) >= 30
+    out = subprocess.run(["nm", "-D", "--defined-only", _native.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r" T (ccs_\w+_cuda)", out))
+    missing = [s for s in syms if s not in exported]
+    assert not missing, missing
+    assert set(syms) == set(_native.SIGNATURES), set(syms) ^ set(_native.SIGNATURES)
+    for s in syms:
+        getattr(lib, s)
+
+
+def test_header_compiles_as_c_and_cpp(tmp_path):
+    src = tmp_path / "t.c"
+    src.write_text('#include "ccs_cuda.h"\nint main(void){ cc_Subd *s = ccs_Create_cuda(0, 1);\n'
+                   ' ccs_Refine_Scatter_cuda(s); ccs_Release_cuda(s); return 0; }\n')
+    for cc, std in (("gcc", "-std=c11"), ("g++", "-std=c++17")):
+        r = subprocess.run([cc, std, "-fsyntax-only", "-I" + os.path.dirname(HEADER), "-x",
+                            "c" if cc == "gcc" else "c++", str(src)], capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+
+
+def test_header_shares_types_with_reference_header(tmp_path):
+    ref = "/root/reference/CatmullClark.h"
+    if not os.path.exists(ref):
+        pytest.skip("reference header not available")
+    src = tmp_path / "t.c"
+    src.write_text('#include "CatmullClark.h"\n#include "ccs_cuda.h"\n'
+                   '_Static_assert(sizeof(cc_Halfedge_SemiRegular) == 16, "record");\n'
+                   '_Static_assert(sizeof(cc_Crease) == 12, "crease");\n'
+                   'int f(cc_Subd *s){ return ccs_Refine_Scatter_cuda(s) + ccs_HalfedgeTwinID(s, 0, 1); }\n')
+    r = subprocess.run(["gcc", "-std=gnu11", "-fsyntax-only", "-I/root/reference",
+                        "-I" + os.path.dirname(HEADER), str(src)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+
+
+def test_error_strings(lib):
+    for code in (0, -1, -2, -3, -4, -5, -6, -7):
+        assert lib.ccs_ErrorString_cuda(code)
+    assert b"sm_100a" in lib.ccs_Version_cuda()
+
+
+def test_invalid_arguments_are_refused_on_the_host(lib):
+    from halfedgecatmullclark_b200 import configs
+    out = ctypes.c_void_p()
+    assert lib.ccs_CreateEx_cuda(None, 3, 0, ctypes.byref(out)) == -1
+    assert lib.ccs_LastError_cuda() == -1
+    w = configs.torus_quads()
+    m = w.cage.as_cc_mesh()
+    assert lib.ccs_CreateEx_cuda(ctypes.byref(m), 0, 0, ctypes.byref(out)) == -1     # depth 0
+    assert lib.ccs_CreateEx_cuda(ctypes.byref(m), 3, 0, None) == -1                 # no out
+    bad = w.cage.copy()
+    bad.halfedges["twinID"][5] = bad.H + 3                                          # twin out of range
+    mb = bad.as_cc_mesh()
+    assert lib.ccs_CreateEx_cuda(ctypes.byref(mb), 3, 0, ctypes.byref(out)) == -1
+    bad = w.cage.copy()
+    bad.halfedges["nextID"][0], bad.halfedges["nextID"][1] = bad.halfedges["nextID"][1], bad.halfedges["nextID"][0]
+    mb = bad.as_cc_mesh()
+    assert lib.ccs_CreateEx_cuda(ctypes.byref(mb), 3, 0, ctypes.byref(out)) == -1   # next/prev broken
+    bad = w.cage.copy()
+    bad.creases["nextID"][2] = -5
+    mb = bad.as_cc_mesh()
+    assert lib.ccs_CreateEx_cuda(ctypes.byref(mb), 3, 0, ctypes.byref(out)) == -1   # crease link
+    big = configs.height_grid(n=256)
+    mg = big.cage.as_cc_mesh()
+    assert lib.ccs_CreateEx_cuda(ctypes.byref(mg), 6, 0, ctypes.byref(out)) == -3   # int32 overflow
+    # calls on a subd this library did not create
+    fake = ctypes.create_string_buffer(64)
+    assert lib.ccs_Refine_Scatter_cuda(fake) == -1
+    assert lib.ccs_Download_cuda(fake) == -1
+    lib.ccs_Release_cuda(None)
+
+
+def test_create_without_gpu_reports_cuda_error(lib):
+    if gpu_available():
+        pytest.skip("a GPU is present")
+    from halfedgecatmullclark_b200 import configs
+    w = configs.torus_quads()
+    m = w.cage.as_cc_mesh()
+    out = ctypes.c_void_p()
+    assert lib.ccs_CreateEx_cuda(ctypes.byref(m), 2, 0, ctypes.byref(out)) == -4
+    assert not out.value
+
+
+def test_level_counts_api(lib):
+    from halfedgecatmullclark_b200 import _native as N
+    from halfedgecatmullclark_b200 import configs
+    w = configs.torus_quads()
+    m = w.cage.as_cc_mesh()
+    arr = (N.LevelCounts * 5)()
+    assert lib.ccs_LevelCounts_cuda(ctypes.byref(m), 4, arr) == 0
+    assert [arr[d].H for d in range(5)] == [2048 * 4 ** d for d in range(5)]
+    assert arr[4].cumH == sum(2048 * 4 ** d for d in range(1, 4))
+    assert lib.ccs_MaxSupportedDepth_cuda(ctypes.byref(m)) >= 9
