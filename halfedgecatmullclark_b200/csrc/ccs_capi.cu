@@ -120,6 +120,18 @@ static int validate_cage(const cc_Mesh* m) {
     return CCS_OK;
 }
 
+// The fused level kernels read a twin's endpoints from its partner:
+// vertex(twin(h)) == vertex(next(h)).  Refinement preserves the relation, so
+// checking the cage is enough.
+static bool twins_consistent(const cc_Mesh* m) {
+    const cc_Halfedge* he = m->halfedges;
+    for (int32_t h = 0; h < m->halfedgeCount; ++h) {
+        const int32_t t = he[h].twinID;
+        if (t >= 0 && he[t].vertexID != he[he[h].nextID].vertexID) return false;
+    }
+    return true;
+}
+
 // ---------------------------------------------------------------------------
 // profiling
 // ---------------------------------------------------------------------------
@@ -157,6 +169,7 @@ struct SubdImpl {
     bool own_stream = false;
     bool pinned = true;
     bool topo_ready = false, creases_ready = false;
+    bool fusable = true;           // twin relation holds: fused kernels allowed
     Profiler prof;
     std::map<int, cudaGraphExec_t> graphs;
 
@@ -249,6 +262,7 @@ static int create(const cc_Mesh* cage, int32_t D, uint32_t flags, cc_Subd** out)
     s->cage = cage;
     s->D = D;
     s->flags = flags;
+    s->fusable = twins_consistent(cage);
     s->rw = (flags & CCS_FLAG_NO_UV) ? 3 : 4;
     s->lv = lv;
     s->cumH = cum_of(lv, 'H');
@@ -307,23 +321,25 @@ enum Op {
 // Enqueue the launches of one operation on `st`.
 static cudaError_t enqueue(SubdImpl* s, int op, cudaStream_t st) {
     Ctx c = s->ctx(st);
-    const bool det = (s->flags & CCS_FLAG_DETERMINISTIC) != 0;
-    (void)det;
     const bool uv = s->dc.U > 0 && s->rw == 4;
     cudaError_t e = cudaSuccess;
     if (op == OP_HALFEDGES) return run_topology(c, true, false);
     if (op == OP_CREASES) return run_creases(c);
     if (op == OP_UVS) return uv ? run_topology(c, false, true) : cudaSuccess;
-    if (op >= OP_REFINE_BASE) {
-        const int k = op - OP_REFINE_BASE;
-        e = run_topology(c, true, uv);
-        if (e == cudaSuccess) e = run_creases(c);
-        if (e == cudaSuccess) e = run_points(c, s->dc.pts, s->pts, k >> 1, (k & 1) != 0);
+    if (op >= OP_REFINE_BASE || op >= OP_POINTS_BASE) {
+        const bool refine = op >= OP_REFINE_BASE;
+        const int k = op - (refine ? OP_REFINE_BASE : OP_POINTS_BASE);
+        const int mode = k >> 1;
+        const bool det = (k & 1) != 0;
+        const bool scatter = mode == CCS_POINTS_SCATTER || mode == CCS_POINTS_NOCREASES_SCATTER;
+        if (scatter && s->fusable && !(s->flags & CCS_FLAG_SEPARATE_PASSES))
+            return run_fused(c, refine, s->dc.pts, s->pts, mode, det);
+        if (refine) {
+            e = run_topology(c, true, uv);
+            if (e == cudaSuccess) e = run_creases(c);
+        }
+        if (e == cudaSuccess) e = run_points(c, s->dc.pts, s->pts, mode, det);
         return e;
-    }
-    if (op >= OP_POINTS_BASE) {
-        const int k = op - OP_POINTS_BASE;
-        return run_points(c, s->dc.pts, s->pts, k >> 1, (k & 1) != 0);
     }
     return cudaErrorInvalidValue;
 }
@@ -527,7 +543,11 @@ int ccs_RefinePointsDevice_cuda(cc_Subd* subd, const float* cagePoints, float* p
     DeviceGuard g(s->device);
     Ctx c = s->ctx((cudaStream_t)stream);
     const bool det = (s->flags & CCS_FLAG_DETERMINISTIC) != 0;
-    return ret(run_points(c, cagePoints, points, mode, det) == cudaSuccess ? CCS_OK : CCS_ERR_CUDA);
+    const bool scatter = mode == CCS_POINTS_SCATTER || mode == CCS_POINTS_NOCREASES_SCATTER;
+    const cudaError_t e = (scatter && s->fusable && !(s->flags & CCS_FLAG_SEPARATE_PASSES))
+                              ? run_fused(c, false, cagePoints, points, mode, det)
+                              : run_points(c, cagePoints, points, mode, det);
+    return ret(e == cudaSuccess ? CCS_OK : CCS_ERR_CUDA);
 }
 
 int ccs_AdjointPointsDevice_cuda(cc_Subd* subd, const float* gradPoints, float* gradCage, void* stream) {
@@ -595,7 +615,7 @@ int ccs_ReadProfile_cuda(cc_Subd* subd, ccs_KernelTime* out, int cap) {
 
 const char* ccs_KernelName_cuda(int kernel) {
     static const char* names[] = {"topology", "creases", "face_points", "edge_points", "vertex_points",
-                                  "clear", "level_fused", "adjoint", "uvs"};
+                                  "clear", "level_fused", "adjoint", "uvs", "level_points"};
     return (kernel >= 0 && kernel < CCS_K_COUNT) ? names[kernel] : "unknown";
 }
 

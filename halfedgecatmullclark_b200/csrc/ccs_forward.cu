@@ -603,6 +603,42 @@ static void points_level(const Ctx& c, const View& L, const float* pin, float* p
     }
 }
 
+// The cage step of the fused pipeline: topology (+UV) and creases of depth 1,
+// then the cage's face, edge and vertex points.
+cudaError_t run_cage_step(const Ctx& c, bool topo, bool uv, const float* cagePts, float* pout, int mode, bool det) {
+    if (topo) {
+        if (c.rw == 4) {
+            if (uv) launch_topology_level<4, true, true>(c, 0);
+            else launch_topology_level<4, true, false>(c, 0);
+        } else {
+            launch_topology_level<3, true, false>(c, 0);
+        }
+        const int32_t C = c.lv[0].C;
+        c.prof->begin(c.stream, CCS_K_CREASES, 0, C);
+        k_creases<<<nblocks(C), kBlock, 0, c.stream>>>(c.cage->cr, c.cr + c.lv[1].crOff, C);
+        c.prof->end(c.stream);
+    }
+    points_level(c, cage_view(c), cagePts, pout, mode, det);
+    return cudaGetLastError();
+}
+
+// Vertex pass of quad level d, summed per vertex in increasing halfedge order.
+cudaError_t run_vertex_det_level(const Ctx& c, int d, const float* pin, float* pout, bool creased) {
+    c.prof->begin(c.stream, CCS_K_VERTEX_POINTS, d, c.lv[d].H);
+    const unsigned nb = nblocks(c.lv[d].V);
+    if (c.rw == 4) {
+        const QuadView<4> L = quad_view<4>(c, d);
+        if (creased) k_vertex_det<QuadView<4>, true><<<nb, kBlock, 0, c.stream>>>(L, pin, pout);
+        else k_vertex_det<QuadView<4>, false><<<nb, kBlock, 0, c.stream>>>(L, pin, pout);
+    } else {
+        const QuadView<3> L = quad_view<3>(c, d);
+        if (creased) k_vertex_det<QuadView<3>, true><<<nb, kBlock, 0, c.stream>>>(L, pin, pout);
+        else k_vertex_det<QuadView<3>, false><<<nb, kBlock, 0, c.stream>>>(L, pin, pout);
+    }
+    c.prof->end(c.stream);
+    return cudaGetLastError();
+}
+
 cudaError_t run_points(const Ctx& c, const float* cagePts, float* pts, int mode, bool det) {
     for (int d = 0; d < c.D; ++d) {
         float* pout = pts + 3 * c.lv[d + 1].ptOff;

@@ -64,6 +64,10 @@ cudaError_t run_topology(const Ctx& c, bool topo, bool uv);
 cudaError_t run_creases(const Ctx& c);
 // mode: CCS_POINTS_*; deterministic selects the fixed-order scatter sum.
 cudaError_t run_points(const Ctx& c, const float* cagePts, float* pts, int mode, bool deterministic);
+// Fused scatter pipeline (ccs_level.cu): cage step, then two kernels per quad
+// level.  topo = also refine halfedges, UVs and creases.  mode must be
+// CCS_POINTS_SCATTER or CCS_POINTS_NOCREASES_SCATTER.
+cudaError_t run_fused(const Ctx& c, bool topo, const float* cagePts, float* pts, int mode, bool deterministic);
 
 // Adjoint (ccs_adjoint.cu).  `work` holds cumV x 3 floats.
 cudaError_t run_adjoint(const Ctx& c, const float* gradPts, float* work, float* gradCage, int64_t cumV);

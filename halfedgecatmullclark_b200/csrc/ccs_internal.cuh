@@ -13,6 +13,9 @@
 
 namespace ccs {
 
+// Upper bound on the steps of any ring or face walk in device code.
+static constexpr int kWalkCap = 1 << 16;
+
 // ---------------------------------------------------------------------------
 // Exact float helpers (CatmullClark.h:295-392)
 // ---------------------------------------------------------------------------
@@ -251,7 +254,10 @@ __device__ __forceinline__ RingStats creased_ring(const View& L, int32_t h) {
     r.creaseCount = fsign(prevS);
     r.valence = 1.0f;
     int32_t fwd, bwd;
-    for (fwd = L.twin(prev); fwd >= 0 && fwd != h; fwd = L.twin(fwd)) {
+    // Both walks terminate on a manifold ring; the cap only bounds the work
+    // on a malformed one (it never triggers on a valid mesh).
+    int guard = 0;
+    for (fwd = L.twin(prev); fwd >= 0 && fwd != h && guard < kWalkCap; fwd = L.twin(fwd), ++guard) {
         const int32_t p = L.prev(fwd);
         const float s = L.hsharp(p);
         r.valence = fadd(r.valence, 1.0f);
@@ -259,7 +265,8 @@ __device__ __forceinline__ RingStats creased_ring(const View& L, int32_t h) {
         r.creaseCount = fadd(r.creaseCount, fsign(s));
         fwd = p;
     }
-    for (bwd = L.twin(h); fwd < 0 && bwd >= 0 && bwd != h; bwd = L.twin(bwd)) {
+    guard = 0;
+    for (bwd = L.twin(h); fwd < 0 && bwd >= 0 && bwd != h && guard < kWalkCap; bwd = L.twin(bwd), ++guard) {
         const int32_t n = L.next(bwd);
         const float s = L.hsharp(n);
         r.valence = fadd(r.valence, 1.0f);
@@ -309,9 +316,12 @@ __device__ __forceinline__ f3 creased_vertex_share(const View& L, int32_t h, con
 template <class View>
 __device__ __forceinline__ f3 smooth_vertex_share(const View& L, int32_t h, const float* __restrict__ pin,
                                                   const float* __restrict__ fpt, const float* __restrict__ ept) {
-    int32_t valence = 1, fwd, bwd;
-    for (fwd = L.prev_vertex_he(h); fwd >= 0 && fwd != h; fwd = L.prev_vertex_he(fwd)) ++valence;
-    for (bwd = L.next_vertex_he(h); fwd < 0 && bwd >= 0 && bwd != h; bwd = L.next_vertex_he(bwd)) ++valence;
+    int32_t valence = 1, fwd, bwd, guard = 0;
+    for (fwd = L.prev_vertex_he(h); fwd >= 0 && fwd != h && guard < kWalkCap; fwd = L.prev_vertex_he(fwd), ++guard)
+        ++valence;
+    guard = 0;
+    for (bwd = L.next_vertex_he(h); fwd < 0 && bwd >= 0 && bwd != h && guard < kWalkCap; bwd = L.next_vertex_he(bwd), ++guard)
+        ++valence;
     const f3 v = ld3(pin + 3 * (int64_t)L.vert(h));
     const f3 f = ld3(fpt + 3 * (int64_t)L.face(h));
     const f3 e = ld3(ept + 3 * (int64_t)L.edge(h));

@@ -40,7 +40,13 @@ def kernel_bytes(kernel: str, lv: dict, rec: int = 16) -> int:
     if kernel == "clear":
         return int(12 * V)
     if kernel == "level_fused":
-        return int(rec * H + 4 * rec * H + 36 * C + 12 * V + 12 * (V + F + E))
+        # records in + children out + creases + old points in + face points
+        # out + the cleared old-vertex slots
+        return int(rec * H + 4 * rec * H + 36 * C + 12 * V + 12 * F + 12 * V)
+    if kernel == "level_points":
+        # records + old points + face points + crease records in; edge points
+        # out; vertex points accumulated (written once)
+        return int(rec * H + 12 * V + 12 * F + 12 * C + 12 * E + 12 * V)
     if kernel == "adjoint":
         return int(rec * H + 12 * C + 12 * (V + F + E) + 12 * V)
     return 0

@@ -131,6 +131,19 @@ def test_points_before_topology_is_an_error(small_workloads):
         assert ei.value.code == -6
 
 
+@pytest.mark.parametrize("mode", ["scatter", "nocreases_scatter"])
+def test_fused_and_separate_passes_agree(small_workloads, mode):
+    """Fused level kernels == the reference's pass structure, bit for bit."""
+    from halfedgecatmullclark_b200 import _native as N
+    for w in small_workloads:
+        a = gpu_refine(w.cage, w.depth, mode, N.FLAG_DETERMINISTIC)
+        b = gpu_refine(w.cage, w.depth, mode, N.FLAG_DETERMINISTIC | N.FLAG_SEPARATE_PASSES)
+        for x, y in zip(a, b):
+            assert np.array_equal(x.view(np.uint8), y.view(np.uint8)), (w.name, mode)
+        c = gpu_refine(w.cage, w.depth, mode, N.FLAG_SEPARATE_PASSES)
+        assert rel_err(c[2], a[2]) <= TOL_POINTS
+
+
 def test_graph_and_direct_launch_agree(small_workloads):
     from halfedgecatmullclark_b200 import _native as N
     w = small_workloads[1]
