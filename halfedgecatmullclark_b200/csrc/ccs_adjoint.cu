@@ -192,12 +192,7 @@ k_adj_vertices(View L, const float* __restrict__ gNew, float* __restrict__ gOld)
     o[2] += acc.z;
 }
 
-static CageTables cage_tables_a(const DevCage& c) {
-    CageTables t;
-    t.he = c.he; t.v2h = c.v2h; t.e2h = c.e2h; t.f2h = c.f2h; t.uvs = c.uvs;
-    t.n.V = c.V; t.n.F = c.F; t.n.E = c.E; t.n.H = c.H;
-    return t;
-}
+static CageTables cage_tables_a(const DevCage& c) { return make_cage_tables(c); }
 
 template <class View>
 static void adjoint_level(const Ctx& c, const View& L, float* gNew, float* gOld) {

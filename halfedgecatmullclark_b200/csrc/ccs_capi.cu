@@ -209,7 +209,7 @@ static void free_impl(SubdImpl* s) {
     s->graphs.clear();
     for (auto& t : s->prof.pending) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
     cudaFree(s->dc.he); cudaFree(s->dc.cr); cudaFree(s->dc.pts); cudaFree(s->dc.uvs);
-    cudaFree(s->dc.v2h); cudaFree(s->dc.e2h); cudaFree(s->dc.f2h);
+    cudaFree(s->dc.v2h); cudaFree(s->dc.e2h); cudaFree(s->dc.f2h); cudaFree(s->dc.fsz);
     cudaFree(s->he); cudaFree(s->cr); cudaFree(s->pts); cudaFree(s->work); cudaFree(s->err);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     if (s->host) {
@@ -244,6 +244,12 @@ static int upload_cage(SubdImpl* s, const cc_Mesh* m) {
         cudaMemcpyAsync(d.v2h, m->vertexToHalfedgeIDs, sizeof(int32_t) * (size_t)d.V, cudaMemcpyHostToDevice, st) ||
         cudaMemcpyAsync(d.e2h, m->edgeToHalfedgeIDs, sizeof(int32_t) * (size_t)d.E, cudaMemcpyHostToDevice, st) ||
         cudaMemcpyAsync(d.f2h, m->faceToHalfedgeIDs, sizeof(int32_t) * (size_t)d.F, cudaMemcpyHostToDevice, st))
+        return CCS_ERR_CUDA;
+    // face sizes (face-centre valences of depth 1)
+    std::vector<int32_t> fsz((size_t)d.F, 0);
+    for (int32_t h = 0; h < d.H; ++h) ++fsz[(size_t)m->halfedges[h].faceID];
+    if (dmalloc(&d.fsz, sizeof(int32_t) * (size_t)d.F)) return CCS_ERR_ALLOC;
+    if (cudaMemcpyAsync(d.fsz, fsz.data(), sizeof(int32_t) * (size_t)d.F, cudaMemcpyHostToDevice, st))
         return CCS_ERR_CUDA;
     if (cudaStreamSynchronize(st) != cudaSuccess) return CCS_ERR_CUDA;
     return CCS_OK;

@@ -98,7 +98,7 @@ k_quad_topology(const int32_t* __restrict__ in, int32_t* __restrict__ out,
                     fu = fadd(fu, uv_dec(q));
                     fv = fadd(fv, uv_dec(q >> 16));
                 }
-                o_uv = uv_enc(fdiv(fu, 4.0f), fdiv(fv, 4.0f));
+                o_uv = uv_enc(fquarter(fu), fquarter(fv));
                 break;
             }
             default: {
@@ -204,8 +204,8 @@ k_creases(const cc_Crease* __restrict__ in, cc_Crease* __restrict__ out, int32_t
     b.nextID = 2 * nx + (t1 ? 0 : 1);
     a.prevID = 2 * pv + (t2 ? 1 : 0);
     b.prevID = 2 * e + 0;
-    a.sharpness = fmax_ref(0.0f, fsub(fdiv(fadd(cp.sharpness, thisS), 4.0f), 1.0f));
-    b.sharpness = fmax_ref(0.0f, fsub(fdiv(fadd(thisS, cn.sharpness), 4.0f), 1.0f));
+    a.sharpness = fmax_ref(0.0f, fsub(fquarter(fadd(cp.sharpness, thisS)), 1.0f));
+    b.sharpness = fmax_ref(0.0f, fsub(fquarter(fadd(thisS, cn.sharpness)), 1.0f));
     out[2 * i + 0] = a;
     out[2 * i + 1] = b;
 }
@@ -232,7 +232,7 @@ k_face_points(View L, const float* __restrict__ pin, float* __restrict__ pout) {
         } else {
             f3 acc = zero3();
 #pragma unroll
-            for (int k = 0; k < 4; ++k) acc = add3(acc, div3(p[k], 4.0f));
+            for (int k = 0; k < 4; ++k) acc = add3(acc, quarter3(p[k]));
             st3(fp, acc);
         }
     } else {
@@ -245,7 +245,7 @@ k_face_points(View L, const float* __restrict__ pin, float* __restrict__ pout) {
             guard = 0;
             for (int32_t it = L.next(h0); it != h0 && guard < kRingCap; it = L.next(it), ++guard)
                 acc = add3(acc, ld3(pin + 3 * (int64_t)L.vert(it)));
-            st3(fp, mul3(acc, fdiv(1.0f, n)));
+            st3(fp, mul3(acc, frcp(n)));
         } else {
             f3 acc = add3(zero3(), div3(ld3(pin + 3 * (int64_t)L.vert(h0)), n));
             guard = 0;
@@ -426,7 +426,7 @@ k_vertex_gather_smooth(View L, const float* __restrict__ pin, float* __restrict_
         smooth = add3(smooth, mul3(ld3(ept + 3 * (int64_t)L.edge(it)), 4.0f));
         valence = fadd(valence, 1.0f);
     }
-    smooth = add3(mul3(smooth, fdiv(1.0f, fmul(valence, valence))), mul3(P, fsub(1.0f, fdiv(3.0f, valence))));
+    smooth = add3(mul3(smooth, frcp(fmul(valence, valence))), mul3(P, fsub(1.0f, fdiv(3.0f, valence))));
     st3(pout + 3 * (int64_t)v, lerp3(P, smooth, it != h ? 0.0f : 1.0f));
 }
 
@@ -482,7 +482,7 @@ k_vertex_gather_creased(View L, const float* __restrict__ pin, float* __restrict
         creaseCount = fadd(creaseCount, cw);
         valence = fadd(valence, 1.0f);
     }
-    smooth = add3(mul3(smooth, fdiv(1.0f, fmul(valence, valence))), mul3(P, fsub(1.0f, fdiv(3.0f, valence))));
+    smooth = add3(mul3(smooth, frcp(fmul(valence, valence))), mul3(P, fsub(1.0f, fdiv(3.0f, valence))));
     crease = add3(mul3(crease, View::kQuad ? fdiv(0.5f, creaseCount) : 0.25f), mul3(P, 0.5f));
     f3 o;
     if (creaseCount <= 1.0f) o = smooth;
@@ -494,12 +494,7 @@ k_vertex_gather_creased(View L, const float* __restrict__ pin, float* __restrict
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
-static CageTables cage_tables(const DevCage& c) {
-    CageTables t;
-    t.he = c.he; t.v2h = c.v2h; t.e2h = c.e2h; t.f2h = c.f2h; t.uvs = c.uvs;
-    t.n.V = c.V; t.n.F = c.F; t.n.E = c.E; t.n.H = c.H;
-    return t;
-}
+static CageTables cage_tables(const DevCage& c) { return make_cage_tables(c); }
 
 static CageView cage_view(const Ctx& c) {
     CageView L;

@@ -22,6 +22,7 @@ struct DevCage {
     int32_t* v2h = nullptr;
     int32_t* e2h = nullptr;
     int32_t* f2h = nullptr;
+    int32_t* fsz = nullptr;     // F x face size (halfedges per cage face)
     int32_t V = 0, U = 0, H = 0, E = 0, F = 0;
 };
 

@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include "ccs_cuda.h"
+#include "ccs_host.h"
 
 namespace ccs {
 
@@ -36,6 +37,12 @@ __device__ __forceinline__ void st3(float* p, f3 v) { p[0] = v.x; p[1] = v.y; p[
 __device__ __forceinline__ f3 add3(f3 a, f3 b) { return f3{fadd(a.x, b.x), fadd(a.y, b.y), fadd(a.z, b.z)}; }
 __device__ __forceinline__ f3 mul3(f3 a, float s) { return f3{fmul(a.x, s), fmul(a.y, s), fmul(a.z, s)}; }
 __device__ __forceinline__ f3 div3(f3 a, float s) { return f3{fdiv(a.x, s), fdiv(a.y, s), fdiv(a.z, s)}; }
+// x / 4 and x * 0.25 are the same correctly rounded value of x * 2^-2, so the
+// reference's divisions by 4.0f are taken as multiplications.
+__device__ __forceinline__ float fquarter(float x) { return __fmul_rn(x, 0.25f); }
+__device__ __forceinline__ f3 quarter3(f3 a) { return f3{fquarter(a.x), fquarter(a.y), fquarter(a.z)}; }
+// 1.0f / x, correctly rounded (the same value as IEEE division).
+__device__ __forceinline__ float frcp(float x) { return __frcp_rn(x); }
 __device__ __forceinline__ f3 lerp3(f3 a, f3 b, float u) { return f3{flerp(a.x, b.x, u), flerp(a.y, b.y, u), flerp(a.z, b.z, u)}; }
 __device__ __forceinline__ f3 zero3() { return f3{0.0f, 0.0f, 0.0f}; }
 
@@ -92,9 +99,17 @@ struct CageTables {
     const int32_t* __restrict__ v2h;
     const int32_t* __restrict__ e2h;
     const int32_t* __restrict__ f2h;
+    const int32_t* __restrict__ fsz;   // cage face sizes
     const float* __restrict__ uvs;     // U x 2
     CageCounts n;
 };
+
+inline CageTables make_cage_tables(const DevCage& c) {
+    CageTables t;
+    t.he = c.he; t.v2h = c.v2h; t.e2h = c.e2h; t.f2h = c.f2h; t.fsz = c.fsz; t.uvs = c.uvs;
+    t.n.V = c.V; t.n.F = c.F; t.n.E = c.E; t.n.H = c.H;
+    return t;
+}
 
 struct CageView {
     static constexpr bool kQuad = false;
@@ -291,11 +306,11 @@ __device__ __forceinline__ f3 creased_vertex_share(const View& L, int32_t h, con
     const f3 P = ld3(pin + 3 * (int64_t)L.vert(h));
     float valence = r.valence, creaseCount = r.creaseCount;
 
-    const f3 corner = mul3(P, fdiv(1.0f, valence));
+    const f3 corner = mul3(P, frcp(valence));
     f3 crease = add3(mul3(P, fmul(0.25f, cw)), mul3(E, fmul(0.25f, cw)));
     f3 smooth = add3(mul3(F, -1.0f), mul3(E, 4.0f));
     smooth = add3(smooth, mul3(P, fsub(valence, 3.0f)));
-    smooth = mul3(smooth, fdiv(1.0f, fmul(valence, valence)));
+    smooth = mul3(smooth, frcp(fmul(valence, valence)));
     if (r.fwd < 0) {
         creaseCount = fadd(creaseCount, cw);
         valence = fadd(valence, 1.0f);
@@ -325,7 +340,7 @@ __device__ __forceinline__ f3 smooth_vertex_share(const View& L, int32_t h, cons
     const f3 v = ld3(pin + 3 * (int64_t)L.vert(h));
     const f3 f = ld3(fpt + 3 * (int64_t)L.face(h));
     const f3 e = ld3(ept + 3 * (int64_t)L.edge(h));
-    const float w = fdiv(1.0f, (float)valence);
+    const float w = frcp((float)valence);
     const float s = fwd < 0 ? 0.0f : 1.0f;
     const float ws = fmul(w, s);
     f3 o;

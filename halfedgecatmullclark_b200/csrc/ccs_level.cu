@@ -78,7 +78,7 @@ __device__ __forceinline__ f3 shfl3(f3 v, int src) {
 __device__ __forceinline__ f3 quad_face_point(f3 p, int qb) {
     f3 acc = zero3();
 #pragma unroll
-    for (int i = 0; i < 4; ++i) acc = add3(acc, div3(shfl3(p, qb + i), 4.0f));
+    for (int i = 0; i < 4; ++i) acc = add3(acc, quarter3(shfl3(p, qb + i)));
     return acc;
 }
 
@@ -117,8 +117,8 @@ k_level_a(LevelArgs a) {
         y.nextID = 2 * nx + (t1 ? 0 : 1);
         x.prevID = 2 * pv + (t2 ? 1 : 0);
         y.prevID = 2 * e + 0;
-        x.sharpness = fmax_ref(0.0f, fsub(fdiv(fadd(cp.sharpness, thisS), 4.0f), 1.0f));
-        y.sharpness = fmax_ref(0.0f, fsub(fdiv(fadd(thisS, cn.sharpness), 4.0f), 1.0f));
+        x.sharpness = fmax_ref(0.0f, fsub(fquarter(fadd(cp.sharpness, thisS)), 1.0f));
+        y.sharpness = fmax_ref(0.0f, fsub(fquarter(fadd(thisS, cn.sharpness)), 1.0f));
         a.crOut[2 * i + 0] = x;
         a.crOut[2 * i + 1] = y;
         return;
@@ -152,8 +152,8 @@ k_level_a(LevelArgs a) {
             const float uo = __shfl_sync(0xffffffffu, u, lo), vo = __shfl_sync(0xffffffffu, v, lo);
             const float up = __shfl_sync(0xffffffffu, u, lp), vp = __shfl_sync(0xffffffffu, v, lp);
             uvc[1] = uv_enc_fast(flerp(u, un, 0.5f), flerp(v, vn, 0.5f));
-            uvc[2] = uv_enc_fast(fdiv(fadd(fadd(fadd(u, un), uo), up), 4.0f),
-                                 fdiv(fadd(fadd(fadd(v, vn), vo), vp), 4.0f));
+            uvc[2] = uv_enc_fast(fquarter(fadd(fadd(fadd(u, un), uo), up)),
+                                 fquarter(fadd(fadd(fadd(v, vn), vo), vp)));
             uvc[3] = uv_enc_fast(flerp(u, up, 0.5f), flerp(v, vp, 0.5f));
         }
         int32_t* t = tile + tid * 4 * RW;
@@ -246,35 +246,65 @@ k_level_b(QuadView<RW> L, const float* __restrict__ pin, float* __restrict__ pou
     // ---- vertex point share ---------------------------------------------------
     const f3 Ep = shfl3(Eh, qb | ((k + 3) & 3));     // edge point of prev(h)
     const int32_t ped = __shfl_sync(0xffffffffu, ed, qb | ((k + 3) & 3));
+    const int32_t ptw = __shfl_sync(0xffffffffu, tw, qb | ((k + 3) & 3));
     int32_t key = -1 - lane;
     f3 s = zero3();
     if (valid) {
         key = vx;
-        if (CREASED) {
+        // Ring statistics of vertex(h) as the reference's walk from h finds
+        // them (:2523-2566).  At a refined level the vertex of child k of a
+        // parent halfedge is known: k = 2 is a face centre (valence = parent
+        // face size, all edges crease-free), k = 1 and 3 are edge midpoints
+        // (valence 4, or 2 on a boundary; the creased edges are the two halves
+        // e and e^1 of the parent edge), k = 0 is an older vertex that needs
+        // the walk.  Sharpness at depth >= 1 is +0 or positive, so sums with
+        // the crease-free edges' zeros are exact in any order.
+        float vpre, cpre, avgS;
+        bool bnd;
+        if (k == 2) {
+            vpre = L.d == 1 ? (float)L.t.fsz[L.t.he[(int64_t)CH_WORDS * (h >> 2) + CH_FACE]] : 4.0f;
+            cpre = 0.0f; avgS = 0.0f; bnd = false;
+        } else if (k == 1) {
+            const float sa = L.sharp(ped), sb = L.sharp(ped ^ 1);
+            bnd = ptw < 0;
+            vpre = bnd ? 2.0f : 4.0f;
+            avgS = fadd(sa, sb);
+            cpre = fadd(fsign(sa), fsign(sb));
+        } else if (k == 3) {
+            const float sa = L.sharp(ed), sb = L.sharp(ed ^ 1);
+            bnd = tw < 0;
+            vpre = bnd ? 2.0f : 4.0f;
+            avgS = bnd ? sb : fadd(sa, sb);
+            cpre = bnd ? fsign(sb) : fadd(fsign(sa), fsign(sb));
+        } else if (CREASED) {
             const RingStats r = creased_ring(L, h);
+            vpre = r.valence; cpre = r.creaseCount; avgS = r.avgS; bnd = r.fwd < 0;
+        } else {
+            int32_t valence = 1, fwd, bwd, guard = 0;
+            for (fwd = L.prev_vertex_he(h); fwd >= 0 && fwd != h && guard < kWalkCap; fwd = L.prev_vertex_he(fwd), ++guard) ++valence;
+            guard = 0;
+            for (bwd = L.next_vertex_he(h); fwd < 0 && bwd >= 0 && bwd != h && guard < kWalkCap; bwd = L.next_vertex_he(bwd), ++guard) ++valence;
+            vpre = (float)valence; cpre = 0.0f; avgS = 0.0f; bnd = fwd < 0;
+        }
+        if (CREASED) {
             const float cw = fsign(L.sharp(ed)), pcw = fsign(L.sharp(ped));
-            float valence = r.valence, creaseCount = r.creaseCount;
-            const f3 corner = mul3(p, fdiv(1.0f, valence));
+            float valence = vpre, creaseCount = cpre;
+            const f3 corner = mul3(p, frcp(valence));
             f3 crease = add3(mul3(p, fmul(0.25f, cw)), mul3(Eh, fmul(0.25f, cw)));
             f3 smooth = add3(mul3(Fh, -1.0f), mul3(Eh, 4.0f));
             smooth = add3(smooth, mul3(p, fsub(valence, 3.0f)));
-            smooth = mul3(smooth, fdiv(1.0f, fmul(valence, valence)));
-            if (r.fwd < 0) {
+            smooth = mul3(smooth, frcp(fmul(valence, valence)));
+            if (bnd) {
                 creaseCount = fadd(creaseCount, cw);
                 valence = fadd(valence, 1.0f);
                 crease = add3(crease, add3(mul3(p, fmul(0.25f, pcw)), mul3(Ep, fmul(0.25f, pcw))));
             }
             if (creaseCount >= 3.0f || valence == 2.0f) s = corner;
             else if (creaseCount <= 1.0f) s = smooth;
-            else s = lerp3(corner, crease, fsat(fmul(r.avgS, 0.5f)));
+            else s = lerp3(corner, crease, fsat(fmul(avgS, 0.5f)));
         } else {
-            int32_t valence = 1, fwd, bwd;
-            int guard = 0;
-            for (fwd = L.prev_vertex_he(h); fwd >= 0 && fwd != h && guard < (1 << 16); fwd = L.prev_vertex_he(fwd), ++guard) ++valence;
-            guard = 0;
-            for (bwd = L.next_vertex_he(h); fwd < 0 && bwd >= 0 && bwd != h && guard < (1 << 16); bwd = L.next_vertex_he(bwd), ++guard) ++valence;
-            const float w = fdiv(1.0f, (float)valence);
-            const float ws = fmul(w, fwd < 0 ? 0.0f : 1.0f);
+            const float w = frcp(vpre);
+            const float ws = fmul(w, bnd ? 0.0f : 1.0f);
             s.x = fmul(w, fadd(p.x, fmul(ws, fsub(fsub(fmul(4.0f, Eh.x), Fh.x), fmul(3.0f, p.x)))));
             s.y = fmul(w, fadd(p.y, fmul(ws, fsub(fsub(fmul(4.0f, Eh.y), Fh.y), fmul(3.0f, p.y)))));
             s.z = fmul(w, fadd(p.z, fmul(ws, fsub(fsub(fmul(4.0f, Eh.z), Fh.z), fmul(3.0f, p.z)))));
@@ -305,9 +335,7 @@ template <int RW>
 static QuadView<RW> quad_view_l(const Ctx& c, int d) {
     QuadView<RW> L;
     const Level& lv = c.lv[d];
-    L.t.he = c.cage->he; L.t.v2h = c.cage->v2h; L.t.e2h = c.cage->e2h; L.t.f2h = c.cage->f2h;
-    L.t.uvs = c.cage->uvs;
-    L.t.n.V = c.cage->V; L.t.n.F = c.cage->F; L.t.n.E = c.cage->E; L.t.n.H = c.cage->H;
+    L.t = make_cage_tables(*c.cage);
     L.he = c.he + (int64_t)RW * lv.heOff;
     L.cr = c.cr + lv.crOff;
     L.V = lv.V; L.F = lv.F; L.E = lv.E; L.H = lv.H; L.C = lv.C;
