@@ -11,21 +11,26 @@
 //        cp.async.bulk store (TMA engine, no multicast);
 //      - face point of its face (lanes' vertex points combined by shuffles,
 //        in halfedge order), stored by the face's first lane;
+//      - edge point of its edge, computed and stored by the pair's larger
+//        halfedge: both halves of the edge rule, the twin face's point
+//        rebuilt from the twin quad's four records (the same value, bit for
+//        bit, as the twin quad's lanes store);
 //      - clears the vertex slots the atomics of kernel B accumulate into;
 //      - extra blocks refine the creases of the level.
 //   B  (one thread per halfedge)
-//      - edge point: both halves of the edge rule (its own face point is
-//        rebuilt from the quad's lanes, the twin face's point is read from
-//        kernel A's output); the pair's larger halfedge stores it;
-//      - vertex point share (ring walk for valence / crease statistics),
-//        summed across lanes of the warp that hit the same vertex, one float
-//        atomic per vertex and warp.
+//      - vertex point share of its halfedge: face and edge points come from
+//        kernel A's output, the ring statistics from the known structure of
+//        refined levels (face centres and edge midpoints need no walk);
+//      - shares of the same vertex are summed inside the warp where the
+//        structure puts them together (a face centre's 4 shares: plain
+//        store, no atomic; an edge midpoint's 2 shares per side: one atomic
+//        triple), other shares go to memory with one float atomic triple.
 //
 // Both kernels evaluate every float expression in the reference's order, so
 // topology, creases, UVs, face and edge points are bit-identical to the
 // reference; vertex points differ only by the order of the atomic sums.
 //
-// Twin relation used by B: for a twin pair (h, t), vertex(t) = vertex(next h)
+// Twin relation used by A: for a twin pair (h, t), vertex(t) = vertex(next h)
 // and vertex(next t) = vertex(h).  The C ABI checks this on the cage (it is
 // then preserved by every refinement step) and uses the unfused kernels for
 // cages that break it.
@@ -72,6 +77,10 @@ __device__ __forceinline__ f3 shfl3(f3 v, int src) {
     return f3{__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src),
               __shfl_sync(0xffffffffu, v.z, src)};
 }
+__device__ __forceinline__ f3 shfl_xor3(f3 v, int m) {
+    return f3{__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m),
+              __shfl_xor_sync(0xffffffffu, v.z, m)};
+}
 
 // Face point of the quad held by lanes qb..qb+3, in halfedge order:
 // ((0 + p0/4) + p1/4) + p2/4) + p3/4   (CatmullClark.h:2032-2052)
@@ -80,6 +89,19 @@ __device__ __forceinline__ f3 quad_face_point(f3 p, int qb) {
 #pragma unroll
     for (int i = 0; i < 4; ++i) acc = add3(acc, quarter3(shfl3(p, qb + i)));
     return acc;
+}
+
+// One halfedge's share of its edge point: v0 = its vertex, v1 = the next
+// vertex, F = its face point (creased rule :2194-2241, plain rule :2107-2139).
+template <bool CREASED>
+__device__ __forceinline__ f3 edge_share(f3 v0, f3 v1, f3 F, bool boundary, float w) {
+    if (CREASED) {
+        const f3 sharpP = mul3(lerp3(v0, v1, 0.5f), boundary ? 1.0f : 0.5f);
+        const f3 smoothP = mul3(lerp3(v0, F, 0.5f), 0.5f);
+        return lerp3(smoothP, sharpP, w);
+    }
+    const float wh = boundary ? 1.0f : 0.5f;
+    return lerp3(mul3(F, 0.5f), lerp3(mul3(v0, wh), mul3(v1, wh), 0.5f), wh);
 }
 
 struct LevelArgs {
@@ -96,7 +118,7 @@ struct LevelArgs {
 // ---------------------------------------------------------------------------
 // kernel A
 // ---------------------------------------------------------------------------
-template <int RW, bool TOPO, bool UV, bool PTS>
+template <int RW, bool TOPO, bool UV, bool PTS, bool CREASED>
 __global__ void __launch_bounds__(kBlockL)
 k_level_a(LevelArgs a) {
     const int nbH = (a.H + kBlockL - 1) / kBlockL;
@@ -174,8 +196,30 @@ k_level_a(LevelArgs a) {
     if (PTS) {
         const f3 p = valid ? ld3(a.pin + 3 * (int64_t)vx) : zero3();
         const f3 Fp = quad_face_point(p, qb);
+        const f3 pn = shfl3(p, ln);
         if (valid && k == 0) st3(a.pout + 3 * ((int64_t)a.V + f), Fp);
         if (a.zeroV && h64 < a.V) st3(a.pout + 3 * h64, zero3());
+        // edge point, by the pair's larger halfedge; the smaller one's share
+        // is added first, as a one-thread reference run adds it
+        if (valid && h > tw) {
+            const float w = CREASED ? fsat(ed < a.C ? a.crIn[ed].sharpness : 0.0f) : 0.0f;
+            const f3 sh_h = edge_share<CREASED>(p, pn, Fp, tw < 0, w);
+            f3 E;
+            if (tw >= 0) {
+                const int32_t tb = tw & ~3;
+                f3 Ft = zero3();
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int32_t tv = __ldg(a.in + (int64_t)RW * (tb + i) + 2);
+                    Ft = add3(Ft, quarter3(ld3(a.pin + 3 * (int64_t)tv)));
+                }
+                const f3 sh_t = edge_share<CREASED>(pn, p, Ft, false, w);
+                E = add3(add3(zero3(), sh_t), sh_h);
+            } else {
+                E = add3(zero3(), sh_h);
+            }
+            st3(a.pout + 3 * ((int64_t)a.V + a.F + ed), E);
+        }
     }
     if (TOPO) {
         __syncthreads();
@@ -190,16 +234,25 @@ k_level_a(LevelArgs a) {
 // ---------------------------------------------------------------------------
 // kernel B
 // ---------------------------------------------------------------------------
-template <int RW, bool CREASED, bool VERTEX>
+__device__ __forceinline__ void atomic_add3(float* o, f3 v) {
+    atomicAdd(o + 0, v.x);
+    atomicAdd(o + 1, v.y);
+    atomicAdd(o + 2, v.z);
+}
+
+// STRUCT: depth >= 2, where a 16-lane group holds the 16 children of one
+// parent quad face, so a face centre's 4 shares sit in lanes 2, 6, 10, 14 and
+// an edge midpoint's shares from this face in lanes 4j+1 and 4(j+1 mod 4)+3.
+template <int RW, bool CREASED, bool STRUCT>
 __global__ void __launch_bounds__(kBlockL)
 k_level_b(QuadView<RW> L, const float* __restrict__ pin, float* __restrict__ pout) {
     const int tid = threadIdx.x, lane = tid & 31;
     const int64_t h64 = (int64_t)blockIdx.x * kBlockL + tid;
     const bool valid = h64 < L.H;
     const int32_t h = (int32_t)h64;
-    const int k = lane & 3, qb = lane & ~3;
+    const int k = lane & 3, qb = lane & ~3, lp = qb | ((k + 3) & 3);
     const float* fpt = pout + 3 * (int64_t)L.V;
-    float* ept = pout + 3 * ((int64_t)L.V + L.F);
+    const float* ept = pout + 3 * ((int64_t)L.V + L.F);
     int32_t tw = -1, ed = 0, vx = 0;
     if (valid) {
         if constexpr (RW == 4) {
@@ -211,46 +264,17 @@ k_level_b(QuadView<RW> L, const float* __restrict__ pin, float* __restrict__ pou
             vx = __ldg(L.he + 3 * h64 + 2);
         }
     }
-    const f3 p = valid ? ld3(pin + 3 * (int64_t)vx) : zero3();
-    const f3 Fh = quad_face_point(p, qb);
-    const f3 pn = shfl3(p, qb | ((k + 1) & 3));
-    // ---- edge point ---------------------------------------------------------
-    f3 Eh = zero3();
+    f3 p = zero3(), Fh = zero3(), Eh = zero3();
     if (valid) {
-        f3 sh_h, sh_t = zero3();
-        if (CREASED) {
-            const float w = fsat(L.sharp(ed));
-            const f3 sharpP = mul3(lerp3(p, pn, 0.5f), tw < 0 ? 1.0f : 0.5f);
-            const f3 smoothP = mul3(lerp3(p, Fh, 0.5f), 0.5f);
-            sh_h = lerp3(smoothP, sharpP, w);
-            if (tw >= 0) {
-                const f3 Ft = ld3(fpt + 3 * (int64_t)(tw >> 2));
-                const f3 sharpT = mul3(lerp3(pn, p, 0.5f), 0.5f);
-                const f3 smoothT = mul3(lerp3(pn, Ft, 0.5f), 0.5f);
-                sh_t = lerp3(smoothT, sharpT, w);
-            }
-        } else {
-            const float wh = tw >= 0 ? 0.5f : 1.0f;
-            sh_h = lerp3(mul3(Fh, 0.5f), lerp3(mul3(p, wh), mul3(pn, wh), 0.5f), wh);
-            if (tw >= 0) {
-                const f3 Ft = ld3(fpt + 3 * (int64_t)(tw >> 2));
-                sh_t = lerp3(mul3(Ft, 0.5f), lerp3(mul3(pn, 0.5f), mul3(p, 0.5f), 0.5f), 0.5f);
-            }
-        }
-        if (tw < 0) Eh = add3(zero3(), sh_h);
-        else if (h > tw) Eh = add3(add3(zero3(), sh_t), sh_h);   // lower halfedge ID first
-        else Eh = add3(add3(zero3(), sh_h), sh_t);
-        if (h > tw) st3(ept + 3 * (int64_t)ed, Eh);
+        p = ld3(pin + 3 * (int64_t)vx);
+        Fh = ld3(fpt + 3 * (int64_t)(h >> 2));
+        Eh = ld3(ept + 3 * (int64_t)ed);
     }
-    if (!VERTEX) return;
-    // ---- vertex point share ---------------------------------------------------
-    const f3 Ep = shfl3(Eh, qb | ((k + 3) & 3));     // edge point of prev(h)
-    const int32_t ped = __shfl_sync(0xffffffffu, ed, qb | ((k + 3) & 3));
-    const int32_t ptw = __shfl_sync(0xffffffffu, tw, qb | ((k + 3) & 3));
-    int32_t key = -1 - lane;
+    const f3 Ep = shfl3(Eh, lp);                         // edge point of prev(h)
+    const int32_t ped = __shfl_sync(0xffffffffu, ed, lp);
+    const int32_t ptw = __shfl_sync(0xffffffffu, tw, lp);
     f3 s = zero3();
     if (valid) {
-        key = vx;
         // Ring statistics of vertex(h) as the reference's walk from h finds
         // them (:2523-2566).  At a refined level the vertex of child k of a
         // parent halfedge is known: k = 2 is a face centre (valence = parent
@@ -264,18 +288,14 @@ k_level_b(QuadView<RW> L, const float* __restrict__ pin, float* __restrict__ pou
         if (k == 2) {
             vpre = L.d == 1 ? (float)L.t.fsz[L.t.he[(int64_t)CH_WORDS * (h >> 2) + CH_FACE]] : 4.0f;
             cpre = 0.0f; avgS = 0.0f; bnd = false;
-        } else if (k == 1) {
-            const float sa = L.sharp(ped), sb = L.sharp(ped ^ 1);
-            bnd = ptw < 0;
+        } else if (k != 0) {
+            const int32_t eh = k == 1 ? ped : ed;        // one half of the parent edge
+            const float sa = L.sharp(eh), sb = L.sharp(eh ^ 1);
+            bnd = (k == 1 ? ptw : tw) < 0;
             vpre = bnd ? 2.0f : 4.0f;
-            avgS = fadd(sa, sb);
-            cpre = fadd(fsign(sa), fsign(sb));
-        } else if (k == 3) {
-            const float sa = L.sharp(ed), sb = L.sharp(ed ^ 1);
-            bnd = tw < 0;
-            vpre = bnd ? 2.0f : 4.0f;
-            avgS = bnd ? sb : fadd(sa, sb);
-            cpre = bnd ? fsign(sb) : fadd(fsign(sa), fsign(sb));
+            const bool own = k == 3;                     // the walk from h skips its own edge
+            avgS = (bnd && own) ? sb : fadd(sa, sb);
+            cpre = (bnd && own) ? fsign(sb) : fadd(fsign(sa), fsign(sb));
         } else if (CREASED) {
             const RingStats r = creased_ring(L, h);
             vpre = r.valence; cpre = r.creaseCount; avgS = r.avgS; bnd = r.fwd < 0;
@@ -287,22 +307,24 @@ k_level_b(QuadView<RW> L, const float* __restrict__ pin, float* __restrict__ pou
             vpre = (float)valence; cpre = 0.0f; avgS = 0.0f; bnd = fwd < 0;
         }
         if (CREASED) {
+            // vertex rule, corner-first branch order of quad levels (:2567-2607)
             const float cw = fsign(L.sharp(ed)), pcw = fsign(L.sharp(ped));
-            float valence = vpre, creaseCount = cpre;
-            const f3 corner = mul3(p, frcp(valence));
-            f3 crease = add3(mul3(p, fmul(0.25f, cw)), mul3(Eh, fmul(0.25f, cw)));
-            f3 smooth = add3(mul3(Fh, -1.0f), mul3(Eh, 4.0f));
-            smooth = add3(smooth, mul3(p, fsub(valence, 3.0f)));
-            smooth = mul3(smooth, frcp(fmul(valence, valence)));
-            if (bnd) {
-                creaseCount = fadd(creaseCount, cw);
-                valence = fadd(valence, 1.0f);
-                crease = add3(crease, add3(mul3(p, fmul(0.25f, pcw)), mul3(Ep, fmul(0.25f, pcw))));
+            const float valence = bnd ? fadd(vpre, 1.0f) : vpre;
+            const float creaseCount = bnd ? fadd(cpre, cw) : cpre;
+            if (creaseCount >= 3.0f || valence == 2.0f) {
+                s = mul3(p, frcp(vpre));
+            } else if (creaseCount <= 1.0f) {
+                f3 smooth = add3(mul3(Fh, -1.0f), mul3(Eh, 4.0f));
+                smooth = add3(smooth, mul3(p, fsub(vpre, 3.0f)));
+                s = mul3(smooth, frcp(fmul(vpre, vpre)));
+            } else {
+                const f3 corner = mul3(p, frcp(vpre));
+                f3 crease = add3(mul3(p, fmul(0.25f, cw)), mul3(Eh, fmul(0.25f, cw)));
+                if (bnd) crease = add3(crease, add3(mul3(p, fmul(0.25f, pcw)), mul3(Ep, fmul(0.25f, pcw))));
+                s = lerp3(corner, crease, fsat(fmul(avgS, 0.5f)));
             }
-            if (creaseCount >= 3.0f || valence == 2.0f) s = corner;
-            else if (creaseCount <= 1.0f) s = smooth;
-            else s = lerp3(corner, crease, fsat(fmul(avgS, 0.5f)));
         } else {
+            // crease-free vertex rule (:2307-2351)
             const float w = frcp(vpre);
             const float ws = fmul(w, bnd ? 0.0f : 1.0f);
             s.x = fmul(w, fadd(p.x, fmul(ws, fsub(fsub(fmul(4.0f, Eh.x), Fh.x), fmul(3.0f, p.x)))));
@@ -310,21 +332,23 @@ k_level_b(QuadView<RW> L, const float* __restrict__ pin, float* __restrict__ pou
             s.z = fmul(w, fadd(p.z, fmul(ws, fsub(fsub(fmul(4.0f, Eh.z), Fh.z), fmul(3.0f, p.z)))));
         }
     }
-    const unsigned full = 0xffffffffu;
-    const unsigned grp = __match_any_sync(full, key);
-    const int n = __popc(grp);
-    const int maxn = (int)__reduce_max_sync(full, (unsigned)n);
-    f3 acc = zero3();
-    for (int i = 0; i < maxn; ++i) {
-        const int src = i < n ? (int)__fns(grp, 0, i + 1) : lane;
-        const f3 t = shfl3(s, src);
-        if (i < n) acc = add3(acc, t);
-    }
-    if (valid && lane == __ffs(grp) - 1) {
-        float* o = pout + 3 * (int64_t)vx;
-        atomicAdd(o + 0, acc.x);
-        atomicAdd(o + 1, acc.y);
-        atomicAdd(o + 2, acc.z);
+    float* o = pout + 3 * (int64_t)vx;
+    if (STRUCT) {
+        const f3 u = add3(s, shfl_xor3(s, 4));
+        const f3 fsum = add3(u, shfl_xor3(u, 8));       // (s2 + s6) + (s10 + s14)
+        const int partner = (lane & ~15) | ((((lane >> 2) + 1) & 3) << 2) | 3;
+        const f3 pe = shfl3(s, partner);
+        if (valid) {
+            if (k == 2) {
+                if ((lane & 15) == 2) st3(o, fsum);     // all 4 shares of this vertex
+            } else if (k == 1) {
+                atomic_add3(o, add3(s, pe));
+            } else if (k == 0) {
+                atomic_add3(o, s);
+            }
+        }
+    } else if (valid) {
+        atomic_add3(o, s);
     }
 }
 
@@ -343,7 +367,7 @@ static QuadView<RW> quad_view_l(const Ctx& c, int d) {
     return L;
 }
 
-template <int RW>
+template <int RW, bool CREASED>
 static void level_a(const Ctx& c, int d, bool topo, bool uv, const float* pin, float* pout, bool zeroV) {
     const Level& lv = c.lv[d];
     LevelArgs a;
@@ -358,55 +382,52 @@ static void level_a(const Ctx& c, int d, bool topo, bool uv, const float* pin, f
     const unsigned nb = nblocksL(lv.H) + (topo ? nblocksL(lv.C) : 0u);
     c.prof->begin(c.stream, topo ? CCS_K_LEVEL_FUSED : CCS_K_FACE_POINTS, d, lv.H);
     if (topo) {
-        if (RW == 4 && uv) k_level_a<RW, true, true, true><<<nb, kBlockL, 0, c.stream>>>(a);
-        else k_level_a<RW, true, false, true><<<nb, kBlockL, 0, c.stream>>>(a);
+        if (RW == 4 && uv) k_level_a<RW, true, true, true, CREASED><<<nb, kBlockL, 0, c.stream>>>(a);
+        else k_level_a<RW, true, false, true, CREASED><<<nb, kBlockL, 0, c.stream>>>(a);
     } else {
-        k_level_a<RW, false, false, true><<<nb, kBlockL, 0, c.stream>>>(a);
+        k_level_a<RW, false, false, true, CREASED><<<nb, kBlockL, 0, c.stream>>>(a);
     }
     c.prof->end(c.stream);
 }
 
-template <int RW>
-static void level_b(const Ctx& c, int d, bool creased, bool vertex, const float* pin, float* pout) {
+template <int RW, bool CREASED>
+static void level_b(const Ctx& c, int d, const float* pin, float* pout) {
     const QuadView<RW> L = quad_view_l<RW>(c, d);
-    c.prof->begin(c.stream, vertex ? CCS_K_LEVEL_POINTS : CCS_K_EDGE_POINTS, d, L.H);
+    c.prof->begin(c.stream, CCS_K_LEVEL_POINTS, d, L.H);
     const unsigned nb = nblocksL(L.H);
-    if (creased) {
-        if (vertex) k_level_b<RW, true, true><<<nb, kBlockL, 0, c.stream>>>(L, pin, pout);
-        else k_level_b<RW, true, false><<<nb, kBlockL, 0, c.stream>>>(L, pin, pout);
-    } else {
-        if (vertex) k_level_b<RW, false, true><<<nb, kBlockL, 0, c.stream>>>(L, pin, pout);
-        else k_level_b<RW, false, false><<<nb, kBlockL, 0, c.stream>>>(L, pin, pout);
-    }
+    if (d >= 2) k_level_b<RW, CREASED, true><<<nb, kBlockL, 0, c.stream>>>(L, pin, pout);
+    else k_level_b<RW, CREASED, false><<<nb, kBlockL, 0, c.stream>>>(L, pin, pout);
     c.prof->end(c.stream);
 }
 
 // Declared in ccs_forward.cu: the vertex pass of one quad level when the
-// fixed-order (deterministic) sum is requested.
+// fixed-order (deterministic) sum is requested, and the cage step.
 cudaError_t run_vertex_det_level(const Ctx& c, int d, const float* pin, float* pout, bool creased);
 cudaError_t run_cage_step(const Ctx& c, bool topo, bool uv, const float* cagePts, float* pout, int mode, bool det);
+
+template <int RW, bool CREASED>
+static cudaError_t fused_levels(const Ctx& c, bool topo, bool uv, float* pts, bool det) {
+    for (int d = 1; d < c.D; ++d) {
+        const float* pin = pts + 3 * c.lv[d].ptOff;
+        float* pout = pts + 3 * c.lv[d + 1].ptOff;
+        level_a<RW, CREASED>(c, d, topo, uv, pin, pout, !det);
+        if (det) {
+            const cudaError_t e = run_vertex_det_level(c, d, pin, pout, CREASED);
+            if (e != cudaSuccess) return e;
+        } else {
+            level_b<RW, CREASED>(c, d, pin, pout);
+        }
+    }
+    return cudaGetLastError();
+}
 
 cudaError_t run_fused(const Ctx& c, bool topo, const float* cagePts, float* pts, int mode, bool det) {
     const bool creased = mode == CCS_POINTS_SCATTER;
     const bool uv = c.cage->U > 0 && c.rw == 4;
     cudaError_t e = run_cage_step(c, topo, uv, cagePts, pts + 3 * c.lv[1].ptOff, mode, det);
     if (e != cudaSuccess) return e;
-    for (int d = 1; d < c.D; ++d) {
-        const float* pin = pts + 3 * c.lv[d].ptOff;
-        float* pout = pts + 3 * c.lv[d + 1].ptOff;
-        if (c.rw == 4) {
-            level_a<4>(c, d, topo, uv, pin, pout, !det);
-            level_b<4>(c, d, creased, !det, pin, pout);
-        } else {
-            level_a<3>(c, d, topo, false, pin, pout, !det);
-            level_b<3>(c, d, creased, !det, pin, pout);
-        }
-        if (det) {
-            e = run_vertex_det_level(c, d, pin, pout, creased);
-            if (e != cudaSuccess) return e;
-        }
-    }
-    return cudaGetLastError();
+    if (c.rw == 4) return creased ? fused_levels<4, true>(c, topo, uv, pts, det) : fused_levels<4, false>(c, topo, uv, pts, det);
+    return creased ? fused_levels<3, true>(c, topo, false, pts, det) : fused_levels<3, false>(c, topo, false, pts, det);
 }
 
 }  // namespace ccs
