@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(PKG, "lib", "libccs_cuda.so")
 CCS_OK = 0
 STATUS = {
     0: "CCS_OK", -1: "CCS_ERR_ARG", -2: "CCS_ERR_ALLOC", -3: "CCS_ERR_OVERFLOW", -4: "CCS_ERR_CUDA",
-    -5: "CCS_ERR_TIMEOUT", -6: "CCS_ERR_STATE", -7: "CCS_ERR_UNSUPPORTED",
+    -5: "CCS_ERR_TIMEOUT", -6: "CCS_ERR_STATE", -7: "CCS_ERR_UNSUPPORTED", -8: "CCS_ERR_SCRATCH_LIMIT",
 }
 FLAG_NO_UV = 1 << 0
 FLAG_PAGEABLE_HOST = 1 << 1
@@ -82,6 +82,7 @@ SIGNATURES = {
     "ccs_GetDeviceArrays_cuda": ([_P, ctypes.POINTER(DeviceArrays)], _I),
     "ccs_RefinePointsDevice_cuda": ([_P, _P, _P, _I, _P], _I),
     "ccs_AdjointPointsDevice_cuda": ([_P, _P, _P, _P], _I),
+    "ccs_AdjointPointsDeviceNoAlloc_cuda": ([_P, _P, _P, _P], _I),
     "ccs_LevelCounts_cuda": ([_P, ctypes.c_int32, ctypes.POINTER(LevelCounts)], _I),
     "ccs_MaxSupportedDepth_cuda": ([_P], ctypes.c_int32),
     "ccs_SetProfiling_cuda": ([_P, _I], _I),

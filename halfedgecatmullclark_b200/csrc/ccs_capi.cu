@@ -399,6 +399,21 @@ static int refine_op(cc_Subd* subd, int mode) {
     return ret(st);
 }
 
+// Adjoint over a caller-provided work buffer (`workFloats` floats); used by
+// the allocation-free entry point in ccs_noalloc.cu.
+int adjoint_into(const cc_Subd* subd, const float* gradPoints, float* gradCage, float* work, int64_t workFloats,
+                 cudaStream_t stream) {
+    SubdImpl* s = find(subd);
+    if (!s || !gradPoints || !gradCage || !work) return CCS_ERR_ARG;
+    if (!s->topo_ready || !s->creases_ready) return CCS_ERR_STATE;
+    if (3 * s->cumV > workFloats) return CCS_ERR_SCRATCH_LIMIT;
+    DeviceGuard g(s->device);
+    Ctx c = s->ctx(stream);
+    return run_adjoint(c, gradPoints, work, gradCage, s->cumV) == cudaSuccess ? CCS_OK : CCS_ERR_CUDA;
+}
+
+int set_last_error(int status) { return ret(status); }
+
 }  // namespace ccs
 
 using namespace ccs;
@@ -637,6 +652,7 @@ const char* ccs_ErrorString_cuda(int status) {
         case CCS_ERR_TIMEOUT: return "bounded device wait timed out";
         case CCS_ERR_STATE: return "topology not refined yet";
         case CCS_ERR_UNSUPPORTED: return "unsupported for this subd layout";
+        case CCS_ERR_SCRATCH_LIMIT: return "the subd's points exceed the static scratch of the allocation-free adjoint";
         default: return "unknown status";
     }
 }

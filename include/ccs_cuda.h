@@ -86,7 +86,8 @@ enum {
     CCS_ERR_CUDA = -4,         /* a CUDA call failed                      */
     CCS_ERR_TIMEOUT = -5,      /* a bounded device wait gave up           */
     CCS_ERR_STATE = -6,        /* call order (e.g. points before topology) */
-    CCS_ERR_UNSUPPORTED = -7   /* option not available for this layout     */
+    CCS_ERR_UNSUPPORTED = -7,  /* option not available for this layout     */
+    CCS_ERR_SCRATCH_LIMIT = -8 /* problem larger than a fixed scratch area */
 };
 
 /* Flags for ccs_CreateEx_cuda / ccs_SetFlags_cuda. */
@@ -186,6 +187,32 @@ int ccs_RefinePointsDevice_cuda(cc_Subd *subd, const float *cagePoints, float *p
  * of cumV x 3 floats that the library allocates on first use and keeps. */
 int ccs_AdjointPointsDevice_cuda(cc_Subd *subd, const float *gradPoints, float *gradCage,
                                  void *stream);
+
+/* ccs_AdjointPointsDevice_cuda for callers that must not allocate GPU memory.
+ * No counterpart in the reference (which has no adjoint).
+ *
+ * ccs_AdjointPointsDevice_cuda allocates its working buffer with cudaMalloc
+ * on first use.  Some callers cannot allow that: code that is recording a
+ * CUDA graph through stream capture (cudaMalloc is not allowed while a
+ * stream is being captured), applications whose device memory is owned by
+ * their own pool allocator (PyTorch's caching allocator, a renderer's arena)
+ * and would be fragmented or overcommitted by allocations behind their
+ * back, and real-time loops that forbid allocation after start-up.  This
+ * entry point allocates nothing: its working buffer is a fixed array of
+ * 16 MiB (4,194,304 floats) compiled into the library, which every GPU that
+ * loads the library holds until the process exits.  It therefore accepts
+ * subds whose refined points fit: 3 * (total refined points) <= 4,194,304,
+ * i.e. at most 1,398,101 points over all levels; larger subds are refused
+ * with CCS_ERR_SCRATCH_LIMIT.  The caller passes the inputs and outputs as
+ * for ccs_AdjointPointsDevice_cuda; the results are identical.
+ *
+ * The first call on a device looks up that device's address of the array
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls share the one array, so calls whose work can overlap on the GPU
+ * (different streams, or different host threads) race and must be
+ * serialised by the caller. */
+int ccs_AdjointPointsDeviceNoAlloc_cuda(cc_Subd *subd, const float *gradPoints, float *gradCage,
+                                        void *stream);
 
 /* ---------------------------------------------------------------------- */
 /* Counts (int64, with the int32 overflow check the library applies)       */
