@@ -50,6 +50,23 @@ class LevelCounts(ctypes.Structure):
                 ("cumH", ctypes.c_int64), ("cumC", ctypes.c_int64), ("cumV", ctypes.c_int64)]
 
 
+class BatchArrays(ctypes.Structure):
+    _fields_ = [("halfedges", ctypes.c_void_p), ("creases", ctypes.c_void_p), ("points", ctypes.c_void_p),
+                ("cagePoints", ctypes.c_void_p), ("gradPoints", ctypes.c_void_p),
+                ("gradCagePoints", ctypes.c_void_p), ("halfedgeCount", ctypes.c_int64),
+                ("creaseCount", ctypes.c_int64), ("pointCount", ctypes.c_int64),
+                ("cagePointCount", ctypes.c_int64)]
+
+
+class BatchCageInfo(ctypes.Structure):
+    _fields_ = [("depth", ctypes.c_int32), ("cagePointOffset", ctypes.c_int64),
+                ("cagePointCount", ctypes.c_int64), ("halfedgeOffset", ctypes.c_int64),
+                ("halfedgeCount", ctypes.c_int64), ("creaseOffset", ctypes.c_int64),
+                ("creaseCount", ctypes.c_int64), ("pointOffset", ctypes.c_int64),
+                ("pointCount", ctypes.c_int64), ("finestPointOffset", ctypes.c_int64),
+                ("finestPointCount", ctypes.c_int64)]
+
+
 class KernelTime(ctypes.Structure):
     _fields_ = [("kernel", ctypes.c_int32), ("level", ctypes.c_int32), ("ms", ctypes.c_float),
                 ("units", ctypes.c_int64)]
@@ -83,6 +100,18 @@ SIGNATURES = {
     "ccs_RefinePointsDevice_cuda": ([_P, _P, _P, _I, _P], _I),
     "ccs_AdjointPointsDevice_cuda": ([_P, _P, _P, _P], _I),
     "ccs_AdjointPointsDeviceNoAlloc_cuda": ([_P, _P, _P, _P], _I),
+    "ccs_BatchCreate_cuda": ([_P, _P, ctypes.c_int32, _U, ctypes.POINTER(_P)], _I),
+    "ccs_BatchRelease_cuda": ([_P], None),
+    "ccs_BatchRefine_cuda": ([_P, _I], _I),
+    "ccs_BatchRefinePoints_cuda": ([_P, _I], _I),
+    "ccs_BatchAdjointPoints_cuda": ([_P], _I),
+    "ccs_BatchGetArrays_cuda": ([_P, ctypes.POINTER(BatchArrays)], _I),
+    "ccs_BatchCageInfo_cuda": ([_P, ctypes.c_int32, ctypes.POINTER(BatchCageInfo)], _I),
+    "ccs_BatchSetStream_cuda": ([_P, _P], _I),
+    "ccs_BatchSetSchedule_cuda": ([_P, ctypes.c_int32], _I),
+    "ccs_BatchSynchronize_cuda": ([_P], _I),
+    "ccs_BatchDownload_cuda": ([_P, ctypes.c_int32, _P], _I),
+    "ccs_BarrierTimeoutSelfTest_cuda": ([], _I),
     "ccs_LevelCounts_cuda": ([_P, ctypes.c_int32, ctypes.POINTER(LevelCounts)], _I),
     "ccs_MaxSupportedDepth_cuda": ([_P], ctypes.c_int32),
     "ccs_SetProfiling_cuda": ([_P, _I], _I),

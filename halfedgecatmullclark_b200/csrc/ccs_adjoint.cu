@@ -26,170 +26,32 @@
 // Levels run deepest first; only the level offsets are needed (no state is
 // saved by the forward pass).
 #include "ccs_host.h"
-#include "ccs_internal.cuh"
+#include "ccs_tiles.cuh"
 
 namespace ccs {
 
 static constexpr int kBlockA = 256;
-static constexpr int kRingCapA = 1 << 16;
 static inline unsigned nblocksA(int64_t n) { return (unsigned)((n + kBlockA - 1) / kBlockA); }
 
-struct VCoef {
-    float a, bF, cE, dE;
-};
-
-// Coefficients of halfedge h's vertex share (linearisation of
-// creased_vertex_share; :1872-1991 and :2496-2615).
-template <class View>
-__device__ __forceinline__ VCoef vertex_coef(const View& L, int32_t h) {
-    const RingStats r = creased_ring(L, h);
-    const int32_t prev = L.prev(h);
-    const float cw = fsign(L.hsharp(h)), pcw = fsign(L.hsharp(prev));
-    const float vp = r.valence;
-    const bool bnd = r.fwd < 0;
-    const float valence = bnd ? vp + 1.0f : vp;
-    const float creaseCount = bnd ? r.creaseCount + cw : r.creaseCount;
-    int branch;  // 0 corner, 1 smooth, 2 blend
-    if (View::kQuad) {
-        if (creaseCount >= 3.0f || valence == 2.0f) branch = 0;
-        else if (creaseCount <= 1.0f) branch = 1;
-        else branch = 2;
-    } else {
-        if (creaseCount <= 1.0f) branch = 1;
-        else if (creaseCount >= 3.0f || valence == 2.0f) branch = 0;
-        else branch = 2;
-    }
-    VCoef k{0.0f, 0.0f, 0.0f, 0.0f};
-    if (branch == 0) {
-        k.a = 1.0f / vp;
-    } else if (branch == 1) {
-        const float inv = 1.0f / (vp * vp);
-        k.a = (vp - 3.0f) * inv;
-        k.bF = -inv;
-        k.cE = 4.0f * inv;
-    } else {
-        const float t = fsat(r.avgS * 0.5f);
-        k.a = (1.0f - t) / vp + t * 0.25f * (cw + (bnd ? pcw : 0.0f));
-        k.cE = t * 0.25f * cw;
-        k.dE = bnd ? t * 0.25f * pcw : 0.0f;
-    }
-    return k;
-}
-
-struct ECoef {
-    float al, be, ga;
-};
-// Coefficients of halfedge h's edge share (:1602-1648, :2194-2241)
-template <class View>
-__device__ __forceinline__ ECoef edge_coef(const View& L, int32_t h) {
-    const float w = fsat(L.sharp(L.edge(h)));
-    const float b = L.twin(h) < 0 ? 1.0f : 0.5f;
-    ECoef k;
-    k.al = (1.0f - w) * 0.25f + w * b * 0.5f;
-    k.be = w * b * 0.5f;
-    k.ga = (1.0f - w) * 0.25f;
-    return k;
-}
-
-template <class View>
-__device__ __forceinline__ int32_t face_size(const View& L, int32_t h) {
-    if (View::kQuad) return 4;
-    int32_t n = 1, guard = 0;
-    for (int32_t it = L.next(h); it != h && guard < kRingCapA; it = L.next(it), ++guard) ++n;
-    return n;
-}
-
-__device__ __forceinline__ void axpy3(f3& acc, float s, const float* p) {
-    acc.x += s * p[0];
-    acc.y += s * p[1];
-    acc.z += s * p[2];
-}
-
-// 1. edge gather: gE[e] += vertex-pass terms
 template <class View>
 __global__ void __launch_bounds__(kBlockA)
 k_adj_edges(View L, float* __restrict__ gNew) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= L.H) return;
-    const int32_t h = (int32_t)i, tw = L.twin(h);
-    if (!(h > tw)) return;
-    const float* gV = gNew;
-    float* gE = gNew + 3 * ((int64_t)L.V + L.F);
-    f3 acc = zero3();
-    const int32_t sides[2] = {h, tw};
-    for (int s = 0; s < (tw >= 0 ? 2 : 1); ++s) {
-        const int32_t x = sides[s], nx = L.next(x);
-        axpy3(acc, vertex_coef(L, x).cE, gV + 3 * (int64_t)L.vert(x));
-        axpy3(acc, vertex_coef(L, nx).dE, gV + 3 * (int64_t)L.vert(nx));
-    }
-    float* o = gE + 3 * (int64_t)L.edge(h);
-    o[0] += acc.x;
-    o[1] += acc.y;
-    o[2] += acc.z;
+    if (i < L.H) adj_edge_item(L, gNew, (int32_t)i);
 }
 
-// 2. face gather: gF[f] += vertex-pass and edge-pass terms
 template <class View>
 __global__ void __launch_bounds__(kBlockA)
 k_adj_faces(View L, float* __restrict__ gNew) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= L.F) return;
-    const int32_t f = (int32_t)i;
-    const float* gV = gNew;
-    float* gF = gNew + 3 * (int64_t)L.V;
-    const float* gE = gNew + 3 * ((int64_t)L.V + L.F);
-    const int32_t h0 = L.face_he(f);
-    f3 acc = zero3();
-    int32_t h = h0;
-    int guard = 0;
-    do {
-        axpy3(acc, vertex_coef(L, h).bF, gV + 3 * (int64_t)L.vert(h));
-        axpy3(acc, edge_coef(L, h).ga, gE + 3 * (int64_t)L.edge(h));
-        h = L.next(h);
-    } while (h != h0 && ++guard < kRingCapA);
-    float* o = gF + 3 * (int64_t)f;
-    o[0] += acc.x;
-    o[1] += acc.y;
-    o[2] += acc.z;
-}
-
-// 3. vertex gather: gOld[v] += all terms that read P[v]
-template <class View>
-__device__ __forceinline__ void adj_vertex_term(const View& L, int32_t x, const float* gVv, const float* gF,
-                                                const float* gE, f3& acc) {
-    axpy3(acc, vertex_coef(L, x).a, gVv);
-    axpy3(acc, edge_coef(L, x).al, gE + 3 * (int64_t)L.edge(x));
-    axpy3(acc, 1.0f / (float)face_size(L, x), gF + 3 * (int64_t)L.face(x));
-    const int32_t p = L.prev(x);
-    axpy3(acc, edge_coef(L, p).be, gE + 3 * (int64_t)L.edge(p));
+    if (i < L.F) adj_face_item(L, gNew, (int32_t)i);
 }
 
 template <class View>
 __global__ void __launch_bounds__(kBlockA)
 k_adj_vertices(View L, const float* __restrict__ gNew, float* __restrict__ gOld) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= L.V) return;
-    const int32_t v = (int32_t)i;
-    const float* gVv = gNew + 3 * (int64_t)v;
-    const float* gF = gNew + 3 * (int64_t)L.V;
-    const float* gE = gNew + 3 * ((int64_t)L.V + L.F);
-    const int32_t h0 = L.vert_he(v);
-    f3 acc = zero3();
-    int32_t it = h0;
-    int n = 0;
-    do {
-        adj_vertex_term(L, it, gVv, gF, gE, acc);
-        it = L.prev_vertex_he(it);
-    } while (it >= 0 && it != h0 && ++n < kRingCapA);
-    if (it < 0) {
-        n = 0;
-        for (it = L.next_vertex_he(h0); it >= 0 && it != h0 && n < kRingCapA; it = L.next_vertex_he(it), ++n)
-            adj_vertex_term(L, it, gVv, gF, gE, acc);
-    }
-    float* o = gOld + 3 * (int64_t)v;
-    o[0] += acc.x;
-    o[1] += acc.y;
-    o[2] += acc.z;
+    if (i < L.V) adj_vertex_item(L, gNew, gOld, (int32_t)i);
 }
 
 static CageTables cage_tables_a(const DevCage& c) { return make_cage_tables(c); }

@@ -1,0 +1,695 @@
+// ccs_batch.cu -- many cages of uneven size and depth refined together.
+//
+// Every cage keeps the single-mesh layout (its own packed halfedges, creases
+// and points), placed one after the other in batch-wide buffers.  Work is
+// cut into tiles of 256 items that never span two cages (so the lane
+// structure the level kernels rely on -- quads in 4 adjacent lanes, a parent
+// face's 16 children in 16 lanes -- holds in every tile).  For each depth d
+// one persistent kernel covers every cage still active at d: its blocks
+// stride over the tiles of one phase, meet at a grid barrier, and go on
+// with the next phase:
+//
+//   forward, d = 0:  cage topology + creases + face points + clearing,
+//                    | edge points | vertex points (atomics)
+//   forward, d >= 1: kernel A tiles + crease tiles | kernel B tiles
+//   adjoint, each d: edge gathers | face gathers | vertex gathers
+//
+// The tile bodies are the single-mesh ones (ccs_tiles.cuh).  The kernels run
+// as cooperative launches (all blocks resident), and every barrier wait is
+// bounded: a wait that gives up sets an error word, the kernel returns, and
+// the host reports CCS_ERR_TIMEOUT.  A tile -> cage lookup is a binary
+// search over the per-phase tile prefix sums.
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <new>
+#include <vector>
+
+#include "ccs_host.h"
+#include "ccs_tiles.cuh"
+
+namespace ccs {
+
+static constexpr int kBatchBlock = 256;
+static constexpr int kMaxBatchDepth = 10;
+
+enum Phase {
+    PH_CAGE_TOPO = 0,   // 4 H0 child halfedges
+    PH_CAGE_CREASE,     // E0 creases
+    PH_CAGE_FACE,       // F0 faces
+    PH_CAGE_ZERO,       // V0 old-vertex slots of depth 1
+    PH_CAGE_EDGE,       // H0 halfedges
+    PH_CAGE_VERT,       // H0 halfedges
+    PH_A,               // H_d parent halfedges
+    PH_A_CREASE,        // C_d creases
+    PH_B,               // H_d halfedges
+    PH_ADJ_EDGE,        // H_d
+    PH_ADJ_FACE,        // F_d
+    PH_ADJ_VERT,        // V_d
+    PH_COUNT
+};
+
+struct BatchCage {
+    DevCage cage;        // pointers into the batch's cage arrays
+    int32_t depth;
+    int32_t uv;          // UV codes are refined
+    int64_t cagePt;      // first cage point of this cage in the batch's cage-point buffer
+    int64_t he, cr, pt;  // first record / crease / point of this cage's hierarchy
+    Level lv[kMaxBatchDepth + 1];
+};
+
+struct GridSync {
+    unsigned int count;
+    unsigned int gen;
+    int err;
+};
+
+struct BatchArgs {
+    const BatchCage* __restrict__ cages;
+    const int64_t* __restrict__ tiles;   // [(d * PH_COUNT + phase) * (count + 1) + c]
+    int32_t count;
+    int32_t* he;
+    cc_Crease* cr;
+    const float* cagePts;
+    float* pts;
+    float* work;                         // adjoint: running gradient per refined point
+    float* gradCage;                     // adjoint output
+    GridSync* sync;
+    unsigned int spinCap;                // polls before a barrier wait gives up
+};
+
+// ---------------------------------------------------------------------------
+// device side
+// ---------------------------------------------------------------------------
+static constexpr unsigned kSpinCap = 1u << 22;
+
+// Grid-wide barrier for a cooperative launch.  `expected` blocks must arrive;
+// a waiting block gives up after `cap` polls (about a second with the
+// default cap), records CCS_ERR_TIMEOUT and leaves.
+__device__ bool grid_sync(GridSync* gs, unsigned int cap, unsigned int expected) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ok = 1;
+        volatile unsigned int* vgen = &gs->gen;
+        const unsigned int g = *vgen;
+        __threadfence();
+        const unsigned int arrived = atomicAdd(&gs->count, 1u) + 1u;
+        if (arrived == expected) {
+            atomicExch(&gs->count, 0u);
+            __threadfence();
+            atomicAdd(&gs->gen, 1u);
+        } else {
+            unsigned int spins = 0;
+            while (*vgen == g) {
+                if (++spins > cap || *(volatile int*)&gs->err) {
+                    atomicExch(&gs->err, CCS_ERR_TIMEOUT);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(256);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+__device__ __forceinline__ int find_cage(const int64_t* ts, int32_t count, int64_t t) {
+    int lo = 0, hi = count;            // ts[lo] <= t < ts[hi]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (ts[mid] <= t) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ CageView batch_cage_view(const BatchCage& bc) {
+    CageView L;
+    L.t = make_cage_tables(bc.cage);
+    L.cr = bc.cage.cr;
+    L.V = bc.cage.V; L.F = bc.cage.F; L.E = bc.cage.E; L.H = bc.cage.H; L.C = bc.cage.E;
+    L.d = 0;
+    return L;
+}
+
+__device__ __forceinline__ QuadView<4> batch_quad_view(const BatchArgs& a, const BatchCage& bc, int d) {
+    QuadView<4> L;
+    L.t = make_cage_tables(bc.cage);
+    L.he = a.he + 4 * (bc.he + bc.lv[d].heOff);
+    L.cr = a.cr + bc.cr + bc.lv[d].crOff;
+    const Level& lv = bc.lv[d];
+    L.V = lv.V; L.F = lv.F; L.E = lv.E; L.H = lv.H; L.C = lv.C;
+    L.d = d;
+    return L;
+}
+
+// Runs `body(cage, tile index within the cage)` over one phase's tiles.
+template <class Body>
+__device__ __forceinline__ void for_tiles(const BatchArgs& a, int d, int phase, Body body) {
+    const int64_t* ts = a.tiles + ((int64_t)d * PH_COUNT + phase) * (a.count + 1);
+    const int64_t total = ts[a.count];
+    for (int64_t t = blockIdx.x; t < total; t += gridDim.x) {
+        const int c = find_cage(ts, a.count, t);
+        body(a.cages[c], t - ts[c]);
+    }
+}
+
+template <bool TOPO, bool CREASED>
+__global__ void __launch_bounds__(kBatchBlock)
+k_batch_forward(BatchArgs a, int d) {
+    __shared__ __align__(128) int32_t tile[kBatchBlock * 4 * 4];
+    const int tid = threadIdx.x;
+    if (d == 0) {
+        if (TOPO) {
+            for_tiles(a, 0, PH_CAGE_TOPO, [&](const BatchCage& bc, int64_t lt) {
+                const int64_t i = lt * kBatchBlock + tid;
+                if (i >= 4 * (int64_t)bc.cage.H) return;
+                int32_t* out = a.he + 4 * (bc.he + bc.lv[1].heOff);
+                if (bc.uv) cage_topology_item<4, true, true>(make_cage_tables(bc.cage), out, i);
+                else cage_topology_item<4, true, false>(make_cage_tables(bc.cage), out, i);
+            });
+            for_tiles(a, 0, PH_CAGE_CREASE, [&](const BatchCage& bc, int64_t lt) {
+                const int64_t i = lt * kBatchBlock + tid;
+                if (i < bc.cage.E) crease_item(bc.cage.cr, a.cr + bc.cr + bc.lv[1].crOff, (int32_t)i);
+            });
+        }
+        for_tiles(a, 0, PH_CAGE_FACE, [&](const BatchCage& bc, int64_t lt) {
+            const int64_t i = lt * kBatchBlock + tid;
+            if (i >= bc.cage.F) return;
+            face_point_item<CageView, false>(batch_cage_view(bc), a.cagePts + 3 * bc.cagePt,
+                                             a.pts + 3 * (bc.pt + bc.lv[1].ptOff), (int32_t)i);
+        });
+        for_tiles(a, 0, PH_CAGE_ZERO, [&](const BatchCage& bc, int64_t lt) {
+            const int64_t i = lt * kBatchBlock + tid;
+            if (i < bc.cage.V) st3(a.pts + 3 * (bc.pt + bc.lv[1].ptOff + i), zero3());
+        });
+        if (!grid_sync(a.sync, a.spinCap, gridDim.x)) return;
+        for_tiles(a, 0, PH_CAGE_EDGE, [&](const BatchCage& bc, int64_t lt) {
+            const int64_t i = lt * kBatchBlock + tid;
+            if (i >= bc.cage.H) return;
+            edge_owner_item<CageView, CREASED>(batch_cage_view(bc), a.cagePts + 3 * bc.cagePt,
+                                               a.pts + 3 * (bc.pt + bc.lv[1].ptOff), (int32_t)i);
+        });
+        if (!grid_sync(a.sync, a.spinCap, gridDim.x)) return;
+        for_tiles(a, 0, PH_CAGE_VERT, [&](const BatchCage& bc, int64_t lt) {
+            const int64_t i = lt * kBatchBlock + tid;
+            vertex_atomic_item<CageView, CREASED>(batch_cage_view(bc), a.cagePts + 3 * bc.cagePt,
+                                                  a.pts + 3 * (bc.pt + bc.lv[1].ptOff), (int32_t)i,
+                                                  i < bc.cage.H);
+        });
+        return;
+    }
+    for_tiles(a, d, PH_A, [&](const BatchCage& bc, int64_t lt) {
+        const Level& lv = bc.lv[d];
+        LevelArgs la;
+        la.in = a.he + 4 * (bc.he + lv.heOff);
+        la.out = a.he + 4 * (bc.he + bc.lv[d + 1].heOff);
+        la.crIn = a.cr + bc.cr + lv.crOff;
+        la.crOut = a.cr + bc.cr + bc.lv[d + 1].crOff;
+        la.pin = a.pts + 3 * (bc.pt + lv.ptOff);
+        la.pout = a.pts + 3 * (bc.pt + bc.lv[d + 1].ptOff);
+        la.H = lv.H; la.V = lv.V; la.F = lv.F; la.E = lv.E; la.C = lv.C;
+        la.zeroV = 1;
+        if (bc.uv) tile_level_a<kBatchBlock, 4, TOPO, true, true, CREASED>(la, lt * kBatchBlock, tile);
+        else tile_level_a<kBatchBlock, 4, TOPO, false, true, CREASED>(la, lt * kBatchBlock, tile);
+        __syncthreads();   // the tile's shared memory is reused by the next tile
+    });
+    if (TOPO) {
+        for_tiles(a, d, PH_A_CREASE, [&](const BatchCage& bc, int64_t lt) {
+            const int64_t i = lt * kBatchBlock + tid;
+            if (i < bc.lv[d].C)
+                crease_item(a.cr + bc.cr + bc.lv[d].crOff, a.cr + bc.cr + bc.lv[d + 1].crOff, (int32_t)i);
+        });
+    }
+    if (!grid_sync(a.sync, a.spinCap, gridDim.x)) return;
+    for_tiles(a, d, PH_B, [&](const BatchCage& bc, int64_t lt) {
+        const QuadView<4> L = batch_quad_view(a, bc, d);
+        const float* pin = a.pts + 3 * (bc.pt + bc.lv[d].ptOff);
+        float* pout = a.pts + 3 * (bc.pt + bc.lv[d + 1].ptOff);
+        if (d >= 2) tile_level_b<4, CREASED, true>(L, pin, pout, lt * kBatchBlock);
+        else tile_level_b<4, CREASED, false>(L, pin, pout, lt * kBatchBlock);
+    });
+}
+
+__global__ void __launch_bounds__(kBatchBlock)
+k_batch_adjoint(BatchArgs a, int d) {
+    const int tid = threadIdx.x;
+    auto gnew = [&](const BatchCage& bc) { return a.work + 3 * (bc.pt + bc.lv[d + 1].ptOff); };
+    for_tiles(a, d, PH_ADJ_EDGE, [&](const BatchCage& bc, int64_t lt) {
+        const int64_t i = lt * kBatchBlock + tid;
+        if (i >= bc.lv[d].H) return;
+        if (d == 0) adj_edge_item(batch_cage_view(bc), gnew(bc), (int32_t)i);
+        else adj_edge_item(batch_quad_view(a, bc, d), gnew(bc), (int32_t)i);
+    });
+    if (!grid_sync(a.sync, a.spinCap, gridDim.x)) return;
+    for_tiles(a, d, PH_ADJ_FACE, [&](const BatchCage& bc, int64_t lt) {
+        const int64_t i = lt * kBatchBlock + tid;
+        if (i >= bc.lv[d].F) return;
+        if (d == 0) adj_face_item(batch_cage_view(bc), gnew(bc), (int32_t)i);
+        else adj_face_item(batch_quad_view(a, bc, d), gnew(bc), (int32_t)i);
+    });
+    if (!grid_sync(a.sync, a.spinCap, gridDim.x)) return;
+    for_tiles(a, d, PH_ADJ_VERT, [&](const BatchCage& bc, int64_t lt) {
+        const int64_t i = lt * kBatchBlock + tid;
+        if (i >= bc.lv[d].V) return;
+        if (d == 0) adj_vertex_item(batch_cage_view(bc), gnew(bc), a.gradCage + 3 * bc.cagePt, (int32_t)i);
+        else adj_vertex_item(batch_quad_view(a, bc, d), gnew(bc), a.work + 3 * (bc.pt + bc.lv[d].ptOff), (int32_t)i);
+    });
+}
+
+// A one-block barrier that waits for a second arrival that never comes: the
+// bounded wait must give up and report, leaving the context usable.
+__global__ void k_barrier_timeout_probe(GridSync* gs, unsigned int cap) {
+    grid_sync(gs, cap, 2u);
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+int level_counts_ex(const cc_Mesh* cage, int32_t D, std::vector<Level>* out);   // ccs_capi.cu
+int validate_cage_ex(const cc_Mesh* m);                                           // ccs_capi.cu
+bool twins_consistent_ex(const cc_Mesh* m);                                       // ccs_capi.cu
+int set_last_error(int status);                                                  // ccs_capi.cu
+
+}  // namespace ccs
+
+struct ccs_Batch {
+    int device = 0;
+    int32_t count = 0, maxDepth = 0;
+    uint32_t flags = 0;
+    std::vector<ccs::BatchCage> host;        // descriptors (device pointers inside)
+    std::vector<int64_t> tiles;              // host copy of the tile prefix sums
+    ccs::BatchCage* dCages = nullptr;
+    int64_t* dTiles = nullptr;
+    // cage arrays (concatenated)
+    int32_t *cHe = nullptr, *cV2h = nullptr, *cE2h = nullptr, *cF2h = nullptr, *cFsz = nullptr;
+    cc_Crease* cCr = nullptr;
+    float *cUv = nullptr, *cagePts = nullptr;
+    // hierarchy and buffers
+    int32_t* he = nullptr;
+    cc_Crease* cr = nullptr;
+    float *pts = nullptr, *work = nullptr, *gradCage = nullptr;
+    ccs::GridSync* sync = nullptr;
+    int64_t totH = 0, totC = 0, totV = 0, totCagePts = 0;
+    cudaStream_t stream = nullptr;
+    bool ownStream = false;
+    int blocksPerSM = 0;                     // 0 = as many as fit
+    int numSMs = 148;
+    bool graphOk = true;
+    bool topoReady = false;                  // ccs_BatchRefine_cuda has run
+    std::map<int, cudaGraphExec_t> graphs;
+    std::mutex mu;
+};
+
+namespace ccs {
+
+static const int kPhasesPerDepth = PH_COUNT;
+
+static int64_t phase_units(const BatchCage& bc, int d, int ph) {
+    if (d >= bc.depth) return 0;
+    const Level& lv = bc.lv[d];
+    switch (ph) {
+        case PH_CAGE_TOPO: return d == 0 ? 4 * (int64_t)lv.H : 0;
+        case PH_CAGE_CREASE: return d == 0 ? lv.E : 0;
+        case PH_CAGE_FACE: return d == 0 ? lv.F : 0;
+        case PH_CAGE_ZERO: return d == 0 ? lv.V : 0;
+        case PH_CAGE_EDGE: return d == 0 ? lv.H : 0;
+        case PH_CAGE_VERT: return d == 0 ? lv.H : 0;
+        case PH_A: return d >= 1 ? lv.H : 0;
+        case PH_A_CREASE: return d >= 1 ? lv.C : 0;
+        case PH_B: return d >= 1 ? lv.H : 0;
+        case PH_ADJ_EDGE: return lv.H;
+        case PH_ADJ_FACE: return lv.F;
+        case PH_ADJ_VERT: return lv.V;
+        default: return 0;
+    }
+}
+
+static void free_batch(ccs_Batch* b) {
+    if (!b) return;
+    for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
+    cudaFree(b->dCages); cudaFree(b->dTiles);
+    cudaFree(b->cHe); cudaFree(b->cV2h); cudaFree(b->cE2h); cudaFree(b->cF2h); cudaFree(b->cFsz);
+    cudaFree(b->cCr); cudaFree(b->cUv); cudaFree(b->cagePts);
+    cudaFree(b->he); cudaFree(b->cr); cudaFree(b->pts); cudaFree(b->work); cudaFree(b->gradCage);
+    cudaFree(b->sync);
+    if (b->ownStream && b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+template <class T>
+static bool bmalloc(T** p, int64_t n) {
+    return cudaMalloc((void**)p, sizeof(T) * (size_t)(n > 0 ? n : 1)) == cudaSuccess;
+}
+
+static int batch_create(const cc_Mesh* const* cages, const int32_t* depths, int32_t count, uint32_t flags,
+                        ccs_Batch** out) {
+    if (!out || !cages || !depths || count <= 0) return CCS_ERR_ARG;
+    *out = nullptr;
+    if (flags & (CCS_FLAG_NO_UV | CCS_FLAG_DETERMINISTIC)) return CCS_ERR_UNSUPPORTED;
+    ccs_Batch* b = new (std::nothrow) ccs_Batch();
+    if (!b) return CCS_ERR_ALLOC;
+    b->count = count;
+    b->flags = flags;
+    b->host.resize(count);
+    int64_t oHe = 0, oCr = 0, oUv = 0, oV = 0, oE = 0, oF = 0;
+    for (int32_t c = 0; c < count; ++c) {
+        const cc_Mesh* m = cages[c];
+        const int32_t D = depths[c];
+        if (D < 1 || D > kMaxBatchDepth) { delete b; return CCS_ERR_ARG; }
+        int st = validate_cage_ex(m);
+        if (st != CCS_OK) { delete b; return st; }
+        if (!twins_consistent_ex(m)) { delete b; return CCS_ERR_UNSUPPORTED; }
+        std::vector<Level> lv;
+        st = level_counts_ex(m, D, &lv);
+        if (st != CCS_OK) { delete b; return st; }
+        BatchCage& bc = b->host[c];
+        memset(&bc, 0, sizeof bc);
+        bc.depth = D;
+        bc.uv = m->uvCount > 0;
+        for (int d = 0; d <= D; ++d) bc.lv[d] = lv[d];
+        bc.cage.V = m->vertexCount; bc.cage.U = m->uvCount; bc.cage.H = m->halfedgeCount;
+        bc.cage.E = m->edgeCount; bc.cage.F = m->faceCount;
+        // offsets for now; turned into device pointers below
+        bc.cage.he = (int32_t*)(intptr_t)oHe; bc.cage.cr = (cc_Crease*)(intptr_t)oE;
+        bc.cage.uvs = (float*)(intptr_t)oUv; bc.cage.v2h = (int32_t*)(intptr_t)oV;
+        bc.cage.e2h = (int32_t*)(intptr_t)oE; bc.cage.f2h = (int32_t*)(intptr_t)oF;
+        bc.cage.fsz = (int32_t*)(intptr_t)oF;
+        bc.cagePt = oV;
+        bc.he = b->totH; bc.cr = b->totC; bc.pt = b->totV;
+        const Level& last = lv[D];
+        b->totH += last.heOff + last.H;
+        b->totC += last.crOff + last.C;
+        b->totV += last.ptOff + last.V;
+        oHe += m->halfedgeCount; oCr += m->edgeCount; oUv += m->uvCount;
+        oV += m->vertexCount; oE += m->edgeCount; oF += m->faceCount;
+        b->maxDepth = std::max(b->maxDepth, D);
+    }
+    b->totCagePts = oV;
+    if (cudaGetDevice(&b->device) != cudaSuccess) { delete b; return CCS_ERR_CUDA; }
+    cudaDeviceGetAttribute(&b->numSMs, cudaDevAttrMultiProcessorCount, b->device);
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) { delete b; return CCS_ERR_CUDA; }
+    b->ownStream = true;
+    if (!bmalloc(&b->cHe, 7 * oHe) || !bmalloc(&b->cCr, oE) || !bmalloc(&b->cUv, 2 * oUv) ||
+        !bmalloc(&b->cV2h, oV) || !bmalloc(&b->cE2h, oE) || !bmalloc(&b->cF2h, oF) || !bmalloc(&b->cFsz, oF) ||
+        !bmalloc(&b->cagePts, 3 * oV) || !bmalloc(&b->he, 4 * b->totH) || !bmalloc(&b->cr, b->totC) ||
+        !bmalloc(&b->pts, 3 * b->totV) || !bmalloc(&b->sync, 1)) {
+        free_batch(b);
+        return CCS_ERR_ALLOC;
+    }
+    // upload the cages
+    for (int32_t c = 0; c < count; ++c) {
+        const cc_Mesh* m = cages[c];
+        BatchCage& bc = b->host[c];
+        const int64_t iHe = (int64_t)(intptr_t)bc.cage.he, iE = (int64_t)(intptr_t)bc.cage.e2h;
+        const int64_t iUv = (int64_t)(intptr_t)bc.cage.uvs, iV = (int64_t)(intptr_t)bc.cage.v2h;
+        const int64_t iF = (int64_t)(intptr_t)bc.cage.f2h;
+        bc.cage.he = b->cHe + 7 * iHe; bc.cage.cr = b->cCr + iE; bc.cage.uvs = b->cUv + 2 * iUv;
+        bc.cage.v2h = b->cV2h + iV; bc.cage.e2h = b->cE2h + iE; bc.cage.f2h = b->cF2h + iF;
+        bc.cage.fsz = b->cFsz + iF; bc.cage.pts = b->cagePts + 3 * iV;
+        std::vector<int32_t> fsz((size_t)m->faceCount, 0);
+        for (int32_t h = 0; h < m->halfedgeCount; ++h) ++fsz[(size_t)m->halfedges[h].faceID];
+        cudaStream_t st = b->stream;
+        if (cudaMemcpyAsync(bc.cage.he, m->halfedges, sizeof(cc_Halfedge) * (size_t)m->halfedgeCount, cudaMemcpyHostToDevice, st) ||
+            cudaMemcpyAsync(bc.cage.cr, m->creases, sizeof(cc_Crease) * (size_t)m->edgeCount, cudaMemcpyHostToDevice, st) ||
+            (m->uvCount > 0 && cudaMemcpyAsync(bc.cage.uvs, m->uvs, sizeof(float) * 2 * (size_t)m->uvCount, cudaMemcpyHostToDevice, st)) ||
+            cudaMemcpyAsync(bc.cage.v2h, m->vertexToHalfedgeIDs, sizeof(int32_t) * (size_t)m->vertexCount, cudaMemcpyHostToDevice, st) ||
+            cudaMemcpyAsync(bc.cage.e2h, m->edgeToHalfedgeIDs, sizeof(int32_t) * (size_t)m->edgeCount, cudaMemcpyHostToDevice, st) ||
+            cudaMemcpyAsync(bc.cage.f2h, m->faceToHalfedgeIDs, sizeof(int32_t) * (size_t)m->faceCount, cudaMemcpyHostToDevice, st) ||
+            cudaMemcpyAsync(bc.cage.fsz, fsz.data(), sizeof(int32_t) * fsz.size(), cudaMemcpyHostToDevice, st) ||
+            cudaMemcpyAsync(bc.cage.pts, m->vertexPoints, sizeof(float) * 3 * (size_t)m->vertexCount, cudaMemcpyHostToDevice, st) ||
+            cudaStreamSynchronize(st)) {
+            free_batch(b);
+            return CCS_ERR_CUDA;
+        }
+    }
+    // tile prefix sums per (depth, phase)
+    const int64_t stride = (int64_t)count + 1;
+    b->tiles.assign((size_t)(b->maxDepth * kPhasesPerDepth * stride), 0);
+    for (int d = 0; d < b->maxDepth; ++d)
+        for (int ph = 0; ph < PH_COUNT; ++ph) {
+            int64_t* ts = &b->tiles[(size_t)((d * PH_COUNT + ph) * stride)];
+            for (int32_t c = 0; c < count; ++c)
+                ts[c + 1] = ts[c] + (phase_units(b->host[c], d, ph) + kBatchBlock - 1) / kBatchBlock;
+        }
+    if (!bmalloc(&b->dCages, count) || !bmalloc(&b->dTiles, (int64_t)b->tiles.size()) ||
+        cudaMemcpy(b->dCages, b->host.data(), sizeof(BatchCage) * (size_t)count, cudaMemcpyHostToDevice) ||
+        cudaMemcpy(b->dTiles, b->tiles.data(), sizeof(int64_t) * b->tiles.size(), cudaMemcpyHostToDevice)) {
+        free_batch(b);
+        return CCS_ERR_ALLOC;
+    }
+    *out = b;
+    return CCS_OK;
+}
+
+static BatchArgs batch_args(ccs_Batch* b) {
+    BatchArgs a;
+    a.cages = b->dCages; a.tiles = b->dTiles; a.count = b->count;
+    a.he = b->he; a.cr = b->cr; a.cagePts = b->cagePts; a.pts = b->pts;
+    a.work = b->work; a.gradCage = b->gradCage; a.sync = b->sync;
+    a.spinCap = kSpinCap;
+    return a;
+}
+
+template <class Kernel>
+static cudaError_t launch_coop(ccs_Batch* b, Kernel kernel, int64_t maxTiles, BatchArgs a, int d) {
+    int perSM = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kernel, kBatchBlock, 0);
+    if (e != cudaSuccess || perSM <= 0) return e != cudaSuccess ? e : cudaErrorLaunchOutOfResources;
+    if (b->blocksPerSM > 0) perSM = std::min(perSM, b->blocksPerSM);
+    int64_t grid = (int64_t)perSM * b->numSMs;
+    grid = std::max<int64_t>(1, std::min<int64_t>(grid, maxTiles));
+    cudaLaunchConfig_t cfg;
+    memset(&cfg, 0, sizeof cfg);
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(kBatchBlock);
+    cfg.stream = b->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, a, d);
+}
+
+static int64_t max_tiles(const ccs_Batch* b, int d, std::initializer_list<int> phases) {
+    int64_t m = 0;
+    const int64_t stride = (int64_t)b->count + 1;
+    for (int ph : phases) m = std::max(m, b->tiles[(size_t)((d * PH_COUNT + ph) * stride + b->count)]);
+    return m;
+}
+
+enum BatchOp { BOP_REFINE = 0, BOP_POINTS = 1, BOP_ADJOINT = 2 };
+
+static cudaError_t enqueue_batch(ccs_Batch* b, int op, bool creased) {
+    BatchArgs a = batch_args(b);
+    cudaError_t e = cudaMemsetAsync(b->sync, 0, sizeof(GridSync), b->stream);
+    if (e != cudaSuccess) return e;
+    if (op == BOP_ADJOINT) {
+        e = cudaMemsetAsync(b->gradCage, 0, sizeof(float) * 3 * (size_t)b->totCagePts, b->stream);
+        for (int d = b->maxDepth - 1; d >= 0 && e == cudaSuccess; --d) {
+            const int64_t mt = max_tiles(b, d, {PH_ADJ_EDGE, PH_ADJ_FACE, PH_ADJ_VERT});
+            e = launch_coop(b, k_batch_adjoint, mt, a, d);
+        }
+        return e;
+    }
+    const bool topo = op == BOP_REFINE;
+    for (int d = 0; d < b->maxDepth && e == cudaSuccess; ++d) {
+        const int64_t mt = d == 0 ? max_tiles(b, 0, {PH_CAGE_TOPO, PH_CAGE_CREASE, PH_CAGE_FACE, PH_CAGE_ZERO,
+                                                      PH_CAGE_EDGE, PH_CAGE_VERT})
+                                  : max_tiles(b, d, {PH_A, PH_A_CREASE, PH_B});
+        if (topo) e = creased ? launch_coop(b, k_batch_forward<true, true>, mt, a, d)
+                              : launch_coop(b, k_batch_forward<true, false>, mt, a, d);
+        else e = creased ? launch_coop(b, k_batch_forward<false, true>, mt, a, d)
+                         : launch_coop(b, k_batch_forward<false, false>, mt, a, d);
+    }
+    return e;
+}
+
+// Graph replay when possible; a cooperative launch that cannot be captured
+// falls back to direct launches for the life of the batch.
+static int run_batch(ccs_Batch* b, int op, bool creased) {
+    const int key = op * 2 + (creased ? 1 : 0);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (b->stream) cudaStreamIsCapturing(b->stream, &cap);
+    if (b->graphOk && b->stream && !(b->flags & CCS_FLAG_NO_GRAPH) && cap == cudaStreamCaptureStatusNone) {
+        auto it = b->graphs.find(key);
+        if (it == b->graphs.end()) {
+            cudaGraph_t graph = nullptr;
+            cudaGraphExec_t exec = nullptr;
+            bool ok = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+            cudaError_t e = ok ? enqueue_batch(b, op, creased) : cudaErrorUnknown;
+            if (ok) ok = cudaStreamEndCapture(b->stream, &graph) == cudaSuccess && e == cudaSuccess && graph;
+            if (ok) ok = cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+            if (graph) cudaGraphDestroy(graph);
+            cudaGetLastError();
+            if (!ok) {
+                b->graphOk = false;
+            } else {
+                it = b->graphs.emplace(key, exec).first;
+            }
+        }
+        if (b->graphOk) return cudaGraphLaunch(it->second, b->stream) == cudaSuccess ? CCS_OK : CCS_ERR_CUDA;
+    }
+    return enqueue_batch(b, op, creased) == cudaSuccess ? CCS_OK : CCS_ERR_CUDA;
+}
+
+struct BatchDevice {
+    int prev = -1, dev;
+    explicit BatchDevice(int d) : dev(d) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~BatchDevice() {
+        if (prev >= 0 && prev != dev) cudaSetDevice(prev);
+    }
+};
+
+}  // namespace ccs
+
+using namespace ccs;
+
+extern "C" {
+
+int ccs_BatchCreate_cuda(const cc_Mesh* const* cages, const int32_t* depths, int32_t count, uint32_t flags,
+                         ccs_Batch** out) {
+    return set_last_error(batch_create(cages, depths, count, flags, out));
+}
+
+void ccs_BatchRelease_cuda(ccs_Batch* batch) {
+    if (!batch) return;
+    BatchDevice g(batch->device);
+    if (batch->stream) cudaStreamSynchronize(batch->stream);
+    free_batch(batch);
+}
+
+int ccs_BatchRefine_cuda(ccs_Batch* batch, int mode) {
+    if (!batch || (mode != CCS_POINTS_SCATTER && mode != CCS_POINTS_NOCREASES_SCATTER)) return set_last_error(CCS_ERR_ARG);
+    std::lock_guard<std::mutex> lock(batch->mu);
+    BatchDevice g(batch->device);
+    const int st = run_batch(batch, BOP_REFINE, mode == CCS_POINTS_SCATTER);
+    if (st == CCS_OK) batch->topoReady = true;
+    return set_last_error(st);
+}
+
+int ccs_BatchRefinePoints_cuda(ccs_Batch* batch, int mode) {
+    if (!batch || (mode != CCS_POINTS_SCATTER && mode != CCS_POINTS_NOCREASES_SCATTER)) return set_last_error(CCS_ERR_ARG);
+    std::lock_guard<std::mutex> lock(batch->mu);
+    if (!batch->topoReady) return set_last_error(CCS_ERR_STATE);
+    BatchDevice g(batch->device);
+    return set_last_error(run_batch(batch, BOP_POINTS, mode == CCS_POINTS_SCATTER));
+}
+
+int ccs_BatchAdjointPoints_cuda(ccs_Batch* batch) {
+    if (!batch) return set_last_error(CCS_ERR_ARG);
+    std::lock_guard<std::mutex> lock(batch->mu);
+    if (!batch->topoReady) return set_last_error(CCS_ERR_STATE);
+    BatchDevice g(batch->device);
+    if (!batch->work && (!bmalloc(&batch->work, 3 * batch->totV) || !bmalloc(&batch->gradCage, 3 * batch->totCagePts)))
+        return set_last_error(CCS_ERR_ALLOC);
+    return set_last_error(run_batch(batch, BOP_ADJOINT, true));
+}
+
+int ccs_BatchGetArrays_cuda(ccs_Batch* batch, ccs_BatchArrays* out) {
+    if (!batch || !out) return set_last_error(CCS_ERR_ARG);
+    std::lock_guard<std::mutex> lock(batch->mu);
+    BatchDevice g(batch->device);
+    if (!batch->work && (!bmalloc(&batch->work, 3 * batch->totV) || !bmalloc(&batch->gradCage, 3 * batch->totCagePts)))
+        return set_last_error(CCS_ERR_ALLOC);
+    out->halfedges = batch->he;
+    out->creases = batch->cr;
+    out->points = batch->pts;
+    out->cagePoints = batch->cagePts;
+    out->gradPoints = batch->work;
+    out->gradCagePoints = batch->gradCage;
+    out->halfedgeCount = batch->totH;
+    out->creaseCount = batch->totC;
+    out->pointCount = batch->totV;
+    out->cagePointCount = batch->totCagePts;
+    return set_last_error(CCS_OK);
+}
+
+int ccs_BatchCageInfo_cuda(const ccs_Batch* batch, int32_t cage, ccs_BatchCageInfo* out) {
+    if (!batch || !out || cage < 0 || cage >= batch->count) return set_last_error(CCS_ERR_ARG);
+    const BatchCage& bc = batch->host[(size_t)cage];
+    const Level& last = bc.lv[bc.depth];
+    out->depth = bc.depth;
+    out->cagePointOffset = bc.cagePt;
+    out->cagePointCount = bc.cage.V;
+    out->halfedgeOffset = bc.he;
+    out->halfedgeCount = last.heOff + last.H;
+    out->creaseOffset = bc.cr;
+    out->creaseCount = last.crOff + last.C;
+    out->pointOffset = bc.pt;
+    out->pointCount = last.ptOff + last.V;
+    out->finestPointOffset = bc.pt + last.ptOff;
+    out->finestPointCount = last.V;
+    return set_last_error(CCS_OK);
+}
+
+int ccs_BatchSetStream_cuda(ccs_Batch* batch, void* stream) {
+    if (!batch) return set_last_error(CCS_ERR_ARG);
+    std::lock_guard<std::mutex> lock(batch->mu);
+    BatchDevice g(batch->device);
+    if (batch->stream) cudaStreamSynchronize(batch->stream);
+    if (batch->ownStream && batch->stream) cudaStreamDestroy(batch->stream);
+    batch->stream = (cudaStream_t)stream;
+    batch->ownStream = false;
+    return set_last_error(CCS_OK);
+}
+
+int ccs_BatchSetSchedule_cuda(ccs_Batch* batch, int32_t blocksPerSM) {
+    if (!batch || blocksPerSM < 0) return set_last_error(CCS_ERR_ARG);
+    std::lock_guard<std::mutex> lock(batch->mu);
+    if (batch->blocksPerSM != blocksPerSM) {
+        for (auto& kv : batch->graphs) cudaGraphExecDestroy(kv.second);
+        batch->graphs.clear();
+        batch->blocksPerSM = blocksPerSM;
+    }
+    return set_last_error(CCS_OK);
+}
+
+int ccs_BatchSynchronize_cuda(ccs_Batch* batch) {
+    if (!batch) return set_last_error(CCS_ERR_ARG);
+    BatchDevice g(batch->device);
+    if (cudaStreamSynchronize(batch->stream) != cudaSuccess) return set_last_error(CCS_ERR_CUDA);
+    GridSync gs;
+    if (cudaMemcpy(&gs, batch->sync, sizeof gs, cudaMemcpyDeviceToHost) != cudaSuccess) return set_last_error(CCS_ERR_CUDA);
+    return set_last_error(gs.err ? CCS_ERR_TIMEOUT : CCS_OK);
+}
+
+int ccs_BarrierTimeoutSelfTest_cuda(void) {
+    GridSync* gs = nullptr;
+    if (cudaMalloc((void**)&gs, sizeof(GridSync)) != cudaSuccess) return set_last_error(CCS_ERR_ALLOC);
+    int st = CCS_ERR_CUDA;
+    GridSync h{0u, 0u, 0};
+    if (cudaMemcpy(gs, &h, sizeof h, cudaMemcpyHostToDevice) == cudaSuccess) {
+        k_barrier_timeout_probe<<<1, 32>>>(gs, 1u << 14);
+        if (cudaDeviceSynchronize() == cudaSuccess && cudaMemcpy(&h, gs, sizeof h, cudaMemcpyDeviceToHost) == cudaSuccess)
+            st = h.err == CCS_ERR_TIMEOUT ? CCS_ERR_TIMEOUT : CCS_OK;
+    }
+    cudaFree(gs);
+    return set_last_error(st);
+}
+
+int ccs_BatchDownload_cuda(ccs_Batch* batch, int32_t cage, cc_Subd* subd) {
+    if (!batch || !subd || cage < 0 || cage >= batch->count) return set_last_error(CCS_ERR_ARG);
+    const BatchCage& bc = batch->host[(size_t)cage];
+    if (subd->maxDepth != bc.depth || !subd->halfedges || !subd->creases || !subd->vertexPoints)
+        return set_last_error(CCS_ERR_ARG);
+    BatchDevice g(batch->device);
+    const Level& last = bc.lv[bc.depth];
+    const int64_t nH = last.heOff + last.H, nC = last.crOff + last.C, nV = last.ptOff + last.V;
+    cudaStream_t st = batch->stream;
+    if (cudaMemcpyAsync(subd->halfedges, batch->he + 4 * bc.he, 16 * (size_t)nH, cudaMemcpyDeviceToHost, st) ||
+        cudaMemcpyAsync(subd->creases, batch->cr + bc.cr, sizeof(cc_Crease) * (size_t)nC, cudaMemcpyDeviceToHost, st) ||
+        cudaMemcpyAsync(subd->vertexPoints, batch->pts + 3 * bc.pt, 12 * (size_t)nV, cudaMemcpyDeviceToHost, st) ||
+        cudaStreamSynchronize(st))
+        return set_last_error(CCS_ERR_CUDA);
+    return set_last_error(CCS_OK);
+}
+
+}  // extern "C"

@@ -414,6 +414,11 @@ int adjoint_into(const cc_Subd* subd, const float* gradPoints, float* gradCage, 
 
 int set_last_error(int status) { return ret(status); }
 
+// Used by the batched path (ccs_batch.cu).
+int level_counts_ex(const cc_Mesh* cage, int32_t D, std::vector<Level>* out) { return level_counts(cage, D, out); }
+int validate_cage_ex(const cc_Mesh* m) { return validate_cage(m); }
+bool twins_consistent_ex(const cc_Mesh* m) { return twins_consistent(m); }
+
 }  // namespace ccs
 
 using namespace ccs;

@@ -32,7 +32,7 @@
 #include <cstdio>
 
 #include "ccs_host.h"
-#include "ccs_internal.cuh"
+#include "ccs_tiles.cuh"
 
 namespace ccs {
 
@@ -118,166 +118,34 @@ k_quad_topology(const int32_t* __restrict__ in, int32_t* __restrict__ out,
 }
 
 // ---------------------------------------------------------------------------
-// Topology + UVs, cage level (CatmullClark.h:2693-2740, :2825-2869)
+// Cage topology + UVs, creases, face / edge / vertex points: thin kernels
+// over the item functions of ccs_tiles.cuh (shared with the batched path).
 // ---------------------------------------------------------------------------
 template <int RW, bool TOPO, bool UV>
 __global__ void __launch_bounds__(kBlock)
 k_cage_topology(CageTables t, int32_t* __restrict__ out) {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= 4 * (int64_t)t.n.H) return;
-    const int32_t h = (int32_t)(c >> 2), m = (int32_t)(c & 3);
-    const int32_t* r = t.he + (int64_t)CH_WORDS * h;
-    const int32_t twin = r[CH_TWIN], next = r[CH_NEXT], prev = r[CH_PREV];
-    const int32_t* rp = t.he + (int64_t)CH_WORDS * prev;
-    int32_t o_tw = 0, o_ed = 0, o_vx = 0, o_uv = 0;
-    if (TOPO) {
-        const int32_t V = t.n.V, F = t.n.F, E = t.n.E;
-        switch (m) {
-            case 0: {
-                const int32_t twinNext = twin >= 0 ? t.he[(int64_t)CH_WORDS * twin + CH_NEXT] : -1;
-                o_tw = child(twinNext, 3); o_ed = 2 * r[CH_EDGE] + (h > twin ? 0 : 1); o_vx = r[CH_VERT];
-                break;
-            }
-            case 1: o_tw = child(next, 2); o_ed = 2 * E + h; o_vx = V + F + r[CH_EDGE]; break;
-            case 2: o_tw = child(prev, 1); o_ed = 2 * E + prev; o_vx = V + r[CH_FACE]; break;
-            default: {
-                const int32_t pt = rp[CH_TWIN], pe = rp[CH_EDGE];
-                o_tw = child(pt, 0); o_ed = 2 * pe + (prev > pt ? 1 : 0); o_vx = V + F + pe;
-                break;
-            }
-        }
-    }
-    if (UV) {
-        const float* uvh = t.uvs + 2 * (int64_t)r[CH_UV];
-        const float u = uvh[0], v = uvh[1];
-        switch (m) {
-            case 0: o_uv = uv_enc(u, v); break;
-            case 1: {
-                const float* q = t.uvs + 2 * (int64_t)t.he[(int64_t)CH_WORDS * next + CH_UV];
-                o_uv = uv_enc(flerp(u, q[0], 0.5f), flerp(v, q[1], 0.5f));
-                break;
-            }
-            case 2: {
-                float fu = u, fv = v;
-                int32_t n = 1, guard = 0;
-                for (int32_t it = next; it != h && guard < kRingCap; it = t.he[(int64_t)CH_WORDS * it + CH_NEXT], ++guard) {
-                    const float* q = t.uvs + 2 * (int64_t)t.he[(int64_t)CH_WORDS * it + CH_UV];
-                    fu = fadd(fu, q[0]);
-                    fv = fadd(fv, q[1]);
-                    ++n;
-                }
-                o_uv = uv_enc(fdiv(fu, (float)n), fdiv(fv, (float)n));
-                break;
-            }
-            default: {
-                const float* q = t.uvs + 2 * (int64_t)rp[CH_UV];
-                o_uv = uv_enc(flerp(u, q[0], 0.5f), flerp(v, q[1], 0.5f));
-                break;
-            }
-        }
-    }
-    if constexpr (RW == 4 && TOPO && UV) {
-        reinterpret_cast<int4*>(out)[c] = make_int4(o_tw, o_ed, o_vx, o_uv);
-    } else {
-        int32_t* o = out + (int64_t)RW * c;
-        if (TOPO) { o[0] = o_tw; o[1] = o_ed; o[2] = o_vx; }
-        if (UV && RW == 4) o[3] = o_uv;
-    }
+    if (c < 4 * (int64_t)t.n.H) cage_topology_item<RW, TOPO, UV>(t, out, c);
 }
 
-// ---------------------------------------------------------------------------
-// Creases (CatmullClark.h:2950-2983 cage, :2992-3026 quad levels)
-// ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kBlock)
 k_creases(const cc_Crease* __restrict__ in, cc_Crease* __restrict__ out, int32_t C) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= C) return;
-    const int32_t e = (int32_t)i;
-    const cc_Crease me = in[e];
-    const int32_t nx = me.nextID, pv = me.prevID;
-    const cc_Crease cn = in[nx], cp = in[pv];
-    const bool t1 = cn.prevID == e && nx != e;
-    const bool t2 = cp.nextID == e && pv != e;
-    const float thisS = fmul(3.0f, me.sharpness);
-    cc_Crease a, b;
-    a.nextID = 2 * e + 1;
-    b.nextID = 2 * nx + (t1 ? 0 : 1);
-    a.prevID = 2 * pv + (t2 ? 1 : 0);
-    b.prevID = 2 * e + 0;
-    a.sharpness = fmax_ref(0.0f, fsub(fquarter(fadd(cp.sharpness, thisS)), 1.0f));
-    b.sharpness = fmax_ref(0.0f, fsub(fquarter(fadd(thisS, cn.sharpness)), 1.0f));
-    out[2 * i + 0] = a;
-    out[2 * i + 1] = b;
+    if (i < C) crease_item(in, out, (int32_t)i);
 }
 
-// ---------------------------------------------------------------------------
-// Face points (:1408-1463 cage, :2004-2052 quad levels)
-// ---------------------------------------------------------------------------
-// GATHER_SEM = sum then scale (gather routines); otherwise each vertex adds
-// p / n in halfedge order (scatter routines, order of a one-thread run).
 template <class View, bool GATHER_SEM>
 __global__ void __launch_bounds__(kBlock)
 k_face_points(View L, const float* __restrict__ pin, float* __restrict__ pout) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= L.F) return;
-    const int32_t f = (int32_t)i;
-    float* fp = pout + 3 * ((int64_t)L.V + f);
-    if constexpr (View::kQuad) {
-        f3 p[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) p[k] = ld3(pin + 3 * (int64_t)L.vert(4 * f + k));
-        if (GATHER_SEM) {
-            f3 acc = add3(add3(add3(p[0], p[1]), p[2]), p[3]);
-            st3(fp, mul3(acc, 0.25f));
-        } else {
-            f3 acc = zero3();
-#pragma unroll
-            for (int k = 0; k < 4; ++k) acc = add3(acc, quarter3(p[k]));
-            st3(fp, acc);
-        }
-    } else {
-        const int32_t h0 = L.face_he(f);
-        float n = 1.0f;
-        int guard = 0;
-        for (int32_t it = L.next(h0); it != h0 && guard < kRingCap; it = L.next(it), ++guard) n = fadd(n, 1.0f);
-        if (GATHER_SEM) {
-            f3 acc = ld3(pin + 3 * (int64_t)L.vert(h0));
-            guard = 0;
-            for (int32_t it = L.next(h0); it != h0 && guard < kRingCap; it = L.next(it), ++guard)
-                acc = add3(acc, ld3(pin + 3 * (int64_t)L.vert(it)));
-            st3(fp, mul3(acc, frcp(n)));
-        } else {
-            f3 acc = add3(zero3(), div3(ld3(pin + 3 * (int64_t)L.vert(h0)), n));
-            guard = 0;
-            for (int32_t it = L.next(h0); it != h0 && guard < kRingCap; it = L.next(it), ++guard)
-                acc = add3(acc, div3(ld3(pin + 3 * (int64_t)L.vert(it)), n));
-            st3(fp, acc);
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Edge points, scatter rule: the pair's larger halfedge adds both shares.
-// ---------------------------------------------------------------------------
-template <class View, bool CREASED>
-__device__ __forceinline__ f3 edge_share(const View& L, int32_t h, const float* pin, const float* fpt) {
-    if (CREASED) return creased_edge_share(L, h, pin, fpt);
-    return smooth_edge_share(L, h, pin, fpt);
+    if (i < L.F) face_point_item<View, GATHER_SEM>(L, pin, pout, (int32_t)i);
 }
 
 template <class View, bool CREASED>
 __global__ void __launch_bounds__(kBlock)
 k_edge_owner(View L, const float* __restrict__ pin, float* __restrict__ pout) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= L.H) return;
-    const int32_t h = (int32_t)i;
-    const int32_t tw = L.twin(h);
-    if (!(h > tw)) return;   // the pair's smaller halfedge defers to its twin
-    const float* fpt = pout + 3 * (int64_t)L.V;
-    float* ept = pout + 3 * ((int64_t)L.V + L.F);
-    f3 acc = add3(zero3(), edge_share<View, CREASED>(L, tw >= 0 ? tw : h, pin, fpt));
-    if (tw >= 0) acc = add3(acc, edge_share<View, CREASED>(L, h, pin, fpt));
-    st3(ept + 3 * (int64_t)L.edge(h), acc);
+    if (i < L.H) edge_owner_item<View, CREASED>(L, pin, pout, (int32_t)i);
 }
 
 // Edge points, gather rule (:1476-1515, :1561-1600, :2065-2105, :2151-2191)
@@ -300,49 +168,18 @@ k_edge_gather(View L, const float* __restrict__ pin, float* __restrict__ pout) {
     else st3(ept + 3 * (int64_t)e, lerp3(sharpP, smoothP, tw < 0 ? 0.0f : 1.0f));
 }
 
-// ---------------------------------------------------------------------------
 // Vertex points, scatter rule with warp-aggregated float atomics
-// ---------------------------------------------------------------------------
-template <class View, bool CREASED>
-__device__ __forceinline__ f3 vertex_share(const View& L, int32_t h, const float* pin, const float* fpt,
-                                           const float* ept) {
-    if (CREASED) return creased_vertex_share(L, h, pin, fpt, ept);
-    return smooth_vertex_share(L, h, pin, fpt, ept);
-}
-
 template <class View, bool CREASED>
 __global__ void __launch_bounds__(kBlock)
 k_vertex_atomic(View L, const float* __restrict__ pin, float* __restrict__ pout) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = i < L.H;
-    const int lane = threadIdx.x & 31;
-    const float* fpt = pout + 3 * (int64_t)L.V;
-    const float* ept = pout + 3 * ((int64_t)L.V + L.F);
-    int32_t v = -1 - lane;           // distinct keys for lanes without work
-    f3 s = zero3();
-    if (valid) {
-        const int32_t h = (int32_t)i;
-        v = L.vert(h);
-        s = vertex_share<View, CREASED>(L, h, pin, fpt, ept);
-    }
-    const unsigned full = 0xffffffffu;
-    const unsigned grp = __match_any_sync(full, v);
-    const int n = __popc(grp);
-    const int maxn = (int)__reduce_max_sync(full, (unsigned)n);
-    f3 acc = zero3();
-    for (int k = 0; k < maxn; ++k) {
-        const int src = k < n ? (int)__fns(grp, 0, k + 1) : lane;
-        const float x = __shfl_sync(full, s.x, src);
-        const float y = __shfl_sync(full, s.y, src);
-        const float z = __shfl_sync(full, s.z, src);
-        if (k < n) acc = add3(acc, f3{x, y, z});
-    }
-    if (valid && lane == __ffs(grp) - 1) {
-        float* o = pout + 3 * (int64_t)v;
-        atomicAdd(o + 0, acc.x);
-        atomicAdd(o + 1, acc.y);
-        atomicAdd(o + 2, acc.z);
-    }
+    vertex_atomic_item<View, CREASED>(L, pin, pout, (int32_t)i, i < L.H);
+}
+
+template <class View, bool CREASED>
+__device__ __forceinline__ f3 vertex_share(const View& L, int32_t h, const float* pin, const float* fpt,
+                                           const float* ept) {
+    return vertex_share_of<View, CREASED>(L, h, pin, fpt, ept);
 }
 
 // ---------------------------------------------------------------------------

@@ -104,7 +104,7 @@ struct CageTables {
     CageCounts n;
 };
 
-inline CageTables make_cage_tables(const DevCage& c) {
+__host__ __device__ inline CageTables make_cage_tables(const DevCage& c) {
     CageTables t;
     t.he = c.he; t.v2h = c.v2h; t.e2h = c.e2h; t.f2h = c.f2h; t.fsz = c.fsz; t.uvs = c.uvs;
     t.n.V = c.V; t.n.F = c.F; t.n.E = c.E; t.n.H = c.H;

@@ -215,6 +215,63 @@ int ccs_AdjointPointsDeviceNoAlloc_cuda(cc_Subd *subd, const float *gradPoints, 
                                         void *stream);
 
 /* ---------------------------------------------------------------------- */
+/* Batched refinement (no reference counterpart).                          */
+/*                                                                         */
+/* Many cages, each with its own depth, refined together: for every depth  */
+/* one persistent cooperative kernel covers all cages still active at that */
+/* depth, and each operation is replayed as one CUDA graph.  Every cage     */
+/* keeps the single-mesh layout inside batch-wide device buffers (see      */
+/* ccs_BatchCageInfo_cuda for its offsets).  Scatter rules only, 16-byte    */
+/* records; atomic vertex sums.                                             */
+/* ---------------------------------------------------------------------- */
+typedef struct ccs_Batch ccs_Batch;
+typedef struct {
+    void *halfedges;          /* all cages' records (16 B)                   */
+    cc_Crease *creases;
+    float *points;            /* refined points, all cages, all depths       */
+    float *cagePoints;        /* input cage points, all cages                */
+    float *gradPoints;        /* adjoint input (consumed by the adjoint)     */
+    float *gradCagePoints;    /* adjoint output                              */
+    int64_t halfedgeCount, creaseCount, pointCount, cagePointCount;
+} ccs_BatchArrays;
+typedef struct {
+    int32_t depth;
+    int64_t cagePointOffset, cagePointCount;   /* in cagePoints / gradCagePoints */
+    int64_t halfedgeOffset, halfedgeCount;
+    int64_t creaseOffset, creaseCount;
+    int64_t pointOffset, pointCount;           /* in points / gradPoints         */
+    int64_t finestPointOffset, finestPointCount;
+} ccs_BatchCageInfo;
+
+/* Uploads `count` cages (validated; each must satisfy the twin relation
+ * vertex(twin(h)) == vertex(next(h))) and sizes every buffer. */
+int ccs_BatchCreate_cuda(const cc_Mesh *const *cages, const int32_t *depths, int32_t count,
+                         uint32_t flags, ccs_Batch **out);
+void ccs_BatchRelease_cuda(ccs_Batch *batch);
+/* Topology, creases, UVs and points of every cage; mode CCS_POINTS_SCATTER
+ * or CCS_POINTS_NOCREASES_SCATTER. */
+int ccs_BatchRefine_cuda(ccs_Batch *batch, int mode);
+/* Points only, from the batch's cagePoints buffer (topology refined before). */
+int ccs_BatchRefinePoints_cuda(ccs_Batch *batch, int mode);
+/* Adjoint of the scatter rule: gradPoints (consumed) -> gradCagePoints. */
+int ccs_BatchAdjointPoints_cuda(ccs_Batch *batch);
+int ccs_BatchGetArrays_cuda(ccs_Batch *batch, ccs_BatchArrays *out);
+int ccs_BatchCageInfo_cuda(const ccs_Batch *batch, int32_t cage, ccs_BatchCageInfo *out);
+int ccs_BatchSetStream_cuda(ccs_Batch *batch, void *stream);
+/* Persistent grid size: resident blocks per SM (0 = all that fit). */
+int ccs_BatchSetSchedule_cuda(ccs_Batch *batch, int32_t blocksPerSM);
+/* Waits for the batch's stream; CCS_ERR_TIMEOUT if a grid barrier gave up. */
+int ccs_BatchSynchronize_cuda(ccs_Batch *batch);
+/* Copies one cage's hierarchy into the host arrays of a cc_Subd made for
+ * the same cage and depth (e.g. by the reference's ccs_Create). */
+int ccs_BatchDownload_cuda(ccs_Batch *batch, int32_t cage, cc_Subd *subd);
+/* Self-test of the bounded grid-barrier wait the batched kernels use: runs a
+ * one-block barrier that waits for an arrival that never comes.  Returns
+ * CCS_ERR_TIMEOUT when the wait gave up and reported as designed (the
+ * expected result; the CUDA context stays usable), CCS_OK if it did not. */
+int ccs_BarrierTimeoutSelfTest_cuda(void);
+
+/* ---------------------------------------------------------------------- */
 /* Counts (int64, with the int32 overflow check the library applies)       */
 /* ---------------------------------------------------------------------- */
 typedef struct {

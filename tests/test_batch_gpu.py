@@ -1,0 +1,108 @@
+"""Batched refinement: every cage of a batch against the single-mesh path and
+the oracle (topology bit-exact, points within 1e-5), the batched adjoint
+against the single-mesh adjoint, the autograd function, the bounded
+grid-barrier wait, and the autotuner's cache."""
+import numpy as np
+import pytest
+
+from conftest import gpu_available, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def built():
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+    from halfedgecatmullclark_b200 import build
+    build.build()
+
+
+@pytest.fixture(scope="module")
+def workloads():
+    from halfedgecatmullclark_b200 import configs
+    ws = configs.batch_cages(count=20, fmin=20, fmax=400, dmin=1, dmax=4, seed=3)
+    ws.append(configs.mixed_torus(nu=10, nv=8, strip=3, depth=3, seed=4))        # with UVs
+    ws.append(configs.torus_quads(nu=8, nv=6, depth=4))
+    return ws
+
+
+def test_batch_refine_matches_oracle(workloads):
+    from halfedgecatmullclark_b200.batch import Batch
+    from oracle import oracle
+    with Batch([w.cage for w in workloads], [w.depth for w in workloads]) as b:
+        b.refine()
+        b.synchronize()
+        for i, w in enumerate(workloads):
+            he, cr, pts = b.download(i)
+            ohe, ocr, opts = oracle.refine(w.cage, w.depth, "scatter")
+            cols = 4 if w.cage.U > 0 else 3
+            assert np.array_equal(he[:, :cols], ohe[:, :cols]), w.name
+            assert np.array_equal(cr.view(np.uint8), ocr.view(np.uint8)), w.name
+            assert rel_err(pts, opts) <= 1e-5, w.name
+
+
+def test_batch_points_and_adjoint_match_single_mesh(workloads):
+    import torch
+    from halfedgecatmullclark_b200.batch import Batch
+    from halfedgecatmullclark_b200.torch_ext import SubdivisionSurface, refine_points
+    rng = np.random.default_rng(5)
+    with Batch([w.cage for w in workloads], [w.depth for w in workloads]) as b:
+        b.refine()
+        arr = b.arrays()
+        newp = [(w.cage.vertex_points + rng.normal(0, 0.02, w.cage.vertex_points.shape)).astype(np.float32)
+                for w in workloads]
+        for i in range(len(workloads)):
+            arr["cage_points"][b.cage_slice(i)] = torch.tensor(newp[i], device="cuda")
+        b.set_stream(torch.cuda.current_stream())
+        b.refine_points()
+        grads = torch.randn_like(arr["points"])
+        arr["grad_points"].copy_(grads)
+        b.adjoint()
+        b.synchronize()
+        for i, w in enumerate(workloads):
+            s = SubdivisionSurface(w.cage, w.depth)
+            x = torch.tensor(newp[i], device="cuda", requires_grad=True)
+            p = refine_points(x, s.subd)
+            assert rel_err(arr["points"][b.point_slice(i)].cpu().numpy(), p.detach().cpu().numpy()) <= 1e-5
+            p.backward(grads[b.point_slice(i)])
+            assert rel_err(arr["grad_cage_points"][b.cage_slice(i)].cpu().numpy(), x.grad.cpu().numpy()) <= 1e-5
+
+
+def test_batch_autograd(workloads):
+    import torch
+    from halfedgecatmullclark_b200 import batch as B
+    with B.Batch([w.cage for w in workloads], [w.depth for w in workloads]) as b:
+        b.refine()
+        x0 = torch.cat([torch.tensor(w.cage.vertex_points) for w in workloads]).cuda()
+        x = x0.clone().requires_grad_(True)
+        pts = B.refine_points(x, b)
+        loss = (pts ** 2).sum()
+        loss.backward()
+        # the same through two independent forwards (linearity): d/dx sum p^2 = 2 S^T S x
+        x2 = x0.clone().requires_grad_(True)
+        pts2 = B.refine_points(x2, b)
+        (2.0 * pts2.detach() * pts2).sum().backward()
+        assert rel_err(x.grad.cpu().numpy(), x2.grad.cpu().numpy()) <= 1e-5
+
+
+def test_bounded_barrier_wait_reports_timeout(workloads):
+    from halfedgecatmullclark_b200 import _native as N
+    from halfedgecatmullclark_b200.batch import Batch
+    L = N.lib()
+    assert L.ccs_BarrierTimeoutSelfTest_cuda() == -5      # gave up and reported
+    # the context is still usable
+    with Batch([w.cage for w in workloads[:3]], [w.depth for w in workloads[:3]]) as b:
+        b.refine()
+        b.synchronize()
+
+
+def test_autotune_writes_and_reuses_cache(workloads, tmp_path, monkeypatch):
+    from halfedgecatmullclark_b200 import batch as B
+    monkeypatch.setenv("CCS_AUTOTUNE_CACHE", str(tmp_path / "tune.json"))
+    with B.Batch([w.cage for w in workloads], [w.depth for w in workloads]) as b:
+        b.refine()
+        first = B.autotune(b, candidates=(0, 1, 2), iters=2)
+        assert not first["cached"] and (tmp_path / "tune.json").exists()
+        again = B.autotune(b, candidates=(0, 1, 2), iters=2)
+        assert again["cached"] and again["blocks_per_sm"] == first["blocks_per_sm"]
