@@ -54,7 +54,7 @@ def test_dot_product_identity(small_workloads):
     y = torch.randn((s.subd.cumV, 3), device="cuda", generator=gen)
     p = refine_points(x, s.subd)
     (p * y).sum().backward()
-    lhs = float((p.double() * y.double()).sum())
+    lhs = float((p.detach().double() * y.double()).sum())
     rhs = float((x.detach().double() * x.grad.double()).sum())
     assert abs(lhs - rhs) <= 1e-5 * max(1.0, abs(lhs))
 
