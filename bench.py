@@ -356,7 +356,8 @@ def run_batch_workload(args):
     tb.record(stream)
     bt.synchronize()
     topo_ms = ta.elapsed_time(tb)
-    tune = B.autotune(bt, use_cache=False, iters=2)
+    tune = B.autotune(bt, use_cache=False, iters=2, stream=stream)
+    bt.set_stream(stream)
     arr = bt.arrays()
     G = torch.cat(grads)          # the batch stores cages one after the other
     del grads

@@ -187,10 +187,11 @@ def _key(batch: Batch) -> str:
     return "%s|cages=%d|halfedges=%d|maxdepth=%d" % (name, len(batch), sh, max(batch.depths))
 
 
-def time_fwd_adj(batch: Batch, iters: int = 5) -> float:
-    """Mean ms of one forward (points) + adjoint, CUDA events on the batch's stream."""
+def time_fwd_adj(batch: Batch, iters: int = 5, stream=None) -> float:
+    """Mean ms of one forward (points) + adjoint, CUDA events on `stream`
+    (default: the current torch stream), which the batch is bound to."""
     import torch
-    s = torch.cuda.current_stream()
+    s = stream if stream is not None else torch.cuda.current_stream()
     batch.set_stream(s)
     batch.refine_points()
     batch.adjoint()
@@ -206,8 +207,10 @@ def time_fwd_adj(batch: Batch, iters: int = 5) -> float:
     return a.elapsed_time(b) / iters
 
 
-def autotune(batch: Batch, candidates=(0, 1, 2, 3, 4, 6, 8), iters: int = 5, use_cache: bool = True) -> dict:
-    """Choose resident blocks per SM for the persistent kernels."""
+def autotune(batch: Batch, candidates=(0, 1, 2, 3, 4, 6, 8), iters: int = 5, use_cache: bool = True,
+             stream=None) -> dict:
+    """Choose resident blocks per SM for the persistent kernels (timed on
+    `stream`, default the current torch stream; the batch stays bound to it)."""
     path = cache_path()
     key = _key(batch)
     cache = {}
@@ -223,7 +226,7 @@ def autotune(batch: Batch, candidates=(0, 1, 2, 3, 4, 6, 8), iters: int = 5, use
     results = {}
     for c in candidates:
         batch.set_schedule(c)
-        results[c] = time_fwd_adj(batch, iters)
+        results[c] = time_fwd_adj(batch, iters, stream)
     best = min(results, key=results.get)
     batch.set_schedule(best)
     entry = {"blocks_per_sm": best, "ms": results[best], "tried": {str(k): v for k, v in results.items()}}

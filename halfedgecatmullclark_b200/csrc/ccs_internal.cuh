@@ -261,7 +261,45 @@ struct RingStats {
     int32_t fwd;
 };
 template <class View>
+__device__ __forceinline__ RingStats creased_ring_walk(const View& L, int32_t h);
+
+// On a quad level the vertex of halfedge h (child h&3 of a parent halfedge)
+// is known: child 2 sits on a face centre (valence = the parent face's size,
+// every incident edge crease-free), children 1 and 3 on an edge midpoint
+// (valence 4, or 2 on a boundary; the only creased edges are the two halves
+// e, e^1 of the parent edge).  Sharpness at depth >= 1 is +0, positive or
+// NaN, so the walk's sums of these values with zeros are exactly the sums
+// below.  Returns false for child 0 (an older vertex: walk its ring).
+template <int RW>
+__device__ __forceinline__ bool quad_ring_known(const QuadView<RW>& L, int32_t h, RingStats& r) {
+    const int k = h & 3;
+    if (k == 0) return false;
+    if (k == 2) {
+        const int32_t n = L.d == 1 ? L.t.fsz[L.t.he[(int64_t)CH_WORDS * (h >> 2) + CH_FACE]] : 4;
+        r.valence = (float)n; r.creaseCount = 0.0f; r.avgS = 0.0f; r.fwd = h;
+        return true;
+    }
+    const int32_t eh = k == 1 ? L.edge(h - 1) : L.edge(h);      // a half of the parent edge
+    const bool bnd = (k == 1 ? L.twin(h - 1) : L.twin(h)) < 0;
+    const float sa = L.sharp(eh), sb = L.sharp(eh ^ 1);
+    const bool own = k == 3;                                     // the walk skips h's own edge
+    r.valence = bnd ? 2.0f : 4.0f;
+    r.avgS = (bnd && own) ? sb : fadd(sa, sb);
+    r.creaseCount = (bnd && own) ? fsign(sb) : fadd(fsign(sa), fsign(sb));
+    r.fwd = bnd ? -1 : h;
+    return true;
+}
+__device__ __forceinline__ bool quad_ring_known(const CageView&, int32_t, RingStats&) { return false; }
+
+template <class View>
 __device__ __forceinline__ RingStats creased_ring(const View& L, int32_t h) {
+    RingStats r;
+    if (quad_ring_known(L, h, r)) return r;
+    return creased_ring_walk(L, h);
+}
+
+template <class View>
+__device__ __forceinline__ RingStats creased_ring_walk(const View& L, int32_t h) {
     RingStats r;
     const int32_t prev = L.prev(h);
     const float prevS = L.hsharp(prev);
@@ -332,11 +370,17 @@ template <class View>
 __device__ __forceinline__ f3 smooth_vertex_share(const View& L, int32_t h, const float* __restrict__ pin,
                                                   const float* __restrict__ fpt, const float* __restrict__ ept) {
     int32_t valence = 1, fwd, bwd, guard = 0;
-    for (fwd = L.prev_vertex_he(h); fwd >= 0 && fwd != h && guard < kWalkCap; fwd = L.prev_vertex_he(fwd), ++guard)
-        ++valence;
-    guard = 0;
-    for (bwd = L.next_vertex_he(h); fwd < 0 && bwd >= 0 && bwd != h && guard < kWalkCap; bwd = L.next_vertex_he(bwd), ++guard)
-        ++valence;
+    RingStats known;
+    if (quad_ring_known(L, h, known)) {      // the valence and boundary are all this rule uses
+        valence = (int32_t)known.valence;
+        fwd = known.fwd;
+    } else {
+        for (fwd = L.prev_vertex_he(h); fwd >= 0 && fwd != h && guard < kWalkCap; fwd = L.prev_vertex_he(fwd), ++guard)
+            ++valence;
+        guard = 0;
+        for (bwd = L.next_vertex_he(h); fwd < 0 && bwd >= 0 && bwd != h && guard < kWalkCap; bwd = L.next_vertex_he(bwd), ++guard)
+            ++valence;
+    }
     const f3 v = ld3(pin + 3 * (int64_t)L.vert(h));
     const f3 f = ld3(fpt + 3 * (int64_t)L.face(h));
     const f3 e = ld3(ept + 3 * (int64_t)L.edge(h));
