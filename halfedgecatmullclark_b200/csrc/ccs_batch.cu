@@ -9,9 +9,11 @@
 // stride over the tiles of one phase, meet at a grid barrier, and go on
 // with the next phase:
 //
-//   forward, d = 0:  cage topology + creases + face points + clearing,
-//                    | edge points | vertex points (atomics)
-//   forward, d >= 1: kernel A tiles + crease tiles | kernel B tiles
+//   forward, d = 0:  cage topology + creases + face points | edge points
+//                    | vertex points (one thread per vertex, sorted ring)
+//   forward, d = 1:  kernel A tiles + crease tiles | vertex points (sorted ring)
+//   forward, d >= 2: kernel A tiles + crease tiles | older vertices + kernel B tiles
+//   (every vertex point summed in the reference's one-thread order: no atomics)
 //   adjoint, each d: edge gathers | face gathers | vertex gathers
 //
 // The tile bodies are the single-mesh ones (ccs_tiles.cuh).  The kernels run
@@ -38,12 +40,12 @@ enum Phase {
     PH_CAGE_TOPO = 0,   // 4 H0 child halfedges
     PH_CAGE_CREASE,     // E0 creases
     PH_CAGE_FACE,       // F0 faces
-    PH_CAGE_ZERO,       // V0 old-vertex slots of depth 1
     PH_CAGE_EDGE,       // H0 halfedges
-    PH_CAGE_VERT,       // H0 halfedges
+    PH_CAGE_VERT,       // V0 vertices
     PH_A,               // H_d parent halfedges
     PH_A_CREASE,        // C_d creases
-    PH_B,               // H_d halfedges
+    PH_V,               // d >= 2: V_(d-1) older vertices
+    PH_B,               // d = 1: V_1 vertices; d >= 2: H_d halfedges
     PH_ADJ_EDGE,        // H_d
     PH_ADJ_FACE,        // F_d
     PH_ADJ_VERT,        // V_d
@@ -182,10 +184,6 @@ k_batch_forward(BatchArgs a, int d) {
             face_point_item<CageView, false>(batch_cage_view(bc), a.cagePts + 3 * bc.cagePt,
                                              a.pts + 3 * (bc.pt + bc.lv[1].ptOff), (int32_t)i);
         });
-        for_tiles(a, 0, PH_CAGE_ZERO, [&](const BatchCage& bc, int64_t lt) {
-            const int64_t i = lt * kBatchBlock + tid;
-            if (i < bc.cage.V) st3(a.pts + 3 * (bc.pt + bc.lv[1].ptOff + i), zero3());
-        });
         if (!grid_sync(a.sync, a.spinCap, gridDim.x)) return;
         for_tiles(a, 0, PH_CAGE_EDGE, [&](const BatchCage& bc, int64_t lt) {
             const int64_t i = lt * kBatchBlock + tid;
@@ -196,9 +194,9 @@ k_batch_forward(BatchArgs a, int d) {
         if (!grid_sync(a.sync, a.spinCap, gridDim.x)) return;
         for_tiles(a, 0, PH_CAGE_VERT, [&](const BatchCage& bc, int64_t lt) {
             const int64_t i = lt * kBatchBlock + tid;
-            vertex_atomic_item<CageView, CREASED>(batch_cage_view(bc), a.cagePts + 3 * bc.cagePt,
-                                                  a.pts + 3 * (bc.pt + bc.lv[1].ptOff), (int32_t)i,
-                                                  i < bc.cage.H);
+            if (i < bc.cage.V)
+                vertex_det_item<CageView, CREASED>(batch_cage_view(bc), a.cagePts + 3 * bc.cagePt,
+                                                   a.pts + 3 * (bc.pt + bc.lv[1].ptOff), (int32_t)i);
         });
         return;
     }
@@ -212,7 +210,6 @@ k_batch_forward(BatchArgs a, int d) {
         la.pin = a.pts + 3 * (bc.pt + lv.ptOff);
         la.pout = a.pts + 3 * (bc.pt + bc.lv[d + 1].ptOff);
         la.H = lv.H; la.V = lv.V; la.F = lv.F; la.E = lv.E; la.C = lv.C;
-        la.zeroV = 1;
         if (bc.uv) tile_level_a<kBatchBlock, 4, TOPO, true, true, CREASED>(la, lt * kBatchBlock, tile);
         else tile_level_a<kBatchBlock, 4, TOPO, false, true, CREASED>(la, lt * kBatchBlock, tile);
         __syncthreads();   // the tile's shared memory is reused by the next tile
@@ -225,12 +222,24 @@ k_batch_forward(BatchArgs a, int d) {
         });
     }
     if (!grid_sync(a.sync, a.spinCap, gridDim.x)) return;
+    if (d >= 2) {
+        for_tiles(a, d, PH_V, [&](const BatchCage& bc, int64_t lt) {
+            const int64_t v = lt * kBatchBlock + tid;
+            if (v < bc.lv[d - 1].V)
+                old_vertex_item<4, CREASED>(batch_quad_view(a, bc, d), a.pts + 3 * (bc.pt + bc.lv[d].ptOff),
+                                            a.pts + 3 * (bc.pt + bc.lv[d + 1].ptOff), (int32_t)v);
+        });
+    }
     for_tiles(a, d, PH_B, [&](const BatchCage& bc, int64_t lt) {
         const QuadView<4> L = batch_quad_view(a, bc, d);
         const float* pin = a.pts + 3 * (bc.pt + bc.lv[d].ptOff);
         float* pout = a.pts + 3 * (bc.pt + bc.lv[d + 1].ptOff);
-        if (d >= 2) tile_level_b<4, CREASED, true>(L, pin, pout, lt * kBatchBlock);
-        else tile_level_b<4, CREASED, false>(L, pin, pout, lt * kBatchBlock);
+        if (d >= 2) {
+            tile_level_b<4, CREASED>(L, pin, pout, lt * kBatchBlock);
+        } else {
+            const int64_t v = lt * kBatchBlock + tid;
+            if (v < L.V) vertex_det_item<QuadView<4>, CREASED>(L, pin, pout, (int32_t)v);
+        }
     });
 }
 
@@ -315,12 +324,12 @@ static int64_t phase_units(const BatchCage& bc, int d, int ph) {
         case PH_CAGE_TOPO: return d == 0 ? 4 * (int64_t)lv.H : 0;
         case PH_CAGE_CREASE: return d == 0 ? lv.E : 0;
         case PH_CAGE_FACE: return d == 0 ? lv.F : 0;
-        case PH_CAGE_ZERO: return d == 0 ? lv.V : 0;
         case PH_CAGE_EDGE: return d == 0 ? lv.H : 0;
-        case PH_CAGE_VERT: return d == 0 ? lv.H : 0;
+        case PH_CAGE_VERT: return d == 0 ? lv.V : 0;
         case PH_A: return d >= 1 ? lv.H : 0;
         case PH_A_CREASE: return d >= 1 ? lv.C : 0;
-        case PH_B: return d >= 1 ? lv.H : 0;
+        case PH_V: return d >= 2 ? bc.lv[d - 1].V : 0;
+        case PH_B: return d == 1 ? lv.V : (d >= 2 ? lv.H : 0);
         case PH_ADJ_EDGE: return lv.H;
         case PH_ADJ_FACE: return lv.F;
         case PH_ADJ_VERT: return lv.V;
@@ -498,9 +507,9 @@ static cudaError_t enqueue_batch(ccs_Batch* b, int op, bool creased) {
     }
     const bool topo = op == BOP_REFINE;
     for (int d = 0; d < b->maxDepth && e == cudaSuccess; ++d) {
-        const int64_t mt = d == 0 ? max_tiles(b, 0, {PH_CAGE_TOPO, PH_CAGE_CREASE, PH_CAGE_FACE, PH_CAGE_ZERO,
-                                                      PH_CAGE_EDGE, PH_CAGE_VERT})
-                                  : max_tiles(b, d, {PH_A, PH_A_CREASE, PH_B});
+        const int64_t mt = d == 0 ? max_tiles(b, 0, {PH_CAGE_TOPO, PH_CAGE_CREASE, PH_CAGE_FACE, PH_CAGE_EDGE,
+                                                      PH_CAGE_VERT})
+                                  : max_tiles(b, d, {PH_A, PH_A_CREASE, PH_V, PH_B});
         if (topo) e = creased ? launch_coop(b, k_batch_forward<true, true>, mt, a, d)
                               : launch_coop(b, k_batch_forward<true, false>, mt, a, d);
         else e = creased ? launch_coop(b, k_batch_forward<false, true>, mt, a, d)

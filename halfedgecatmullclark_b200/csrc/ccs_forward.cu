@@ -176,12 +176,6 @@ k_vertex_atomic(View L, const float* __restrict__ pin, float* __restrict__ pout)
     vertex_atomic_item<View, CREASED>(L, pin, pout, (int32_t)i, i < L.H);
 }
 
-template <class View, bool CREASED>
-__device__ __forceinline__ f3 vertex_share(const View& L, int32_t h, const float* pin, const float* fpt,
-                                           const float* ept) {
-    return vertex_share_of<View, CREASED>(L, h, pin, fpt, ept);
-}
-
 // ---------------------------------------------------------------------------
 // Vertex points, scatter rule summed per vertex in increasing halfedge order
 // ---------------------------------------------------------------------------
@@ -189,56 +183,7 @@ template <class View, bool CREASED>
 __global__ void __launch_bounds__(kBlock)
 k_vertex_det(View L, const float* __restrict__ pin, float* __restrict__ pout) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= L.V) return;
-    const int32_t v = (int32_t)i;
-    const float* fpt = pout + 3 * (int64_t)L.V;
-    const float* ept = pout + 3 * ((int64_t)L.V + L.F);
-    constexpr int kMax = 24;
-    int32_t ring[kMax];
-    int n = 0;
-    const int32_t h0 = L.vert_he(v);
-    int32_t it = h0;
-    do {
-        if (n < kMax) ring[n] = it;
-        ++n;
-        it = L.prev_vertex_he(it);
-    } while (it >= 0 && it != h0 && n < kRingCap);
-    if (it < 0) {
-        for (it = L.next_vertex_he(h0); it >= 0 && it != h0 && n < kRingCap; it = L.next_vertex_he(it)) {
-            if (n < kMax) ring[n] = it;
-            ++n;
-        }
-    }
-    f3 acc = zero3();
-    if (n <= kMax) {
-        for (int a = 1; a < n; ++a) {            // insertion sort, n is small
-            const int32_t x = ring[a];
-            int b = a - 1;
-            while (b >= 0 && ring[b] > x) { ring[b + 1] = ring[b]; --b; }
-            ring[b + 1] = x;
-        }
-        for (int a = 0; a < n; ++a) acc = add3(acc, vertex_share<View, CREASED>(L, ring[a], pin, fpt, ept));
-    } else {
-        // rare high valence: pick ring members in increasing order by walks
-        int32_t last = -1;
-        for (int a = 0; a < n; ++a) {
-            int32_t best = 0x7fffffff;
-            int32_t w = h0;
-            int steps = 0;
-            do {
-                if (w > last && w < best) best = w;
-                w = L.prev_vertex_he(w);
-            } while (w >= 0 && w != h0 && ++steps < kRingCap);
-            if (w < 0) {
-                steps = 0;
-                for (w = L.next_vertex_he(h0); w >= 0 && w != h0 && steps < kRingCap; w = L.next_vertex_he(w), ++steps)
-                    if (w > last && w < best) best = w;
-            }
-            acc = add3(acc, vertex_share<View, CREASED>(L, best, pin, fpt, ept));
-            last = best;
-        }
-    }
-    st3(pout + 3 * (int64_t)v, acc);
+    if (i < L.V) vertex_det_item<View, CREASED>(L, pin, pout, (int32_t)i);
 }
 
 // ---------------------------------------------------------------------------

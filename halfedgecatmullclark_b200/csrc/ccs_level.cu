@@ -15,20 +15,23 @@
 //        halfedge: both halves of the edge rule, the twin face's point
 //        rebuilt from the twin quad's four records (the same value, bit for
 //        bit, as the twin quad's lanes store);
-//      - clears the vertex slots the atomics of kernel B accumulate into;
 //      - extra blocks refine the creases of the level.
-//   B  (one thread per halfedge)
-//      - vertex point share of its halfedge: face and edge points come from
-//        kernel A's output, the ring statistics from the known structure of
-//        refined levels (face centres and edge midpoints need no walk);
-//      - shares of the same vertex are summed inside the warp where the
-//        structure puts them together (a face centre's 4 shares: plain
-//        store, no atomic; an edge midpoint's 2 shares per side: one atomic
-//        triple), other shares go to memory with one float atomic triple.
+//   B  (depth d >= 2; vertex points, no atomics)
+//      - the first blocks take the older vertices (v < V(d-1)), one thread
+//        per vertex: one walk of the ring, every share, summed in
+//        increasing halfedge order;
+//      - the other blocks take one tile of halfedges each, one thread per
+//        halfedge: a face centre's 4 shares meet in 4 lanes of a 16-lane
+//        group and an edge midpoint's 4 shares in the lane of the parent
+//        pair's owner (the twin side's 2 shares rebuilt from face and edge
+//        points), ring statistics from the known structure of refined
+//        levels, sums in increasing halfedge order.
+//   At depth 1 (children of n-gons) the vertex pass is one thread per vertex
+//   with the ring sorted (k_vertex_det).
 //
-// Both kernels evaluate every float expression in the reference's order, so
-// topology, creases, UVs, face and edge points are bit-identical to the
-// reference; vertex points differ only by the order of the atomic sums.
+// Every float expression is evaluated in the reference's order and every sum
+// in its one-thread order, so topology, creases, UVs and all points are
+// bit-identical to the reference's single-threaded refinement.
 //
 // Twin relation used by A: for a twin pair (h, t), vertex(t) = vertex(next h)
 // and vertex(next t) = vertex(h).  The C ABI checks this on the cage (it is
@@ -61,11 +64,19 @@ k_level_a(LevelArgs a) {
     tile_level_a<kBlockL, RW, TOPO, UV, PTS, CREASED>(a, (int64_t)blockIdx.x * kBlockL, tile);
 }
 
-// kernel B: one tile of halfedges per block
-template <int RW, bool CREASED, bool STRUCT>
+// kernel B (d >= 2): blocks [0, nbV) take the older vertices (their walks
+// are the longest-latency work, so they start first), the blocks after them
+// one tile of halfedges each.
+template <int RW, bool CREASED>
 __global__ void __launch_bounds__(kBlockL)
-k_level_b(QuadView<RW> L, const float* __restrict__ pin, float* __restrict__ pout) {
-    tile_level_b<RW, CREASED, STRUCT>(L, pin, pout, (int64_t)blockIdx.x * kBlockL);
+k_level_b(QuadView<RW> L, const float* __restrict__ pin, float* __restrict__ pout, int32_t Vold) {
+    const int nbV = (Vold + kBlockL - 1) / kBlockL;
+    if ((int)blockIdx.x < nbV) {
+        const int64_t v = (int64_t)blockIdx.x * kBlockL + threadIdx.x;
+        if (v < Vold) old_vertex_item<RW, CREASED>(L, pin, pout, (int32_t)v);
+        return;
+    }
+    tile_level_b<RW, CREASED>(L, pin, pout, (int64_t)(blockIdx.x - nbV) * kBlockL);
 }
 
 // ---------------------------------------------------------------------------
@@ -84,7 +95,7 @@ static QuadView<RW> quad_view_l(const Ctx& c, int d) {
 }
 
 template <int RW, bool CREASED>
-static void level_a(const Ctx& c, int d, bool topo, bool uv, const float* pin, float* pout, bool zeroV) {
+static void level_a(const Ctx& c, int d, bool topo, bool uv, const float* pin, float* pout) {
     const Level& lv = c.lv[d];
     LevelArgs a;
     a.in = c.he + (int64_t)RW * lv.heOff;
@@ -94,7 +105,6 @@ static void level_a(const Ctx& c, int d, bool topo, bool uv, const float* pin, f
     a.pin = pin;
     a.pout = pout;
     a.H = lv.H; a.V = lv.V; a.F = lv.F; a.E = lv.E; a.C = lv.C;
-    a.zeroV = zeroV ? 1 : 0;
     const unsigned nb = nblocksL(lv.H) + (topo ? nblocksL(lv.C) : 0u);
     c.prof->begin(c.stream, topo ? CCS_K_LEVEL_FUSED : CCS_K_FACE_POINTS, d, lv.H);
     if (topo) {
@@ -109,10 +119,10 @@ static void level_a(const Ctx& c, int d, bool topo, bool uv, const float* pin, f
 template <int RW, bool CREASED>
 static void level_b(const Ctx& c, int d, const float* pin, float* pout) {
     const QuadView<RW> L = quad_view_l<RW>(c, d);
+    const int32_t Vold = c.lv[d - 1].V;
     c.prof->begin(c.stream, CCS_K_LEVEL_POINTS, d, L.H);
-    const unsigned nb = nblocksL(L.H);
-    if (d >= 2) k_level_b<RW, CREASED, true><<<nb, kBlockL, 0, c.stream>>>(L, pin, pout);
-    else k_level_b<RW, CREASED, false><<<nb, kBlockL, 0, c.stream>>>(L, pin, pout);
+    const unsigned nb = nblocksL(Vold) + nblocksL(L.H);
+    k_level_b<RW, CREASED><<<nb, kBlockL, 0, c.stream>>>(L, pin, pout, Vold);
     c.prof->end(c.stream);
 }
 
@@ -126,8 +136,8 @@ static cudaError_t fused_levels(const Ctx& c, bool topo, bool uv, float* pts, bo
     for (int d = 1; d < c.D; ++d) {
         const float* pin = pts + 3 * c.lv[d].ptOff;
         float* pout = pts + 3 * c.lv[d + 1].ptOff;
-        level_a<RW, CREASED>(c, d, topo, uv, pin, pout, !det);
-        if (det) {
+        level_a<RW, CREASED>(c, d, topo, uv, pin, pout);
+        if (det || d == 1) {
             const cudaError_t e = run_vertex_det_level(c, d, pin, pout, CREASED);
             if (e != cudaSuccess) return e;
         } else {
@@ -137,10 +147,12 @@ static cudaError_t fused_levels(const Ctx& c, bool topo, bool uv, float* pts, bo
     return cudaGetLastError();
 }
 
+// `det` selects the one-thread-per-vertex sorted pass (k_vertex_det) at every
+// depth; either way the sums follow the reference's one-thread order.
 cudaError_t run_fused(const Ctx& c, bool topo, const float* cagePts, float* pts, int mode, bool det) {
     const bool creased = mode == CCS_POINTS_SCATTER;
     const bool uv = c.cage->U > 0 && c.rw == 4;
-    cudaError_t e = run_cage_step(c, topo, uv, cagePts, pts + 3 * c.lv[1].ptOff, mode, det);
+    cudaError_t e = run_cage_step(c, topo, uv, cagePts, pts + 3 * c.lv[1].ptOff, mode, true);
     if (e != cudaSuccess) return e;
     if (c.rw == 4) return creased ? fused_levels<4, true>(c, topo, uv, pts, det) : fused_levels<4, false>(c, topo, uv, pts, det);
     return creased ? fused_levels<3, true>(c, topo, false, pts, det) : fused_levels<3, false>(c, topo, false, pts, det);

@@ -114,7 +114,6 @@ struct LevelArgs {
     const float* __restrict__ pin;      // depth-d points
     float* __restrict__ pout;           // depth-(d+1) points
     int32_t H, V, F, E, C;              // depth-d counts
-    int zeroV;                          // clear the old-vertex slots (atomic path)
 };
 
 // `tile` is BLOCK * 4 * RW ints of shared memory; every thread of the block
@@ -173,7 +172,6 @@ __device__ __forceinline__ void tile_level_a(const LevelArgs& a, int64_t h0, int
         const f3 Fp = quad_face_point(p, qb);
         const f3 pn = shfl3(p, ln);
         if (valid && k == 0) st3(a.pout + 3 * ((int64_t)a.V + f), Fp);
-        if (a.zeroV && h64 < a.V) st3(a.pout + 3 * h64, zero3());
         // edge point, by the pair's larger halfedge; the smaller one's share
         // is added first, as a one-thread reference run adds it
         if (valid && h > tw) {
@@ -206,19 +204,90 @@ __device__ __forceinline__ void tile_level_a(const LevelArgs& a, int64_t h0, int
 }
 
 // ---------------------------------------------------------------------------
-// quad level, kernel B body: vertex shares of halfedges [h0, h0 + blockDim)
+// Vertex rule of quad levels for one halfedge's share (creased rule in the
+// corner-first branch order :2567-2607, crease-free rule :2307-2351), given
+// the ring statistics the reference's walk from that halfedge finds
+// (:2523-2566): vpre = valence before the boundary adjustment, cpre = crease
+// count, avgS = summed sharpness, bnd = the walk met a boundary; cw / pcw =
+// crease signs of the halfedge's edge and of its prev's edge, Ep = edge
+// point of its prev's edge (read on a boundary only).
 // ---------------------------------------------------------------------------
-// STRUCT: depth >= 2, where a 16-lane group holds the 16 children of one
-// parent quad face, so a face centre's 4 shares sit in lanes 2, 6, 10, 14 and
-// an edge midpoint's shares from this face in lanes 4j+1 and 4(j+1 mod 4)+3.
-template <int RW, bool CREASED, bool STRUCT>
+template <bool CREASED>
+__device__ __forceinline__ f3 quad_vertex_rule(f3 p, f3 F, f3 E, f3 Ep, float vpre, float cpre, float avgS,
+                                               bool bnd, float cw, float pcw) {
+    f3 s;
+    if (CREASED) {
+        const float valence = bnd ? fadd(vpre, 1.0f) : vpre;
+        const float creaseCount = bnd ? fadd(cpre, cw) : cpre;
+        if (creaseCount >= 3.0f || valence == 2.0f) {
+            s = mul3(p, frcp(vpre));
+        } else if (creaseCount <= 1.0f) {
+            f3 smooth = add3(mul3(F, -1.0f), mul3(E, 4.0f));
+            smooth = add3(smooth, mul3(p, fsub(vpre, 3.0f)));
+            s = mul3(smooth, frcp(fmul(vpre, vpre)));
+        } else {
+            const f3 corner = mul3(p, frcp(vpre));
+            f3 crease = add3(mul3(p, fmul(0.25f, cw)), mul3(E, fmul(0.25f, cw)));
+            if (bnd) crease = add3(crease, add3(mul3(p, fmul(0.25f, pcw)), mul3(Ep, fmul(0.25f, pcw))));
+            s = lerp3(corner, crease, fsat(fmul(avgS, 0.5f)));
+        }
+    } else {
+        const float w = frcp(vpre);
+        const float ws = fmul(w, bnd ? 0.0f : 1.0f);
+        s.x = fmul(w, fadd(p.x, fmul(ws, fsub(fsub(fmul(4.0f, E.x), F.x), fmul(3.0f, p.x)))));
+        s.y = fmul(w, fadd(p.y, fmul(ws, fsub(fsub(fmul(4.0f, E.y), F.y), fmul(3.0f, p.y)))));
+        s.z = fmul(w, fadd(p.z, fmul(ws, fsub(fsub(fmul(4.0f, E.z), F.z), fmul(3.0f, p.z)))));
+    }
+    return s;
+}
+
+__device__ __forceinline__ f3 shfl_down3(f3 v, int d) {
+    return f3{__shfl_down_sync(0xffffffffu, v.x, d), __shfl_down_sync(0xffffffffu, v.y, d),
+              __shfl_down_sync(0xffffffffu, v.z, d)};
+}
+
+// Order two (id, share) pairs by id.
+__device__ __forceinline__ void order2(int32_t& ia, f3& sa, int32_t& ib, f3& sb) {
+    if (ib < ia) {
+        const int32_t ti = ia; ia = ib; ib = ti;
+        const f3 ts = sa; sa = sb; sb = ts;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// quad level d >= 2, kernel B body: face-centre and edge-midpoint vertex
+// points of depth d+1 from the halfedges [h0, h0 + blockDim) of depth d.
+// ---------------------------------------------------------------------------
+// At depth d >= 2 halfedge h = 16 f + 4 j + k is child k of parent halfedge
+// g = 4 f + j of the parent quad f, and a 16-lane group holds the 16 children
+// of f.  Vertex(h) is known from k:
+//   k = 2: the centre of f; its four shares are lanes 2, 6, 10, 14 of the
+//          group, in increasing halfedge order;
+//   k = 1, 3: the midpoint of a parent edge (valence 4, or 2 on a boundary;
+//          its only creased edges are the two halves e, e^1 of the parent
+//          edge).  Its shares are child 1 of g and child 3 of next(g), here,
+//          and child 1 of t = twin(g) and child 3 of next(t) in t's group.
+//          The lane of child 1 of the pair's owner (g > t, or t < 0) sums
+//          all of them: the twin side's two shares are rebuilt from face and
+//          edge points alone, since their ring statistics equal this side's;
+//   k = 0: an older vertex; old_vertex_item takes those.
+// Every vertex is summed by one thread in increasing halfedge order, starting
+// from zero, so the result is bit-identical to the reference's one-thread
+// scatter loop (:2496-2615) and needs neither atomics nor cleared slots.
+// Sharpness at depth >= 1 is +0 or positive, so the structural sums of
+// sharpness equal the walk's, zeros and order notwithstanding.
+// Requires H to be a multiple of 16 (true at depth >= 2) and blockDim a
+// multiple of 32 with h0 a multiple of 32.
+template <int RW, bool CREASED>
 __device__ __forceinline__ void tile_level_b(const QuadView<RW>& L, const float* __restrict__ pin,
                                              float* __restrict__ pout, int64_t h0) {
+    const unsigned full = 0xffffffffu;
     const int tid = threadIdx.x, lane = tid & 31;
     const int64_t h64 = h0 + tid;
     const bool valid = h64 < L.H;
     const int32_t h = (int32_t)h64;
     const int k = lane & 3, qb = lane & ~3, lp = qb | ((k + 3) & 3);
+    const int gb = lane & ~15, j = (lane >> 2) & 3;
     const float* fpt = pout + 3 * (int64_t)L.V;
     const float* ept = pout + 3 * ((int64_t)L.V + L.F);
     int32_t tw = -1, ed = 0, vx = 0;
@@ -232,31 +301,28 @@ __device__ __forceinline__ void tile_level_b(const QuadView<RW>& L, const float*
             vx = __ldg(L.he + 3 * h64 + 2);
         }
     }
+    // child 0 of g: twin = 4 next(t) + 3 (negative on a boundary), edge = 2 e + (g > t ? 0 : 1)
+    const int32_t tw0 = __shfl_sync(full, tw, qb);
+    const int32_t ed0 = __shfl_sync(full, ed, qb);
+    const int32_t ed0p = __shfl_sync(full, ed, gb | (((j + 3) & 3) << 2));   // child 0 of prev(g)
+    const bool ownG = (ed0 & 1) == 0, ownPrev = (ed0p & 1) == 0;
+    const bool need = k == 2 || (k == 3 ? ownPrev : ownG);
     f3 p = zero3(), Fh = zero3(), Eh = zero3();
-    if (valid) {
-        p = ld3(pin + 3 * (int64_t)vx);
-        Fh = ld3(fpt + 3 * (int64_t)(h >> 2));
-        Eh = ld3(ept + 3 * (int64_t)ed);
+    if (valid && need) {
+        Eh = ld3(ept + 3 * (int64_t)ed);              // k = 0: E of child 0, the twin side's or prev's edge point
+        if (k != 0) {
+            p = ld3(pin + 3 * (int64_t)vx);
+            Fh = ld3(fpt + 3 * (int64_t)(h >> 2));
+        }
     }
-    const f3 Ep = shfl3(Eh, lp);                         // edge point of prev(h)
-    const int32_t ped = __shfl_sync(0xffffffffu, ed, lp);
-    const int32_t ptw = __shfl_sync(0xffffffffu, tw, lp);
+    const f3 Ep = shfl3(Eh, lp);                      // edge point of prev(h)'s edge
+    const int32_t ped = __shfl_sync(full, ed, lp);
+    const int32_t ptw = __shfl_sync(full, tw, lp);
     f3 s = zero3();
-    if (valid) {
-        // Ring statistics of vertex(h) as the reference's walk from h finds
-        // them (:2523-2566).  At a refined level the vertex of child k of a
-        // parent halfedge is known: k = 2 is a face centre (valence = parent
-        // face size, all edges crease-free), k = 1 and 3 are edge midpoints
-        // (valence 4, or 2 on a boundary; the creased edges are the two halves
-        // e and e^1 of the parent edge), k = 0 is an older vertex that needs
-        // the walk.  Sharpness at depth >= 1 is +0 or positive, so sums with
-        // the crease-free edges' zeros are exact in any order.
-        float vpre, cpre, avgS;
-        bool bnd;
-        if (k == 2) {
-            vpre = L.d == 1 ? (float)L.t.fsz[L.t.he[(int64_t)CH_WORDS * (h >> 2) + CH_FACE]] : 4.0f;
-            cpre = 0.0f; avgS = 0.0f; bnd = false;
-        } else if (k != 0) {
+    float vpre = 4.0f, cpre = 0.0f, avgS = 0.0f;
+    bool bnd = false;
+    if (valid && need && k != 0) {
+        if (k != 2) {
             const int32_t eh = k == 1 ? ped : ed;        // one half of the parent edge
             const float sa = L.sharp(eh), sb = L.sharp(eh ^ 1);
             bnd = (k == 1 ? ptw : tw) < 0;
@@ -264,60 +330,218 @@ __device__ __forceinline__ void tile_level_b(const QuadView<RW>& L, const float*
             const bool own = k == 3;                     // the walk from h skips its own edge
             avgS = (bnd && own) ? sb : fadd(sa, sb);
             cpre = (bnd && own) ? fsign(sb) : fadd(fsign(sa), fsign(sb));
-        } else if (CREASED) {
-            const RingStats r = creased_ring(L, h);
-            vpre = r.valence; cpre = r.creaseCount; avgS = r.avgS; bnd = r.fwd < 0;
-        } else {
-            int32_t valence = 1, fwd, bwd, guard = 0;
-            for (fwd = L.prev_vertex_he(h); fwd >= 0 && fwd != h && guard < kWalkCap; fwd = L.prev_vertex_he(fwd), ++guard) ++valence;
-            guard = 0;
-            for (bwd = L.next_vertex_he(h); fwd < 0 && bwd >= 0 && bwd != h && guard < kWalkCap; bwd = L.next_vertex_he(bwd), ++guard) ++valence;
-            vpre = (float)valence; cpre = 0.0f; avgS = 0.0f; bnd = fwd < 0;
         }
-        if (CREASED) {
-            // vertex rule, corner-first branch order of quad levels (:2567-2607)
-            const float cw = fsign(L.sharp(ed)), pcw = fsign(L.sharp(ped));
-            const float valence = bnd ? fadd(vpre, 1.0f) : vpre;
-            const float creaseCount = bnd ? fadd(cpre, cw) : cpre;
-            if (creaseCount >= 3.0f || valence == 2.0f) {
-                s = mul3(p, frcp(vpre));
-            } else if (creaseCount <= 1.0f) {
-                f3 smooth = add3(mul3(Fh, -1.0f), mul3(Eh, 4.0f));
-                smooth = add3(smooth, mul3(p, fsub(vpre, 3.0f)));
-                s = mul3(smooth, frcp(fmul(vpre, vpre)));
-            } else {
-                const f3 corner = mul3(p, frcp(vpre));
-                f3 crease = add3(mul3(p, fmul(0.25f, cw)), mul3(Eh, fmul(0.25f, cw)));
-                if (bnd) crease = add3(crease, add3(mul3(p, fmul(0.25f, pcw)), mul3(Ep, fmul(0.25f, pcw))));
-                s = lerp3(corner, crease, fsat(fmul(avgS, 0.5f)));
-            }
-        } else {
-            // crease-free vertex rule (:2307-2351)
-            const float w = frcp(vpre);
-            const float ws = fmul(w, bnd ? 0.0f : 1.0f);
-            s.x = fmul(w, fadd(p.x, fmul(ws, fsub(fsub(fmul(4.0f, Eh.x), Fh.x), fmul(3.0f, p.x)))));
-            s.y = fmul(w, fadd(p.y, fmul(ws, fsub(fsub(fmul(4.0f, Eh.y), Fh.y), fmul(3.0f, p.y)))));
-            s.z = fmul(w, fadd(p.z, fmul(ws, fsub(fsub(fmul(4.0f, Eh.z), Fh.z), fmul(3.0f, p.z)))));
-        }
+        s = quad_vertex_rule<CREASED>(p, Fh, Eh, Ep, vpre, cpre, avgS, bnd, fsign(L.sharp(ed)),
+                                      fsign(L.sharp(ped)));
     }
+    // face centre: lanes 2, 6, 10, 14
+    const f3 s4 = shfl_down3(s, 4), s8 = shfl_down3(s, 8), s12 = shfl_down3(s, 12);
+    // edge midpoint: child 3 of next(g) sits in lanes 4 (j + 1 mod 4) + 3
+    const int partner = gb | (((j + 1) & 3) << 2) | 3;
+    f3 sA2 = shfl3(s, partner);
+    int32_t iA2 = __shfl_sync(full, h, partner);
+    if (!valid) return;
     float* o = pout + 3 * (int64_t)vx;
-    if (STRUCT) {
-        const f3 u = add3(s, shfl_xor3(s, 4));
-        const f3 fsum = add3(u, shfl_xor3(u, 8));       // (s2 + s6) + (s10 + s14)
-        const int partner = (lane & ~15) | ((((lane >> 2) + 1) & 3) << 2) | 3;
-        const f3 pe = shfl3(s, partner);
-        if (valid) {
-            if (k == 2) {
-                if ((lane & 15) == 2) st3(o, fsum);     // all 4 shares of this vertex
-            } else if (k == 1) {
-                atomic_add3(o, add3(s, pe));
-            } else if (k == 0) {
-                atomic_add3(o, s);
+    if ((lane & 15) == 2) {
+        st3(o, add3(add3(add3(add3(zero3(), s), s4), s8), s12));
+    } else if (k == 1 && ownG) {
+        int32_t iA1 = h;
+        f3 sA1 = s;
+        order2(iA1, sA1, iA2, sA2);
+        f3 acc;
+        if (tw0 < 0) {
+            acc = add3(add3(zero3(), sA1), sA2);
+        } else {
+            const int32_t tn = tw0 >> 2;                 // next(t), depth d-1
+            const int32_t t = qprev(tn);
+            const int32_t eB1 = ed - (h >> 2) + t;       // edge of child 1 of t: 2 E(d-1) + t
+            const int32_t eB2 = ed0;                     // edge of child 3 of next(t): 2 e
+            const f3 sB1 = quad_vertex_rule<CREASED>(p, ld3(fpt + 3 * (int64_t)t), ld3(ept + 3 * (int64_t)eB1),
+                                                     zero3(), vpre, cpre, avgS, false, fsign(L.sharp(eB1)), 0.0f);
+            const f3 sB2 = quad_vertex_rule<CREASED>(p, ld3(fpt + 3 * (int64_t)tn), Ep,
+                                                     zero3(), vpre, cpre, avgS, false, fsign(L.sharp(eB2)), 0.0f);
+            int32_t iB1 = 4 * t + 1, iB2 = 4 * tn + 3;
+            f3 b1 = sB1, b2 = sB2;
+            order2(iB1, b1, iB2, b2);
+            // merge the two ordered pairs
+            order2(iA1, sA1, iB1, b1);                   // smallest in A1
+            order2(iA2, sA2, iB2, b2);                   // largest in B2
+            order2(iA2, sA2, iB1, b1);
+            acc = add3(add3(add3(add3(zero3(), sA1), sA2), b1), b2);
+        }
+        st3(o, acc);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// quad level d >= 2: vertex point of an older vertex v < V(d-1).  Its ring
+// members are child-0 halfedges; one thread walks the ring once, gathers the
+// statistics every member's own walk would find (the valence and crease count
+// of the whole ring; the summed sharpness of the ring, or on a boundary of
+// the ring without the member's own edge -- the sum only matters when the
+// count is 2, where it has at most two nonzero terms and is order-free),
+// and sums the shares in increasing halfedge order.  Rings longer than
+// kRingRegs members take the generic sorted path.
+// ---------------------------------------------------------------------------
+static constexpr int kRingRegs = 8;
+
+template <class View, bool CREASED>
+__device__ __forceinline__ f3 vertex_share_of(const View& L, int32_t h, const float* pin, const float* fpt,
+                                              const float* ept);
+
+// Shares of the ring of h0 summed in increasing halfedge order, any view.
+template <class View, bool CREASED>
+__device__ f3 ring_sorted_sum(const View& L, int32_t h0, const float* __restrict__ pin,
+                              const float* __restrict__ fpt, const float* __restrict__ ept) {
+    constexpr int kMax = 24;
+    int32_t ring[kMax];
+    int n = 0;
+    int32_t it = h0;
+    do {
+        if (n < kMax) ring[n] = it;
+        ++n;
+        it = L.prev_vertex_he(it);
+    } while (it >= 0 && it != h0 && n < kWalkCap);
+    if (it < 0) {
+        for (it = L.next_vertex_he(h0); it >= 0 && it != h0 && n < kWalkCap; it = L.next_vertex_he(it)) {
+            if (n < kMax) ring[n] = it;
+            ++n;
+        }
+    }
+    f3 acc = zero3();
+    if (n <= kMax) {
+        for (int a = 1; a < n; ++a) {            // insertion sort, n is small
+            const int32_t x = ring[a];
+            int b = a - 1;
+            while (b >= 0 && ring[b] > x) { ring[b + 1] = ring[b]; --b; }
+            ring[b + 1] = x;
+        }
+        for (int a = 0; a < n; ++a) acc = add3(acc, vertex_share_of<View, CREASED>(L, ring[a], pin, fpt, ept));
+    } else {
+        // rare high valence: pick ring members in increasing order by walks
+        int32_t last = -1;
+        for (int a = 0; a < n; ++a) {
+            int32_t best = 0x7fffffff;
+            int32_t w = h0;
+            int steps = 0;
+            do {
+                if (w > last && w < best) best = w;
+                w = L.prev_vertex_he(w);
+            } while (w >= 0 && w != h0 && ++steps < kWalkCap);
+            if (w < 0) {
+                steps = 0;
+                for (w = L.next_vertex_he(h0); w >= 0 && w != h0 && steps < kWalkCap; w = L.next_vertex_he(w), ++steps)
+                    if (w > last && w < best) best = w;
+            }
+            acc = add3(acc, vertex_share_of<View, CREASED>(L, best, pin, fpt, ept));
+            last = best;
+        }
+    }
+    return acc;
+}
+
+template <int RW, bool CREASED>
+__device__ __forceinline__ void old_vertex_item(const QuadView<RW>& L, const float* __restrict__ pin,
+                                                float* __restrict__ pout, int32_t v) {
+    constexpr int M = kRingRegs;
+    const float* fpt = pout + 3 * (int64_t)L.V;
+    const float* ept = pout + 3 * ((int64_t)L.V + L.F);
+    const int32_t h0 = L.vert_he(v);
+    int32_t id[M], eo[M], ep[M];      // member, its edge, the edge of its prev
+    // forward: x -> twin(prev(x)); edge(prev(x)) is the next member's edge
+    int32_t x = h0, ex = L.edge(h0);
+    bool run = true;
+    int n = 0;
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+        id[i] = 0x7fffffff; eo[i] = 0; ep[i] = 0;
+        if (run) {
+            id[i] = x; eo[i] = ex;
+            const int32_t pr = qprev(x);
+            ex = L.edge(pr);
+            ep[i] = ex;
+            x = L.twin(pr);
+            n = i + 1;
+            run = x >= 0 && x != h0;
+        }
+    }
+    const bool bnd = x < 0;
+    const int32_t eEnd = ex;          // on a boundary: the ring's last edge, no member's own
+    bool over = run;
+    if (bnd) {
+        // backward: b = twin(c), next member next(b); edge(prev(next(b))) = edge(b) = edge(c)
+        int32_t b = L.twin(h0), pe = eo[0];
+#pragma unroll
+        for (int i = 1; i < M; ++i) {
+            if (i >= n && b >= 0) {
+                const int32_t c = qnext(b);
+                id[i] = c; ep[i] = pe;
+                eo[i] = L.edge(c);
+                pe = eo[i];
+                b = L.twin(c);
+                n = i + 1;
             }
         }
-    } else if (valid) {
-        atomic_add3(o, s);
+        over = b >= 0;
     }
+    float* o = pout + 3 * (int64_t)v;
+    if (over) {
+        st3(o, ring_sorted_sum<QuadView<RW>, CREASED>(L, h0, pin, fpt, ept));
+        return;
+    }
+    // sort the members by halfedge id (odd-even transposition; empty slots hold INT_MAX)
+#pragma unroll
+    for (int r = 0; r < M; ++r) {
+#pragma unroll
+        for (int i = r & 1; i + 1 < M; i += 2) {
+            if (id[i + 1] < id[i]) {
+                int32_t t = id[i]; id[i] = id[i + 1]; id[i + 1] = t;
+                t = eo[i]; eo[i] = eo[i + 1]; eo[i + 1] = t;
+                t = ep[i]; ep[i] = ep[i + 1]; ep[i + 1] = t;
+            }
+        }
+    }
+    const f3 p = ld3(pin + 3 * (int64_t)v);
+    const float vpre = (float)n;
+    float sh[M];
+    float tot = 0.0f, cnt = 0.0f;
+    if (CREASED) {
+#pragma unroll
+        for (int i = 0; i < M; ++i) {
+            sh[i] = i < n ? L.sharp(eo[i]) : 0.0f;
+            tot = fadd(tot, sh[i]);
+            cnt = fadd(cnt, fsign(sh[i]));
+        }
+    }
+    const float sEnd = (CREASED && bnd) ? L.sharp(eEnd) : 0.0f;
+    f3 acc = zero3();
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+        if (i < n) {
+            const f3 F = ld3(fpt + 3 * (int64_t)(id[i] >> 2));
+            const f3 E = ld3(ept + 3 * (int64_t)eo[i]);
+            f3 s;
+            if (CREASED) {
+                float avgS = tot, cpre = cnt, pcw = 0.0f;
+                f3 Ep = zero3();
+                if (bnd) {
+                    avgS = sEnd;
+                    cpre = fsign(sEnd);
+#pragma unroll
+                    for (int m = 0; m < M; ++m) {
+                        if (m != i && m < n) { avgS = fadd(avgS, sh[m]); cpre = fadd(cpre, fsign(sh[m])); }
+                    }
+                    pcw = fsign(L.sharp(ep[i]));
+                    Ep = ld3(ept + 3 * (int64_t)ep[i]);
+                }
+                s = quad_vertex_rule<true>(p, F, E, Ep, vpre, cpre, avgS, bnd, fsign(sh[i]), pcw);
+            } else {
+                s = quad_vertex_rule<false>(p, F, E, zero3(), vpre, 0.0f, 0.0f, bnd, 0.0f, 0.0f);
+            }
+            acc = add3(acc, s);
+        }
+    }
+    st3(o, acc);
 }
 
 // ---------------------------------------------------------------------------
@@ -478,6 +702,16 @@ __device__ __forceinline__ void vertex_atomic_item(const View& L, const float* _
         if (k < n) acc = add3(acc, t);
     }
     if (valid && lane == __ffs(grp) - 1) atomic_add3(pout + 3 * (int64_t)v, acc);
+}
+
+// item = vertex v: its shares summed in increasing halfedge order, which is
+// the reference's one-thread scatter order (any view, any depth)
+template <class View, bool CREASED>
+__device__ __forceinline__ void vertex_det_item(const View& L, const float* __restrict__ pin,
+                                                float* __restrict__ pout, int32_t v) {
+    const float* fpt = pout + 3 * (int64_t)L.V;
+    const float* ept = pout + 3 * ((int64_t)L.V + L.F);
+    st3(pout + 3 * (int64_t)v, ring_sorted_sum<View, CREASED>(L, L.vert_he(v), pin, fpt, ept));
 }
 
 // ---------------------------------------------------------------------------

@@ -58,6 +58,15 @@ def gpu_available():
         return False
 
 
+def fusable(cage):
+    """The twin relation the fused level kernels need: vertex(twin h) ==
+    vertex(next h) for every halfedge with a twin (the C ABI's own check)."""
+    he = cage.halfedges
+    tw = he["twinID"]
+    ok = tw >= 0
+    return bool(np.all(he["vertexID"][tw[ok]] == he["vertexID"][he["nextID"][ok]]))
+
+
 def rel_err(a, b):
     a = np.asarray(a, np.float64)
     b = np.asarray(b, np.float64)
