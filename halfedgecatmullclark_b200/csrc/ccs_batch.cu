@@ -46,6 +46,7 @@ enum Phase {
     PH_A_CREASE,        // C_d creases
     PH_V,               // d >= 2: V_(d-1) older vertices
     PH_B,               // d = 1: V_1 vertices; d >= 2: H_d halfedges
+    PH_ADJ_STATS,       // d >= 1: V_(d-1) older vertices (ring statistics)
     PH_ADJ_EDGE,        // H_d
     PH_ADJ_FACE,        // F_d
     PH_ADJ_VERT,        // V_d
@@ -58,6 +59,7 @@ struct BatchCage {
     int32_t uv;          // UV codes are refined
     int64_t cagePt;      // first cage point of this cage in the batch's cage-point buffer
     int64_t he, cr, pt;  // first record / crease / point of this cage's hierarchy
+    int64_t stats;       // first ring-statistics entry of this cage (adjoint)
     Level lv[kMaxBatchDepth + 1];
 };
 
@@ -77,6 +79,7 @@ struct BatchArgs {
     float* pts;
     float* work;                         // adjoint: running gradient per refined point
     float* gradCage;                     // adjoint output
+    float4* stats;                       // adjoint: ring statistics of the older vertices
     GridSync* sync;
     unsigned int spinCap;                // polls before a barrier wait gives up
 };
@@ -247,25 +250,37 @@ __global__ void __launch_bounds__(kBatchBlock)
 k_batch_adjoint(BatchArgs a, int d) {
     const int tid = threadIdx.x;
     auto gnew = [&](const BatchCage& bc) { return a.work + 3 * (bc.pt + bc.lv[d + 1].ptOff); };
+    auto qview = [&](const BatchCage& bc) {
+        QuadView<4> L = batch_quad_view(a, bc, d);
+        L.ostats = a.stats + bc.stats;
+        return L;
+    };
+    if (d >= 1) {
+        for_tiles(a, d, PH_ADJ_STATS, [&](const BatchCage& bc, int64_t lt) {
+            const int64_t i = lt * kBatchBlock + tid;
+            if (i < bc.lv[d - 1].V) ring_stats_item(batch_quad_view(a, bc, d), a.stats + bc.stats, (int32_t)i);
+        });
+        if (!grid_sync(a.sync, a.spinCap, gridDim.x)) return;
+    }
     for_tiles(a, d, PH_ADJ_EDGE, [&](const BatchCage& bc, int64_t lt) {
         const int64_t i = lt * kBatchBlock + tid;
         if (i >= bc.lv[d].H) return;
         if (d == 0) adj_edge_item(batch_cage_view(bc), gnew(bc), (int32_t)i);
-        else adj_edge_item(batch_quad_view(a, bc, d), gnew(bc), (int32_t)i);
+        else adj_edge_item(qview(bc), gnew(bc), (int32_t)i);
     });
     if (!grid_sync(a.sync, a.spinCap, gridDim.x)) return;
     for_tiles(a, d, PH_ADJ_FACE, [&](const BatchCage& bc, int64_t lt) {
         const int64_t i = lt * kBatchBlock + tid;
         if (i >= bc.lv[d].F) return;
         if (d == 0) adj_face_item(batch_cage_view(bc), gnew(bc), (int32_t)i);
-        else adj_face_item(batch_quad_view(a, bc, d), gnew(bc), (int32_t)i);
+        else adj_face_item(qview(bc), gnew(bc), (int32_t)i);
     });
     if (!grid_sync(a.sync, a.spinCap, gridDim.x)) return;
     for_tiles(a, d, PH_ADJ_VERT, [&](const BatchCage& bc, int64_t lt) {
         const int64_t i = lt * kBatchBlock + tid;
         if (i >= bc.lv[d].V) return;
         if (d == 0) adj_vertex_item(batch_cage_view(bc), gnew(bc), a.gradCage + 3 * bc.cagePt, (int32_t)i);
-        else adj_vertex_item(batch_quad_view(a, bc, d), gnew(bc), a.work + 3 * (bc.pt + bc.lv[d].ptOff), (int32_t)i);
+        else adj_vertex_item(qview(bc), gnew(bc), a.work + 3 * (bc.pt + bc.lv[d].ptOff), (int32_t)i);
     });
 }
 
@@ -302,7 +317,8 @@ struct ccs_Batch {
     cc_Crease* cr = nullptr;
     float *pts = nullptr, *work = nullptr, *gradCage = nullptr;
     ccs::GridSync* sync = nullptr;
-    int64_t totH = 0, totC = 0, totV = 0, totCagePts = 0;
+    int64_t totH = 0, totC = 0, totV = 0, totCagePts = 0, totStats = 0;
+    float4* stats = nullptr;                 // adjoint ring statistics (totStats entries)
     cudaStream_t stream = nullptr;
     bool ownStream = false;
     int blocksPerSM = 0;                     // 0 = as many as fit
@@ -330,6 +346,7 @@ static int64_t phase_units(const BatchCage& bc, int d, int ph) {
         case PH_A_CREASE: return d >= 1 ? lv.C : 0;
         case PH_V: return d >= 2 ? bc.lv[d - 1].V : 0;
         case PH_B: return d == 1 ? lv.V : (d >= 2 ? lv.H : 0);
+        case PH_ADJ_STATS: return d >= 1 ? bc.lv[d - 1].V : 0;
         case PH_ADJ_EDGE: return lv.H;
         case PH_ADJ_FACE: return lv.F;
         case PH_ADJ_VERT: return lv.V;
@@ -344,6 +361,7 @@ static void free_batch(ccs_Batch* b) {
     cudaFree(b->cHe); cudaFree(b->cV2h); cudaFree(b->cE2h); cudaFree(b->cF2h); cudaFree(b->cFsz);
     cudaFree(b->cCr); cudaFree(b->cUv); cudaFree(b->cagePts);
     cudaFree(b->he); cudaFree(b->cr); cudaFree(b->pts); cudaFree(b->work); cudaFree(b->gradCage);
+    cudaFree(b->stats);
     cudaFree(b->sync);
     if (b->ownStream && b->stream) cudaStreamDestroy(b->stream);
     delete b;
@@ -389,6 +407,8 @@ static int batch_create(const cc_Mesh* const* cages, const int32_t* depths, int3
         bc.cage.fsz = (int32_t*)(intptr_t)oF;
         bc.cagePt = oV;
         bc.he = b->totH; bc.cr = b->totC; bc.pt = b->totV;
+        bc.stats = b->totStats;                  // entries: max over 1 <= d < D of V(d-1) = V(D-2)
+        b->totStats += D >= 2 ? lv[D - 2].V : 0;
         const Level& last = lv[D];
         b->totH += last.heOff + last.H;
         b->totC += last.crOff + last.C;
@@ -454,11 +474,21 @@ static int batch_create(const cc_Mesh* const* cages, const int32_t* depths, int3
     return CCS_OK;
 }
 
+// gradient of every refined point, of the cage points, and the ring statistics
+static bool adjoint_buffers(ccs_Batch* b) {
+    if (b->work) return true;
+    if (bmalloc(&b->work, 3 * b->totV) && bmalloc(&b->gradCage, 3 * b->totCagePts) && bmalloc(&b->stats, b->totStats))
+        return true;
+    cudaFree(b->work); cudaFree(b->gradCage); cudaFree(b->stats);
+    b->work = nullptr; b->gradCage = nullptr; b->stats = nullptr;
+    return false;
+}
+
 static BatchArgs batch_args(ccs_Batch* b) {
     BatchArgs a;
     a.cages = b->dCages; a.tiles = b->dTiles; a.count = b->count;
     a.he = b->he; a.cr = b->cr; a.cagePts = b->cagePts; a.pts = b->pts;
-    a.work = b->work; a.gradCage = b->gradCage; a.sync = b->sync;
+    a.work = b->work; a.gradCage = b->gradCage; a.stats = b->stats; a.sync = b->sync;
     a.spinCap = kSpinCap;
     return a;
 }
@@ -500,7 +530,7 @@ static cudaError_t enqueue_batch(ccs_Batch* b, int op, bool creased) {
     if (op == BOP_ADJOINT) {
         e = cudaMemsetAsync(b->gradCage, 0, sizeof(float) * 3 * (size_t)b->totCagePts, b->stream);
         for (int d = b->maxDepth - 1; d >= 0 && e == cudaSuccess; --d) {
-            const int64_t mt = max_tiles(b, d, {PH_ADJ_EDGE, PH_ADJ_FACE, PH_ADJ_VERT});
+            const int64_t mt = max_tiles(b, d, {PH_ADJ_STATS, PH_ADJ_EDGE, PH_ADJ_FACE, PH_ADJ_VERT});
             e = launch_coop(b, k_batch_adjoint, mt, a, d);
         }
         return e;
@@ -597,8 +627,7 @@ int ccs_BatchAdjointPoints_cuda(ccs_Batch* batch) {
     std::lock_guard<std::mutex> lock(batch->mu);
     if (!batch->topoReady) return set_last_error(CCS_ERR_STATE);
     BatchDevice g(batch->device);
-    if (!batch->work && (!bmalloc(&batch->work, 3 * batch->totV) || !bmalloc(&batch->gradCage, 3 * batch->totCagePts)))
-        return set_last_error(CCS_ERR_ALLOC);
+    if (!adjoint_buffers(batch)) return set_last_error(CCS_ERR_ALLOC);
     return set_last_error(run_batch(batch, BOP_ADJOINT, true));
 }
 
@@ -606,8 +635,7 @@ int ccs_BatchGetArrays_cuda(ccs_Batch* batch, ccs_BatchArrays* out) {
     if (!batch || !out) return set_last_error(CCS_ERR_ARG);
     std::lock_guard<std::mutex> lock(batch->mu);
     BatchDevice g(batch->device);
-    if (!batch->work && (!bmalloc(&batch->work, 3 * batch->totV) || !bmalloc(&batch->gradCage, 3 * batch->totCagePts)))
-        return set_last_error(CCS_ERR_ALLOC);
+    if (!adjoint_buffers(batch)) return set_last_error(CCS_ERR_ALLOC);
     out->halfedges = batch->he;
     out->creases = batch->cr;
     out->points = batch->pts;

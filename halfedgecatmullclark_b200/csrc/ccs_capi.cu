@@ -163,7 +163,7 @@ struct SubdImpl {
     int32_t* he = nullptr;
     cc_Crease* cr = nullptr;
     float* pts = nullptr;
-    float* work = nullptr;         // adjoint scratch (cumV x 3)
+    float* work = nullptr;         // adjoint scratch (cumV x 3, then the ring statistics)
     int* err = nullptr;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
@@ -399,6 +399,10 @@ static int refine_op(cc_Subd* subd, int mode) {
     return ret(st);
 }
 
+// Float offset of the adjoint's ring statistics in a work buffer: after the
+// cumV x 3 gradient slots, rounded up to 16 bytes.
+static int64_t stats_offset(int64_t cumV) { return (3 * cumV + 3) & ~(int64_t)3; }
+
 // Adjoint over a caller-provided work buffer (`workFloats` floats); used by
 // the allocation-free entry point in ccs_noalloc.cu.
 int adjoint_into(const cc_Subd* subd, const float* gradPoints, float* gradCage, float* work, int64_t workFloats,
@@ -409,7 +413,12 @@ int adjoint_into(const cc_Subd* subd, const float* gradPoints, float* gradCage, 
     if (3 * s->cumV > workFloats) return CCS_ERR_SCRATCH_LIMIT;
     DeviceGuard g(s->device);
     Ctx c = s->ctx(stream);
-    return run_adjoint(c, gradPoints, work, gradCage, s->cumV) == cudaSuccess ? CCS_OK : CCS_ERR_CUDA;
+    // ring statistics after the gradient slots when they fit, else per-halfedge walks
+    float4* stats = nullptr;
+    const int64_t off = stats_offset(s->cumV);
+    if (off + 4 * adjoint_stats_count(c) <= workFloats && ((uintptr_t)work & 15u) == 0)
+        stats = reinterpret_cast<float4*>(work + off);
+    return run_adjoint(c, gradPoints, work, gradCage, s->cumV, stats) == cudaSuccess ? CCS_OK : CCS_ERR_CUDA;
 }
 
 int set_last_error(int status) { return ret(status); }
@@ -581,9 +590,12 @@ int ccs_AdjointPointsDevice_cuda(cc_Subd* subd, const float* gradPoints, float* 
     if (!s || !gradPoints || !gradCage) return ret(CCS_ERR_ARG);
     if (!s->topo_ready || !s->creases_ready) return ret(CCS_ERR_STATE);
     DeviceGuard g(s->device);
-    if (!s->work && dmalloc(&s->work, sizeof(float) * 3 * (size_t)s->cumV)) return ret(CCS_ERR_ALLOC);
     Ctx c = s->ctx((cudaStream_t)stream);
-    return ret(run_adjoint(c, gradPoints, s->work, gradCage, s->cumV) == cudaSuccess ? CCS_OK : CCS_ERR_CUDA);
+    const int64_t off = stats_offset(s->cumV);
+    if (!s->work && dmalloc(&s->work, sizeof(float) * (size_t)(off + 4 * adjoint_stats_count(c))))
+        return ret(CCS_ERR_ALLOC);
+    return ret(run_adjoint(c, gradPoints, s->work, gradCage, s->cumV, reinterpret_cast<float4*>(s->work + off)) ==
+                       cudaSuccess ? CCS_OK : CCS_ERR_CUDA);
 }
 
 int ccs_LevelCounts_cuda(const cc_Mesh* cage, int32_t maxDepth, ccs_LevelCounts* out) {
@@ -641,7 +653,8 @@ int ccs_ReadProfile_cuda(cc_Subd* subd, ccs_KernelTime* out, int cap) {
 
 const char* ccs_KernelName_cuda(int kernel) {
     static const char* names[] = {"topology", "creases", "face_points", "edge_points", "vertex_points",
-                                  "clear", "level_fused", "adjoint", "uvs", "level_points"};
+                                  "clear", "level_fused", "adjoint", "uvs", "level_points", "old_vertices"};
+    static_assert(sizeof(names) / sizeof(names[0]) == CCS_K_COUNT, "one name per kernel id");
     return (kernel >= 0 && kernel < CCS_K_COUNT) ? names[kernel] : "unknown";
 }
 

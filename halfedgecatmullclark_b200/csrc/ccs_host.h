@@ -70,7 +70,16 @@ cudaError_t run_points(const Ctx& c, const float* cagePts, float* pts, int mode,
 // CCS_POINTS_SCATTER or CCS_POINTS_NOCREASES_SCATTER.
 cudaError_t run_fused(const Ctx& c, bool topo, const float* cagePts, float* pts, int mode, bool deterministic);
 
-// Adjoint (ccs_adjoint.cu).  `work` holds cumV x 3 floats.
-cudaError_t run_adjoint(const Ctx& c, const float* gradPts, float* work, float* gradCage, int64_t cumV);
+// Adjoint (ccs_adjoint.cu).  `work` holds cumV x 3 floats; `stats` (may be
+// null: the rings are then walked per halfedge) holds adjoint_stats_count(c)
+// float4 entries, 16-byte aligned.
+cudaError_t run_adjoint(const Ctx& c, const float* gradPts, float* work, float* gradCage, int64_t cumV,
+                        float4* stats);
+// Older vertices of the largest quad level the adjoint visits: max V(d-1), 1 <= d < D.
+inline int64_t adjoint_stats_count(const Ctx& c) {
+    int64_t m = 0;
+    for (int d = 1; d < c.D; ++d) m = c.lv[d - 1].V > m ? c.lv[d - 1].V : m;
+    return m;
+}
 
 }  // namespace ccs

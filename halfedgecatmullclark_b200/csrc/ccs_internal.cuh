@@ -145,6 +145,9 @@ struct QuadView {
     const cc_Crease* __restrict__ cr;  // level-d creases
     int32_t V, F, E, H, C;
     int32_t d;
+    // optional (adjoint): ring statistics of the older vertices v < V(d-1),
+    // {valence, summed sharpness, crease count, boundary ? 1 : 0}
+    const float4* __restrict__ ostats = nullptr;
     __device__ __forceinline__ int32_t rec(int32_t h, int w) const { return he[(int64_t)RW * h + w]; }
     __device__ __forceinline__ int32_t twin(int32_t h) const { return rec(h, 0); }
     __device__ __forceinline__ int32_t edge(int32_t h) const { return rec(h, 1); }
@@ -291,10 +294,29 @@ __device__ __forceinline__ bool quad_ring_known(const QuadView<RW>& L, int32_t h
 }
 __device__ __forceinline__ bool quad_ring_known(const CageView&, int32_t, RingStats&) { return false; }
 
+// Child 0 (an older vertex) from precomputed whole-ring statistics: the walk
+// from h sees every incident edge but, on a boundary, its own.  The
+// subtraction makes avgS differ from the walk's sum by rounding only; the
+// adjoint uses this, the forward passes never set ostats.
+template <int RW>
+__device__ __forceinline__ bool ring_from_stats(const QuadView<RW>& L, int32_t h, RingStats& r) {
+    if (!L.ostats) return false;
+    const float4 s = L.ostats[L.vert(h)];
+    const bool bnd = s.w != 0.0f;
+    const float own = L.hsharp(h);
+    r.valence = s.x;
+    r.avgS = bnd ? fsub(s.y, own) : s.y;
+    r.creaseCount = bnd ? fsub(s.z, fsign(own)) : s.z;
+    r.fwd = bnd ? -1 : h;
+    return true;
+}
+__device__ __forceinline__ bool ring_from_stats(const CageView&, int32_t, RingStats&) { return false; }
+
 template <class View>
 __device__ __forceinline__ RingStats creased_ring(const View& L, int32_t h) {
     RingStats r;
     if (quad_ring_known(L, h, r)) return r;
+    if (ring_from_stats(L, h, r)) return r;
     return creased_ring_walk(L, h);
 }
 

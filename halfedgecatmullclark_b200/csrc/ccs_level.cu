@@ -16,11 +16,11 @@
 //        rebuilt from the twin quad's four records (the same value, bit for
 //        bit, as the twin quad's lanes store);
 //      - extra blocks refine the creases of the level.
-//   B  (depth d >= 2; vertex points, no atomics)
-//      - the first blocks take the older vertices (v < V(d-1)), one thread
-//        per vertex: one walk of the ring, every share, summed in
-//        increasing halfedge order;
-//      - the other blocks take one tile of halfedges each, one thread per
+//   B  (depth d >= 2; vertex points, no atomics; two launches)
+//      - k_level_v: the older vertices (v < V(d-1)), one thread per
+//        vertex: one walk of the ring, every share, summed in increasing
+//        halfedge order;
+//      - k_level_b: one tile of halfedges per block, one thread per
 //        halfedge: a face centre's 4 shares meet in 4 lanes of a 16-lane
 //        group and an edge midpoint's 4 shares in the lane of the parent
 //        pair's owner (the twin side's 2 shares rebuilt from face and edge
@@ -64,19 +64,21 @@ k_level_a(LevelArgs a) {
     tile_level_a<kBlockL, RW, TOPO, UV, PTS, CREASED>(a, (int64_t)blockIdx.x * kBlockL, tile);
 }
 
-// kernel B (d >= 2): blocks [0, nbV) take the older vertices (their walks
-// are the longest-latency work, so they start first), the blocks after them
-// one tile of halfedges each.
+// kernel B (d >= 2): one tile of halfedges per block (face centres and edge
+// midpoints)
+template <int RW, bool CREASED>
+__global__ void __launch_bounds__(kBlockL, 5)
+k_level_b(QuadView<RW> L, const float* __restrict__ pin, float* __restrict__ pout) {
+    tile_level_b<RW, CREASED>(L, pin, pout, (int64_t)blockIdx.x * kBlockL);
+}
+
+// kernel V (d >= 2): one thread per older vertex (a separate launch, so that
+// kernel B keeps its small register footprint)
 template <int RW, bool CREASED>
 __global__ void __launch_bounds__(kBlockL)
-k_level_b(QuadView<RW> L, const float* __restrict__ pin, float* __restrict__ pout, int32_t Vold) {
-    const int nbV = (Vold + kBlockL - 1) / kBlockL;
-    if ((int)blockIdx.x < nbV) {
-        const int64_t v = (int64_t)blockIdx.x * kBlockL + threadIdx.x;
-        if (v < Vold) old_vertex_item<RW, CREASED>(L, pin, pout, (int32_t)v);
-        return;
-    }
-    tile_level_b<RW, CREASED>(L, pin, pout, (int64_t)(blockIdx.x - nbV) * kBlockL);
+k_level_v(QuadView<RW> L, const float* __restrict__ pin, float* __restrict__ pout, int32_t Vold) {
+    const int64_t v = (int64_t)blockIdx.x * kBlockL + threadIdx.x;
+    if (v < Vold) old_vertex_item<RW, CREASED>(L, pin, pout, (int32_t)v);
 }
 
 // ---------------------------------------------------------------------------
@@ -121,8 +123,10 @@ static void level_b(const Ctx& c, int d, const float* pin, float* pout) {
     const QuadView<RW> L = quad_view_l<RW>(c, d);
     const int32_t Vold = c.lv[d - 1].V;
     c.prof->begin(c.stream, CCS_K_LEVEL_POINTS, d, L.H);
-    const unsigned nb = nblocksL(Vold) + nblocksL(L.H);
-    k_level_b<RW, CREASED><<<nb, kBlockL, 0, c.stream>>>(L, pin, pout, Vold);
+    k_level_b<RW, CREASED><<<nblocksL(L.H), kBlockL, 0, c.stream>>>(L, pin, pout);
+    c.prof->end(c.stream);
+    c.prof->begin(c.stream, CCS_K_OLD_VERTICES, d, Vold);
+    k_level_v<RW, CREASED><<<nblocksL(Vold), kBlockL, 0, c.stream>>>(L, pin, pout, Vold);
     c.prof->end(c.stream);
 }
 

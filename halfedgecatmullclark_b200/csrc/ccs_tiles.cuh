@@ -307,12 +307,22 @@ __device__ __forceinline__ void tile_level_b(const QuadView<RW>& L, const float*
     const int32_t ed0p = __shfl_sync(full, ed, gb | (((j + 3) & 3) << 2));   // child 0 of prev(g)
     const bool ownG = (ed0 & 1) == 0, ownPrev = (ed0p & 1) == 0;
     const bool need = k == 2 || (k == 3 ? ownPrev : ownG);
-    f3 p = zero3(), Fh = zero3(), Eh = zero3();
+    // the owner of an interior parent edge also reads the twin side's face
+    // and edge points (children 1 of t and 3 of next(t)), in the same round
+    const bool twinSide = k == 1 && ownG && tw0 >= 0;
+    const int32_t tn = tw0 >> 2, t = qprev(tn);        // next(t) and t = twin(g), depth d-1
+    const int32_t eB1 = ed - (h >> 2) + t;             // edge of child 1 of t: 2 E(d-1) + t
+    f3 p = zero3(), Fh = zero3(), Eh = zero3(), FB1 = zero3(), FB2 = zero3(), EB1 = zero3();
     if (valid && need) {
         Eh = ld3(ept + 3 * (int64_t)ed);              // k = 0: E of child 0, the twin side's or prev's edge point
         if (k != 0) {
             p = ld3(pin + 3 * (int64_t)vx);
             Fh = ld3(fpt + 3 * (int64_t)(h >> 2));
+        }
+        if (twinSide) {
+            FB1 = ld3(fpt + 3 * (int64_t)t);
+            FB2 = ld3(fpt + 3 * (int64_t)tn);
+            EB1 = ld3(ept + 3 * (int64_t)eB1);
         }
     }
     const f3 Ep = shfl3(Eh, lp);                      // edge point of prev(h)'s edge
@@ -349,17 +359,14 @@ __device__ __forceinline__ void tile_level_b(const QuadView<RW>& L, const float*
         f3 sA1 = s;
         order2(iA1, sA1, iA2, sA2);
         f3 acc;
-        if (tw0 < 0) {
+        if (!twinSide) {
             acc = add3(add3(zero3(), sA1), sA2);
         } else {
-            const int32_t tn = tw0 >> 2;                 // next(t), depth d-1
-            const int32_t t = qprev(tn);
-            const int32_t eB1 = ed - (h >> 2) + t;       // edge of child 1 of t: 2 E(d-1) + t
-            const int32_t eB2 = ed0;                     // edge of child 3 of next(t): 2 e
-            const f3 sB1 = quad_vertex_rule<CREASED>(p, ld3(fpt + 3 * (int64_t)t), ld3(ept + 3 * (int64_t)eB1),
-                                                     zero3(), vpre, cpre, avgS, false, fsign(L.sharp(eB1)), 0.0f);
-            const f3 sB2 = quad_vertex_rule<CREASED>(p, ld3(fpt + 3 * (int64_t)tn), Ep,
-                                                     zero3(), vpre, cpre, avgS, false, fsign(L.sharp(eB2)), 0.0f);
+            // child 3 of next(t) has edge 2 e = ed0, whose edge point is Ep
+            const f3 sB1 = quad_vertex_rule<CREASED>(p, FB1, EB1, zero3(), vpre, cpre, avgS, false,
+                                                     fsign(L.sharp(eB1)), 0.0f);
+            const f3 sB2 = quad_vertex_rule<CREASED>(p, FB2, Ep, zero3(), vpre, cpre, avgS, false,
+                                                     fsign(L.sharp(ed0)), 0.0f);
             int32_t iB1 = 4 * t + 1, iB2 = 4 * tn + 3;
             f3 b1 = sB1, b2 = sB2;
             order2(iB1, b1, iB2, b2);
@@ -717,6 +724,43 @@ __device__ __forceinline__ void vertex_det_item(const View& L, const float* __re
 // ---------------------------------------------------------------------------
 // adjoint of the creased scatter rule (see ccs_adjoint.cu): three gathers
 // ---------------------------------------------------------------------------
+// item = older vertex v < V(d-1) of quad level d: one walk of its ring,
+// {valence, summed sharpness and crease count of every incident edge,
+// boundary} for ring_from_stats.  The walk reads prev(x)'s record only:
+// edge(prev x) is the next member's edge, or on a boundary the last edge.
+template <int RW>
+__device__ __forceinline__ void ring_stats_item(const QuadView<RW>& L, float4* __restrict__ out, int32_t v) {
+    const int32_t h0 = L.vert_he(v);
+    float s = L.hsharp(h0);
+    float n = 1.0f, tot = s, cnt = fsign(s);
+    int32_t x = h0;
+    int guard = 0;
+    for (;;) {
+        const int32_t pr = qprev(x);
+        const int32_t e = L.edge(pr);
+        x = L.twin(pr);
+        if (x == h0 || ++guard >= kWalkCap) break;
+        s = L.sharp(e);
+        tot = fadd(tot, s);
+        cnt = fadd(cnt, fsign(s));
+        if (x < 0) break;
+        n = fadd(n, 1.0f);
+    }
+    const bool bnd = x < 0;
+    if (bnd) {
+        guard = 0;
+        for (int32_t b = L.twin(h0); b >= 0 && guard < kWalkCap; ++guard) {
+            const int32_t c = qnext(b);
+            s = L.hsharp(c);
+            n = fadd(n, 1.0f);
+            tot = fadd(tot, s);
+            cnt = fadd(cnt, fsign(s));
+            b = L.twin(c);
+        }
+    }
+    out[v] = make_float4(n, tot, cnt, bnd ? 1.0f : 0.0f);
+}
+
 struct VCoef {
     float a, bF, cE, dE;
 };

@@ -40,13 +40,20 @@ def kernel_bytes(kernel: str, lv: dict, rec: int = 16) -> int:
     if kernel == "clear":
         return int(12 * V)
     if kernel == "level_fused":
-        # records in + children out + creases + old points in + face points
-        # out + the cleared old-vertex slots
-        return int(rec * H + 4 * rec * H + 36 * C + 12 * V + 12 * F + 12 * V)
+        # records in + children out + creases in and out + points in + face
+        # and edge points out
+        return int(rec * H + 4 * rec * H + 36 * C + 12 * V + 12 * F + 12 * E)
+    # depth d >= 2: F(d-1) = H / 16 face centres and E(d-1) = (E - H / 4) / 2
+    # edge midpoints are the vertices kernel B takes; the rest are older
+    nb = H // 16 + (E - H // 4) // 2
     if kernel == "level_points":
-        # records + old points + face points + crease records in; edge points
-        # out; vertex points accumulated (written once)
-        return int(rec * H + 12 * V + 12 * F + 12 * C + 12 * E + 12 * V)
+        # records + crease records + face and edge points in; the points of
+        # its vertices in and out
+        return int(rec * H + 12 * C + 12 * F + 12 * E + 24 * nb)
+    if kernel == "old_vertices":
+        # records of children 0 and 3 (the ring walk), the ring's face and
+        # edge points (H / 4 members), the points in and out
+        return int(rec * H // 2 + 24 * (H // 4) + 24 * max(V - nb, 0))
     if kernel == "adjoint":
         return int(rec * H + 12 * C + 12 * (V + F + E) + 12 * V)
     return 0

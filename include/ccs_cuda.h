@@ -297,7 +297,7 @@ typedef struct {
 enum {
     CCS_K_TOPOLOGY = 0, CCS_K_CREASES = 1, CCS_K_FACE_POINTS = 2, CCS_K_EDGE_POINTS = 3,
     CCS_K_VERTEX_POINTS = 4, CCS_K_CLEAR = 5, CCS_K_LEVEL_FUSED = 6, CCS_K_ADJOINT = 7,
-    CCS_K_UVS = 8, CCS_K_LEVEL_POINTS = 9, CCS_K_COUNT = 10
+    CCS_K_UVS = 8, CCS_K_LEVEL_POINTS = 9, CCS_K_OLD_VERTICES = 10, CCS_K_COUNT = 11
 };
 /* When enabled, every launch of the subd is bracketed by CUDA events on its
  * stream (and CUDA graphs are not used). */
