@@ -287,6 +287,49 @@ def max_over_ranks(x, world):
     return float(t.item())
 
 
+def adjoint_timing(subd, w, stream, flush, steps, torch):
+    """Device ms of one adjoint pass (ccs_AdjointPointsDevice_cuda) and its
+    per-kernel profile, on the workload's subd (topology already refined)."""
+    import ctypes
+    g = torch.randn((subd.cumV, 3), device="cuda")
+    gc = torch.empty((w.cage.V, 3), device="cuda")
+    sp = ctypes.c_void_p(int(stream.cuda_stream))
+    call = lambda: subd.L.ccs_AdjointPointsDevice_cuda(subd.ptr, g.data_ptr(), gc.data_ptr(), sp)
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            call()
+    torch.cuda.synchronize()
+    ms = []
+    with torch.cuda.stream(stream):
+        for _ in range(max(1, steps)):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            call()
+            b.record(stream)
+            ms.append((a, b))
+    torch.cuda.synchronize()
+    mean = statistics.mean(a.elapsed_time(b) for a, b in ms)
+    subd.set_profiling(True)
+    with torch.cuda.stream(stream):
+        flush.zero_()
+        call()
+    recs = subd.read_profile(1 << 14)
+    subd.set_profiling(False)
+    by = {}
+    for r in recs:
+        by[(r["kernel"], r["level"])] = by.get((r["kernel"], r["level"]), 0.0) + r["ms"]
+    top = sorted(by.items(), key=lambda kv: -kv[1])[:10]
+    return {"ms_per_pass": mean, "halfedges_per_s": subd_halfedges(subd) / (mean / 1e3),
+            "kernels": [{"kernel": k[0], "level": k[1], "ms": v} for k, v in top]}
+
+
+def subd_halfedges(subd):
+    from halfedgecatmullclark_b200 import metrics
+    return metrics.total_halfedges(subd.levels)
+
+
 def run_batch_workload(args):
     """Many uneven cages: forward (points) + adjoint per step, batched (one
     persistent launch per depth, CUDA graph, autotuned grid) against a Python
@@ -298,8 +341,12 @@ def run_batch_workload(args):
     from halfedgecatmullclark_b200 import configs
     from halfedgecatmullclark_b200.subd import Subd
 
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    ws = configs.batch_cages(count=args.batch_count)
+    from halfedgecatmullclark_b200 import shard
+    rank, world = dist_init()
+    ws_all = configs.batch_cages(count=args.batch_count)
+    # independent cages: each rank refines its own share, no exchange
+    parts = shard.shard([shard.cage_work(w.cage, w.depth) for w in ws_all], world)
+    ws = [ws_all[i] for i in parts[rank]]
     cages = [w.cage for w in ws]
     depths = [w.depth for w in ws]
     stream = torch.cuda.Stream()
@@ -331,6 +378,7 @@ def run_batch_workload(args):
     for _ in range(max(1, args.warmup)):
         loop_step()
     torch.cuda.synchronize()
+    barrier(world)
     a = torch.cuda.Event(enable_timing=True)
     b = torch.cuda.Event(enable_timing=True)
     a.record(stream)
@@ -338,7 +386,7 @@ def run_batch_workload(args):
         loop_step()
     b.record(stream)
     torch.cuda.synchronize()
-    loop_ms = a.elapsed_time(b) / steps
+    loop_ms = shard.max_over_ranks(a.elapsed_time(b) / steps, world)
     loop_sample = [bufs[i][3].clone() for i in (0, len(bufs) // 2, len(bufs) - 1)]
     grads = [g for (_, _, g, _) in bufs]
     for s in subds:
@@ -372,26 +420,35 @@ def run_batch_workload(args):
         for _ in range(max(1, args.warmup)):
             batch_step()
     bt.synchronize()
+    barrier(world)
     with torch.cuda.stream(stream):
         a.record(stream)
         for _ in range(steps):
             batch_step()
         b.record(stream)
     bt.synchronize()
-    batch_ms = a.elapsed_time(b) / steps
+    batch_ms = shard.max_over_ranks(a.elapsed_time(b) / steps, world)
     agree = max(float((arr["grad_cage_points"][bt.cage_slice(i)] - ref).abs().max() /
                       max(ref.abs().max(), 1e-30))
                 for i, ref in zip((0, len(ws) // 2, len(ws) - 1), loop_sample))
-    sh = sum(inf["halfedgeCount"] for inf in bt.info)
+    agree = shard.max_over_ranks(agree, world)
+    sh = int(shard.sum_over_ranks(sum(inf["halfedgeCount"] for inf in bt.info), world))
+    topo_ms = shard.max_over_ranks(topo_ms, world)
     bt.close()
-    line = {"metric": "batched forward+adjoint cages/s", "value": len(ws) / (batch_ms / 1e3),
-            "unit": "cages/s", "n_gpus": 1, "steps": steps, "warmup": args.warmup,
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {"metric": "batched forward+adjoint cages/s", "value": len(ws_all) / (batch_ms / 1e3),
+            "unit": "cages/s", "n_gpus": world, "steps": steps, "warmup": args.warmup,
             "ms_per_step": batch_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "batch_cages_%d" % len(ws), "faces": "log-uniform [50, 5000]",
+            "config": {"workload": "batch_cages_%d" % len(ws_all), "faces": "log-uniform [50, 5000]",
                        "depths": "uniform {2..6}", "refined_halfedges": sh,
+                       "parallelism": "cage shards x%d (no exchange)" % world,
                        "schedule": {"blocks_per_sm": tune["blocks_per_sm"], "tried": tune["tried"]}},
-            "loop": {"value": len(ws) / (loop_ms / 1e3), "unit": "cages/s", "ms_per_step": loop_ms,
+            "loop": {"value": len(ws_all) / (loop_ms / 1e3), "unit": "cages/s", "ms_per_step": loop_ms,
                      "how": "Python loop of ccs_RefinePointsDevice_cuda + ccs_AdjointPointsDevice_cuda per cage"},
             "speedup_vs_loop": loop_ms / batch_ms, "topology_refine_ms": topo_ms,
             "grad_agreement_rel": agree}
@@ -488,6 +545,10 @@ def main():
                           "halfedges_per_s": levels[d + 1]["H"] / (ms / 1e3), "alg_bytes": nb,
                           "gbs": nb / (ms / 1e3) / 1e9, "frac_of_peak": nb / (ms / 1e3) / 1e9 / peak})
 
+    # adjoint of the same workload (points of every depth -> cage points),
+    # through the C ABI on the subd's stream
+    adj = adjoint_timing(subd, w, stream, flush, args.steps, torch)
+
     # end to end through the C ABI with host buffers
     host_pts = torch.from_numpy(w.cage.vertex_points.copy()).pin_memory()
     e2e_ms = []
@@ -534,6 +595,7 @@ def main():
                          "traffic": traffic},
             "per_depth": per_depth,
             "kernels": kernels[:12],
+            "adjoint": adj,
             "clocks": clocks,
             "wall_s": wall,
         }

@@ -72,17 +72,23 @@ template <int RW>
 static void attach_stats(const Ctx& c, QuadView<RW>& L, float4* stats) {
     if (!stats) return;
     const int32_t Vold = c.lv[L.d - 1].V;
+    c.prof->begin(c.stream, CCS_K_ADJ_STATS, L.d, Vold);
     k_ring_stats<RW><<<nblocksA(Vold), kBlockA, 0, c.stream>>>(L, stats, Vold);
+    c.prof->end(c.stream);
     L.ostats = stats;
 }
 static void attach_stats(const Ctx&, CageView&, float4*) {}
 
 template <class View>
 static void adjoint_level(const Ctx& c, View L, float* gNew, float* gOld, float4* stats) {
-    c.prof->begin(c.stream, CCS_K_ADJOINT, L.d, L.H);
     attach_stats(c, L, stats);
+    c.prof->begin(c.stream, CCS_K_ADJ_EDGES, L.d, L.H);
     k_adj_edges<View><<<nblocksA(L.H), kBlockA, 0, c.stream>>>(L, gNew);
+    c.prof->end(c.stream);
+    c.prof->begin(c.stream, CCS_K_ADJ_FACES, L.d, L.F);
     k_adj_faces<View><<<nblocksA(L.F), kBlockA, 0, c.stream>>>(L, gNew);
+    c.prof->end(c.stream);
+    c.prof->begin(c.stream, CCS_K_ADJ_VERTICES, L.d, L.V);
     k_adj_vertices<View><<<nblocksA(L.V), kBlockA, 0, c.stream>>>(L, gNew, gOld);
     c.prof->end(c.stream);
 }

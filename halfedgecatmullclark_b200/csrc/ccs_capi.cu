@@ -166,6 +166,8 @@ struct SubdImpl {
     float* work = nullptr;         // adjoint scratch (cumV x 3, then the ring statistics)
     int* err = nullptr;
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;   // second stream: old-vertex kernel beside kernel B
+    cudaEvent_t forkEv = nullptr, joinEv = nullptr;
     bool own_stream = false;
     bool pinned = true;
     bool topo_ready = false, creases_ready = false;
@@ -177,6 +179,7 @@ struct SubdImpl {
         Ctx c;
         c.cage = &dc; c.rw = rw; c.D = D; c.lv = lv.data(); c.he = he; c.cr = cr;
         c.stream = s; c.prof = &prof; c.err = err;
+        c.side = side; c.forkEv = forkEv; c.joinEv = joinEv;
         return c;
     }
 };
@@ -212,6 +215,9 @@ static void free_impl(SubdImpl* s) {
     cudaFree(s->dc.v2h); cudaFree(s->dc.e2h); cudaFree(s->dc.f2h); cudaFree(s->dc.fsz);
     cudaFree(s->he); cudaFree(s->cr); cudaFree(s->pts); cudaFree(s->work); cudaFree(s->err);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+    if (s->side) cudaStreamDestroy(s->side);
+    if (s->forkEv) cudaEventDestroy(s->forkEv);
+    if (s->joinEv) cudaEventDestroy(s->joinEv);
     if (s->host) {
         if (s->pinned) {
             cudaFreeHost(s->host->halfedges); cudaFreeHost(s->host->creases); cudaFreeHost(s->host->vertexPoints);
@@ -278,6 +284,12 @@ static int create(const cc_Mesh* cage, int32_t D, uint32_t flags, cc_Subd** out)
     if (cudaGetDevice(&s->device) != cudaSuccess) { delete s; return CCS_ERR_CUDA; }
     if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) { delete s; return CCS_ERR_CUDA; }
     s->own_stream = true;
+    if (cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->forkEv, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->joinEv, cudaEventDisableTiming) != cudaSuccess) {
+        free_impl(s);
+        return CCS_ERR_CUDA;
+    }
 
     const size_t heBytes = sizeof(int32_t) * (size_t)s->rw * (size_t)s->cumH;
     const size_t crBytes = sizeof(cc_Crease) * (size_t)s->cumC;
@@ -526,6 +538,9 @@ int ccs_SetStream_cuda(cc_Subd* subd, void* stream) {
     DeviceGuard g(s->device);
     if (s->stream) cudaStreamSynchronize(s->stream);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+    if (s->side) cudaStreamDestroy(s->side);
+    if (s->forkEv) cudaEventDestroy(s->forkEv);
+    if (s->joinEv) cudaEventDestroy(s->joinEv);
     s->stream = (cudaStream_t)stream;
     s->own_stream = false;
     return ret(CCS_OK);
@@ -653,7 +668,8 @@ int ccs_ReadProfile_cuda(cc_Subd* subd, ccs_KernelTime* out, int cap) {
 
 const char* ccs_KernelName_cuda(int kernel) {
     static const char* names[] = {"topology", "creases", "face_points", "edge_points", "vertex_points",
-                                  "clear", "level_fused", "adjoint", "uvs", "level_points", "old_vertices"};
+                                  "clear", "level_fused", "adjoint", "uvs", "level_points", "old_vertices",
+                                  "adj_stats", "adj_edges", "adj_faces", "adj_vertices"};
     static_assert(sizeof(names) / sizeof(names[0]) == CCS_K_COUNT, "one name per kernel id");
     return (kernel >= 0 && kernel < CCS_K_COUNT) ? names[kernel] : "unknown";
 }

@@ -58,6 +58,10 @@ struct Ctx {
     cudaStream_t stream;
     Profiler* prof;
     int* err;                    // device error word
+    // optional second stream for independent launches of one step (forked
+    // from and joined back into `stream` by the two events); null = serial
+    cudaStream_t side = nullptr;
+    cudaEvent_t forkEv = nullptr, joinEv = nullptr;
 };
 
 // Forward passes (ccs_forward.cu).  All return cudaError_t of the launches.

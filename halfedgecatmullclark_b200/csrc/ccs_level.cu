@@ -122,12 +122,25 @@ template <int RW, bool CREASED>
 static void level_b(const Ctx& c, int d, const float* pin, float* pout) {
     const QuadView<RW> L = quad_view_l<RW>(c, d);
     const int32_t Vold = c.lv[d - 1].V;
+    // V (memory-latency bound) runs beside B (issue bound) when a second
+    // stream is available: both read only kernel A's output and write
+    // disjoint vertex slots
+    const bool fork = c.side && c.forkEv && c.joinEv;
+    cudaStream_t sv = fork ? c.side : c.stream;
+    if (fork) {
+        cudaEventRecord(c.forkEv, c.stream);
+        cudaStreamWaitEvent(c.side, c.forkEv, 0);
+    }
+    c.prof->begin(sv, CCS_K_OLD_VERTICES, d, Vold);
+    k_level_v<RW, CREASED><<<nblocksL(Vold), kBlockL, 0, sv>>>(L, pin, pout, Vold);
+    c.prof->end(sv);
     c.prof->begin(c.stream, CCS_K_LEVEL_POINTS, d, L.H);
     k_level_b<RW, CREASED><<<nblocksL(L.H), kBlockL, 0, c.stream>>>(L, pin, pout);
     c.prof->end(c.stream);
-    c.prof->begin(c.stream, CCS_K_OLD_VERTICES, d, Vold);
-    k_level_v<RW, CREASED><<<nblocksL(Vold), kBlockL, 0, c.stream>>>(L, pin, pout, Vold);
-    c.prof->end(c.stream);
+    if (fork) {
+        cudaEventRecord(c.joinEv, c.side);
+        cudaStreamWaitEvent(c.stream, c.joinEv, 0);
+    }
 }
 
 // Declared in ccs_forward.cu: the vertex pass of one quad level when the
