@@ -538,9 +538,7 @@ int ccs_SetStream_cuda(cc_Subd* subd, void* stream) {
     DeviceGuard g(s->device);
     if (s->stream) cudaStreamSynchronize(s->stream);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
-    if (s->side) cudaStreamDestroy(s->side);
-    if (s->forkEv) cudaEventDestroy(s->forkEv);
-    if (s->joinEv) cudaEventDestroy(s->joinEv);
+    if (s->side) cudaStreamSynchronize(s->side);
     s->stream = (cudaStream_t)stream;
     s->own_stream = false;
     return ret(CCS_OK);
