@@ -26,8 +26,8 @@ POINTS_SCATTER, POINTS_GATHER, POINTS_NOCREASES_SCATTER, POINTS_NOCREASES_GATHER
 POINT_MODES = {"scatter": 0, "gather": 1, "nocreases_scatter": 2, "nocreases_gather": 3}
 
 KERNEL_NAMES = ["topology", "creases", "face_points", "edge_points", "vertex_points", "clear",
-                "level_fused", "adjoint", "uvs", "level_points", "old_vertices", "adj_stats", "adj_edges",
-                "adj_faces", "adj_vertices"]
+                "level_fused", "adjoint", "uvs", "level_points", "old_vertices", "ring_stats", "adj_edges",
+                "adj_faces", "adj_vertices", "exact_points"]
 
 
 class CcsError(RuntimeError):

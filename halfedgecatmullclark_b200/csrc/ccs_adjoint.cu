@@ -25,8 +25,8 @@
 //
 // The coefficients of a halfedge need its vertex's ring statistics.  On quad
 // levels these are known from the structure for face centres and edge
-// midpoints; for the older vertices one thread per vertex walks the ring
-// once per level (k_ring_stats) and the three gathers read the result.
+// midpoints; for the older vertices the gathers read the per-level table the
+// topology refinement keeps (k_ring_stats, one ring walk per vertex).
 //
 // Levels run deepest first; only the level offsets are needed (no state is
 // saved by the forward pass).
@@ -37,13 +37,6 @@ namespace ccs {
 
 static constexpr int kBlockA = 256;
 static inline unsigned nblocksA(int64_t n) { return (unsigned)((n + kBlockA - 1) / kBlockA); }
-
-template <int RW>
-__global__ void __launch_bounds__(kBlockA)
-k_ring_stats(QuadView<RW> L, float4* __restrict__ out, int32_t Vold) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < Vold) ring_stats_item(L, out, (int32_t)i);
-}
 
 template <class View>
 __global__ void __launch_bounds__(kBlockA)
@@ -68,20 +61,8 @@ k_adj_vertices(View L, const float* __restrict__ gNew, float* __restrict__ gOld)
 
 static CageTables cage_tables_a(const DevCage& c) { return make_cage_tables(c); }
 
-template <int RW>
-static void attach_stats(const Ctx& c, QuadView<RW>& L, float4* stats) {
-    if (!stats) return;
-    const int32_t Vold = c.lv[L.d - 1].V;
-    c.prof->begin(c.stream, CCS_K_ADJ_STATS, L.d, Vold);
-    k_ring_stats<RW><<<nblocksA(Vold), kBlockA, 0, c.stream>>>(L, stats, Vold);
-    c.prof->end(c.stream);
-    L.ostats = stats;
-}
-static void attach_stats(const Ctx&, CageView&, float4*) {}
-
 template <class View>
-static void adjoint_level(const Ctx& c, View L, float* gNew, float* gOld, float4* stats) {
-    attach_stats(c, L, stats);
+static void adjoint_level(const Ctx& c, const View& L, float* gNew, float* gOld) {
     c.prof->begin(c.stream, CCS_K_ADJ_EDGES, L.d, L.H);
     k_adj_edges<View><<<nblocksA(L.H), kBlockA, 0, c.stream>>>(L, gNew);
     c.prof->end(c.stream);
@@ -93,8 +74,7 @@ static void adjoint_level(const Ctx& c, View L, float* gNew, float* gOld, float4
     c.prof->end(c.stream);
 }
 
-cudaError_t run_adjoint(const Ctx& c, const float* gradPts, float* work, float* gradCage, int64_t cumV,
-                        float4* stats) {
+cudaError_t run_adjoint(const Ctx& c, const float* gradPts, float* work, float* gradCage, int64_t cumV) {
     cudaError_t st = cudaMemcpyAsync(work, gradPts, sizeof(float) * 3 * (size_t)cumV,
                                      cudaMemcpyDeviceToDevice, c.stream);
     if (st != cudaSuccess) return st;
@@ -108,7 +88,7 @@ cudaError_t run_adjoint(const Ctx& c, const float* gradPts, float* work, float* 
             L.cr = c.cage->cr;
             L.V = c.cage->V; L.F = c.cage->F; L.E = c.cage->E; L.H = c.cage->H; L.C = c.cage->E;
             L.d = 0;
-            adjoint_level(c, L, gNew, gradCage, stats);
+            adjoint_level(c, L, gNew, gradCage);
         } else {
             float* gOld = work + 3 * c.lv[d].ptOff;
             const Level& lv = c.lv[d];
@@ -118,14 +98,16 @@ cudaError_t run_adjoint(const Ctx& c, const float* gradPts, float* work, float* 
                 L.he = c.he + 4 * lv.heOff;
                 L.cr = c.cr + lv.crOff;
                 L.V = lv.V; L.F = lv.F; L.E = lv.E; L.H = lv.H; L.C = lv.C; L.d = d;
-                adjoint_level(c, L, gNew, gOld, stats);
+                L.ostats = stats_at(c, d);
+                adjoint_level(c, L, gNew, gOld);
             } else {
                 QuadView<3> L;
                 L.t = cage_tables_a(*c.cage);
                 L.he = c.he + 3 * lv.heOff;
                 L.cr = c.cr + lv.crOff;
                 L.V = lv.V; L.F = lv.F; L.E = lv.E; L.H = lv.H; L.C = lv.C; L.d = d;
-                adjoint_level(c, L, gNew, gOld, stats);
+                L.ostats = stats_at(c, d);
+                adjoint_level(c, L, gNew, gOld);
             }
         }
     }

@@ -238,7 +238,7 @@ k_batch_forward(BatchArgs a, int d) {
         const float* pin = a.pts + 3 * (bc.pt + bc.lv[d].ptOff);
         float* pout = a.pts + 3 * (bc.pt + bc.lv[d + 1].ptOff);
         if (d >= 2) {
-            tile_level_b<4, CREASED>(L, pin, pout, lt * kBatchBlock);
+            tile_level_b_exact<4, CREASED>(L, pin, pout, lt * kBatchBlock);
         } else {
             const int64_t v = lt * kBatchBlock + tid;
             if (v < L.V) vertex_det_item<QuadView<4>, CREASED>(L, pin, pout, (int32_t)v);

@@ -163,7 +163,9 @@ struct SubdImpl {
     int32_t* he = nullptr;
     cc_Crease* cr = nullptr;
     float* pts = nullptr;
-    float* work = nullptr;         // adjoint scratch (cumV x 3, then the ring statistics)
+    float* work = nullptr;         // adjoint scratch (cumV x 3)
+    float4* stats = nullptr;       // ring statistics of the older vertices, levels 1..D-1
+    std::vector<int64_t> statsOff; // level d at stats + statsOff[d] (V(d-1) entries)
     int* err = nullptr;
     cudaStream_t stream = nullptr;
     cudaStream_t side = nullptr;   // second stream: old-vertex kernel beside kernel B
@@ -180,6 +182,7 @@ struct SubdImpl {
         c.cage = &dc; c.rw = rw; c.D = D; c.lv = lv.data(); c.he = he; c.cr = cr;
         c.stream = s; c.prof = &prof; c.err = err;
         c.side = side; c.forkEv = forkEv; c.joinEv = joinEv;
+        c.stats = stats; c.statsOff = statsOff.data();
         return c;
     }
 };
@@ -213,7 +216,7 @@ static void free_impl(SubdImpl* s) {
     for (auto& t : s->prof.pending) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
     cudaFree(s->dc.he); cudaFree(s->dc.cr); cudaFree(s->dc.pts); cudaFree(s->dc.uvs);
     cudaFree(s->dc.v2h); cudaFree(s->dc.e2h); cudaFree(s->dc.f2h); cudaFree(s->dc.fsz);
-    cudaFree(s->he); cudaFree(s->cr); cudaFree(s->pts); cudaFree(s->work); cudaFree(s->err);
+    cudaFree(s->he); cudaFree(s->cr); cudaFree(s->pts); cudaFree(s->work); cudaFree(s->err); cudaFree(s->stats);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     if (s->side) cudaStreamDestroy(s->side);
     if (s->forkEv) cudaEventDestroy(s->forkEv);
@@ -314,8 +317,14 @@ static int create(const cc_Mesh* cage, int32_t D, uint32_t flags, cc_Subd** out)
     s->host->creases = (cc_Crease*)hc;
     s->host->vertexPoints = (cc_VertexPoint*)hp;
     if (!hh || !hc || !hp) { free_impl(s); return CCS_ERR_ALLOC; }
+    s->statsOff.assign((size_t)D + 1, 0);
+    int64_t nStats = 0;
+    for (int d = 1; d < D; ++d) {
+        s->statsOff[(size_t)d] = nStats;
+        nStats += lv[(size_t)d - 1].V;
+    }
     if (dmalloc(&s->he, heBytes) || dmalloc(&s->cr, crBytes) || dmalloc(&s->pts, ptBytes) ||
-        dmalloc(&s->err, sizeof(int))) {
+        dmalloc(&s->err, sizeof(int)) || dmalloc(&s->stats, sizeof(float4) * (size_t)(nStats > 0 ? nStats : 1))) {
         free_impl(s);
         return CCS_ERR_ALLOC;
     }
@@ -331,7 +340,7 @@ static int create(const cc_Mesh* cage, int32_t D, uint32_t flags, cc_Subd** out)
 
 // Operation identifiers (graph cache keys).
 enum Op {
-    OP_HALFEDGES = 1, OP_CREASES, OP_UVS,
+    OP_HALFEDGES = 1, OP_CREASES, OP_UVS, OP_RING_STATS,
     OP_POINTS_BASE = 16,        // + mode * 2 + det
     OP_REFINE_BASE = 64,        // + mode * 2 + det
 };
@@ -344,6 +353,7 @@ static cudaError_t enqueue(SubdImpl* s, int op, cudaStream_t st) {
     if (op == OP_HALFEDGES) return run_topology(c, true, false);
     if (op == OP_CREASES) return run_creases(c);
     if (op == OP_UVS) return uv ? run_topology(c, false, true) : cudaSuccess;
+    if (op == OP_RING_STATS) return run_ring_stats(c);
     if (op >= OP_REFINE_BASE || op >= OP_POINTS_BASE) {
         const bool refine = op >= OP_REFINE_BASE;
         const int k = op - (refine ? OP_REFINE_BASE : OP_POINTS_BASE);
@@ -355,6 +365,7 @@ static cudaError_t enqueue(SubdImpl* s, int op, cudaStream_t st) {
         if (refine) {
             e = run_topology(c, true, uv);
             if (e == cudaSuccess) e = run_creases(c);
+            if (e == cudaSuccess) e = run_ring_stats(c);
         }
         if (e == cudaSuccess) e = run_points(c, s->dc.pts, s->pts, mode, det);
         return e;
@@ -411,10 +422,6 @@ static int refine_op(cc_Subd* subd, int mode) {
     return ret(st);
 }
 
-// Float offset of the adjoint's ring statistics in a work buffer: after the
-// cumV x 3 gradient slots, rounded up to 16 bytes.
-static int64_t stats_offset(int64_t cumV) { return (3 * cumV + 3) & ~(int64_t)3; }
-
 // Adjoint over a caller-provided work buffer (`workFloats` floats); used by
 // the allocation-free entry point in ccs_noalloc.cu.
 int adjoint_into(const cc_Subd* subd, const float* gradPoints, float* gradCage, float* work, int64_t workFloats,
@@ -425,12 +432,7 @@ int adjoint_into(const cc_Subd* subd, const float* gradPoints, float* gradCage, 
     if (3 * s->cumV > workFloats) return CCS_ERR_SCRATCH_LIMIT;
     DeviceGuard g(s->device);
     Ctx c = s->ctx(stream);
-    // ring statistics after the gradient slots when they fit, else per-halfedge walks
-    float4* stats = nullptr;
-    const int64_t off = stats_offset(s->cumV);
-    if (off + 4 * adjoint_stats_count(c) <= workFloats && ((uintptr_t)work & 15u) == 0)
-        stats = reinterpret_cast<float4*>(work + off);
-    return run_adjoint(c, gradPoints, work, gradCage, s->cumV, stats) == cudaSuccess ? CCS_OK : CCS_ERR_CUDA;
+    return run_adjoint(c, gradPoints, work, gradCage, s->cumV) == cudaSuccess ? CCS_OK : CCS_ERR_CUDA;
 }
 
 int set_last_error(int status) { return ret(status); }
@@ -488,16 +490,18 @@ int ccs_RefineVertexPoints_NoCreases_Gather_cuda(cc_Subd* subd) {
 int ccs_RefineHalfedges_cuda(cc_Subd* subd) {
     SubdImpl* s = find(subd);
     if (!s) return ret(CCS_ERR_ARG);
-    const int st = execute(s, OP_HALFEDGES);
+    int st = execute(s, OP_HALFEDGES);
     if (st == CCS_OK) s->topo_ready = true;
+    if (st == CCS_OK && s->creases_ready) st = execute(s, OP_RING_STATS);
     return ret(st);
 }
 
 int ccs_RefineCreases_cuda(cc_Subd* subd) {
     SubdImpl* s = find(subd);
     if (!s) return ret(CCS_ERR_ARG);
-    const int st = execute(s, OP_CREASES);
+    int st = execute(s, OP_CREASES);
     if (st == CCS_OK) s->creases_ready = true;
+    if (st == CCS_OK && s->topo_ready) st = execute(s, OP_RING_STATS);
     return ret(st);
 }
 
@@ -603,12 +607,9 @@ int ccs_AdjointPointsDevice_cuda(cc_Subd* subd, const float* gradPoints, float* 
     if (!s || !gradPoints || !gradCage) return ret(CCS_ERR_ARG);
     if (!s->topo_ready || !s->creases_ready) return ret(CCS_ERR_STATE);
     DeviceGuard g(s->device);
+    if (!s->work && dmalloc(&s->work, sizeof(float) * 3 * (size_t)s->cumV)) return ret(CCS_ERR_ALLOC);
     Ctx c = s->ctx((cudaStream_t)stream);
-    const int64_t off = stats_offset(s->cumV);
-    if (!s->work && dmalloc(&s->work, sizeof(float) * (size_t)(off + 4 * adjoint_stats_count(c))))
-        return ret(CCS_ERR_ALLOC);
-    return ret(run_adjoint(c, gradPoints, s->work, gradCage, s->cumV, reinterpret_cast<float4*>(s->work + off)) ==
-                       cudaSuccess ? CCS_OK : CCS_ERR_CUDA);
+    return ret(run_adjoint(c, gradPoints, s->work, gradCage, s->cumV) == cudaSuccess ? CCS_OK : CCS_ERR_CUDA);
 }
 
 int ccs_LevelCounts_cuda(const cc_Mesh* cage, int32_t maxDepth, ccs_LevelCounts* out) {
@@ -667,7 +668,7 @@ int ccs_ReadProfile_cuda(cc_Subd* subd, ccs_KernelTime* out, int cap) {
 const char* ccs_KernelName_cuda(int kernel) {
     static const char* names[] = {"topology", "creases", "face_points", "edge_points", "vertex_points",
                                   "clear", "level_fused", "adjoint", "uvs", "level_points", "old_vertices",
-                                  "adj_stats", "adj_edges", "adj_faces", "adj_vertices"};
+                                  "ring_stats", "adj_edges", "adj_faces", "adj_vertices", "exact_points"};
     static_assert(sizeof(names) / sizeof(names[0]) == CCS_K_COUNT, "one name per kernel id");
     return (kernel >= 0 && kernel < CCS_K_COUNT) ? names[kernel] : "unknown";
 }

@@ -62,7 +62,15 @@ struct Ctx {
     // from and joined back into `stream` by the two events); null = serial
     cudaStream_t side = nullptr;
     cudaEvent_t forkEv = nullptr, joinEv = nullptr;
+    // ring statistics of the older vertices, level d (1 <= d < D) at
+    // stats + statsOff[d], V(d-1) entries; null = not kept
+    float4* stats = nullptr;
+    const int64_t* statsOff = nullptr;
 };
+
+inline float4* stats_at(const Ctx& c, int d) {
+    return (c.stats && c.statsOff && d >= 1 && d < c.D) ? c.stats + c.statsOff[d] : nullptr;
+}
 
 // Forward passes (ccs_forward.cu).  All return cudaError_t of the launches.
 cudaError_t run_topology(const Ctx& c, bool topo, bool uv);
@@ -74,16 +82,12 @@ cudaError_t run_points(const Ctx& c, const float* cagePts, float* pts, int mode,
 // CCS_POINTS_SCATTER or CCS_POINTS_NOCREASES_SCATTER.
 cudaError_t run_fused(const Ctx& c, bool topo, const float* cagePts, float* pts, int mode, bool deterministic);
 
-// Adjoint (ccs_adjoint.cu).  `work` holds cumV x 3 floats; `stats` (may be
-// null: the rings are then walked per halfedge) holds adjoint_stats_count(c)
-// float4 entries, 16-byte aligned.
-cudaError_t run_adjoint(const Ctx& c, const float* gradPts, float* work, float* gradCage, int64_t cumV,
-                        float4* stats);
-// Older vertices of the largest quad level the adjoint visits: max V(d-1), 1 <= d < D.
-inline int64_t adjoint_stats_count(const Ctx& c) {
-    int64_t m = 0;
-    for (int d = 1; d < c.D; ++d) m = c.lv[d - 1].V > m ? c.lv[d - 1].V : m;
-    return m;
-}
+// Ring statistics of the older vertices of every quad level (ccs_level.cu),
+// from the refined halfedges and creases.
+cudaError_t run_ring_stats(const Ctx& c);
+
+// Adjoint (ccs_adjoint.cu).  `work` holds cumV x 3 floats.  Reads the ring
+// statistics of c.stats when kept (else walks the rings per halfedge).
+cudaError_t run_adjoint(const Ctx& c, const float* gradPts, float* work, float* gradCage, int64_t cumV);
 
 }  // namespace ccs

@@ -1,6 +1,6 @@
 // ccs_level.cu -- fused refinement step for quad levels (depth d >= 1).
 //
-// One step d -> d+1 runs as two kernels:
+// One step d -> d+1 runs as kernel A then a vertex pass:
 //
 //   A  (one thread per parent halfedge; the 4 lanes of a face are adjacent)
 //      - reads the parent record with one 16-byte load (a warp reads 512
@@ -15,23 +15,25 @@
 //        halfedge: both halves of the edge rule, the twin face's point
 //        rebuilt from the twin quad's four records (the same value, bit for
 //        bit, as the twin quad's lanes store);
+//      - clears the vertex slots the default vertex pass accumulates into;
 //      - extra blocks refine the creases of the level.
-//   B  (depth d >= 2; vertex points, no atomics; two launches)
-//      - k_level_v: the older vertices (v < V(d-1)), one thread per
-//        vertex: one walk of the ring, every share, summed in increasing
-//        halfedge order;
-//      - k_level_b: one tile of halfedges per block, one thread per
-//        halfedge: a face centre's 4 shares meet in 4 lanes of a 16-lane
-//        group and an edge midpoint's 4 shares in the lane of the parent
-//        pair's owner (the twin side's 2 shares rebuilt from face and edge
-//        points), ring statistics from the known structure of refined
-//        levels, sums in increasing halfedge order.
-//   At depth 1 (children of n-gons) the vertex pass is one thread per vertex
-//   with the ring sorted (k_vertex_det).
+//   Vertex pass, default (k_level_b, one thread per halfedge): the vertex
+//      share of its halfedge with ring statistics from the refined structure
+//      (face centres, edge midpoints) or from the per-level table of the
+//      older vertices' statistics (k_ring_stats, built with the topology);
+//      a face centre's shares are summed in the warp and stored, the other
+//      shares go out as float atomics (pairs combined in the warp first).
+//   Vertex pass, deterministic (CCS_FLAG_DETERMINISTIC): every vertex summed
+//      by one thread in increasing halfedge order, which is the reference's
+//      one-thread order -- bit-identical points.  Depth >= 2: k_level_v (one
+//      thread per older vertex, one ring walk, on a second stream) beside
+//      k_level_b_exact (face centres in the warp, edge midpoints by the
+//      parent pair's owner with the twin side's shares rebuilt).  Depth 1:
+//      k_vertex_det (one thread per vertex, sorted ring).
 //
-// Every float expression is evaluated in the reference's order and every sum
-// in its one-thread order, so topology, creases, UVs and all points are
-// bit-identical to the reference's single-threaded refinement.
+// Kernel A and the exact pass evaluate every float expression in the
+// reference's order; topology, creases, UVs, face and edge points are
+// bit-identical to the reference in both modes.
 //
 // Twin relation used by A: for a twin pair (h, t), vertex(t) = vertex(next h)
 // and vertex(next t) = vertex(h).  The C ABI checks this on the cage (it is
@@ -64,21 +66,35 @@ k_level_a(LevelArgs a) {
     tile_level_a<kBlockL, RW, TOPO, UV, PTS, CREASED>(a, (int64_t)blockIdx.x * kBlockL, tile);
 }
 
-// kernel B (d >= 2): one tile of halfedges per block (face centres and edge
-// midpoints)
-template <int RW, bool CREASED>
+// default vertex pass: one tile of halfedges per block
+template <int RW, bool CREASED, bool STRUCT>
 __global__ void __launch_bounds__(kBlockL, 5)
 k_level_b(QuadView<RW> L, const float* __restrict__ pin, float* __restrict__ pout) {
-    tile_level_b<RW, CREASED>(L, pin, pout, (int64_t)blockIdx.x * kBlockL);
+    tile_level_b<RW, CREASED, STRUCT>(L, pin, pout, (int64_t)blockIdx.x * kBlockL);
 }
 
-// kernel V (d >= 2): one thread per older vertex (a separate launch, so that
-// kernel B keeps its small register footprint)
+// exact vertex pass (d >= 2): face centres and edge midpoints
+template <int RW, bool CREASED>
+__global__ void __launch_bounds__(kBlockL, 5)
+k_level_b_exact(QuadView<RW> L, const float* __restrict__ pin, float* __restrict__ pout) {
+    tile_level_b_exact<RW, CREASED>(L, pin, pout, (int64_t)blockIdx.x * kBlockL);
+}
+
+// exact vertex pass (d >= 2): one thread per older vertex (its own launch,
+// so that k_level_b_exact keeps its small register footprint)
 template <int RW, bool CREASED>
 __global__ void __launch_bounds__(kBlockL)
 k_level_v(QuadView<RW> L, const float* __restrict__ pin, float* __restrict__ pout, int32_t Vold) {
     const int64_t v = (int64_t)blockIdx.x * kBlockL + threadIdx.x;
     if (v < Vold) old_vertex_item<RW, CREASED>(L, pin, pout, (int32_t)v);
+}
+
+// ring statistics of the older vertices of level d (one thread per vertex)
+template <int RW>
+__global__ void __launch_bounds__(kBlockL)
+k_ring_stats(QuadView<RW> L, float4* __restrict__ out, int32_t Vold) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < Vold) ring_stats_item(L, out, (int32_t)i);
 }
 
 // ---------------------------------------------------------------------------
@@ -96,8 +112,47 @@ static QuadView<RW> quad_view_l(const Ctx& c, int d) {
     return L;
 }
 
+template <int RW>
+static void ring_stats_level(const Ctx& c, int d, cudaStream_t s) {
+    float4* out = stats_at(c, d);
+    if (!out || d < 1) return;
+    const int32_t Vold = c.lv[d - 1].V;
+    c.prof->begin(s, CCS_K_RING_STATS, d, Vold);
+    k_ring_stats<RW><<<nblocksL(Vold), kBlockL, 0, s>>>(quad_view_l<RW>(c, d), out, Vold);
+    c.prof->end(s);
+}
+
+cudaError_t run_ring_stats(const Ctx& c) {
+    for (int d = 1; d < c.D; ++d) {
+        if (c.rw == 4) ring_stats_level<4>(c, d, c.stream);
+        else ring_stats_level<3>(c, d, c.stream);
+    }
+    return cudaGetLastError();
+}
+
+// Work on the second stream between a fork from and a join into the main
+// stream; on the main stream itself when there is no second stream.
+struct Fork {
+    const Ctx& c;
+    bool on;
+    explicit Fork(const Ctx& cx) : c(cx), on(cx.side && cx.forkEv && cx.joinEv) {
+        if (on) {
+            cudaEventRecord(c.forkEv, c.stream);
+            cudaStreamWaitEvent(c.side, c.forkEv, 0);
+        }
+    }
+    cudaStream_t stream() const { return on ? c.side : c.stream; }
+    void join() {
+        if (on) {
+            cudaEventRecord(c.joinEv, c.side);
+            cudaStreamWaitEvent(c.stream, c.joinEv, 0);
+            on = false;
+        }
+    }
+};
+
 template <int RW, bool CREASED>
-static void level_a(const Ctx& c, int d, bool topo, bool uv, const float* pin, float* pout) {
+static void level_a(const Ctx& c, int d, bool topo, bool uv, const float* pin, float* pout, bool zeroV) {
     const Level& lv = c.lv[d];
     LevelArgs a;
     a.in = c.he + (int64_t)RW * lv.heOff;
@@ -107,6 +162,7 @@ static void level_a(const Ctx& c, int d, bool topo, bool uv, const float* pin, f
     a.pin = pin;
     a.pout = pout;
     a.H = lv.H; a.V = lv.V; a.F = lv.F; a.E = lv.E; a.C = lv.C;
+    a.zeroV = zeroV ? 1 : 0;
     const unsigned nb = nblocksL(lv.H) + (topo ? nblocksL(lv.C) : 0u);
     c.prof->begin(c.stream, topo ? CCS_K_LEVEL_FUSED : CCS_K_FACE_POINTS, d, lv.H);
     if (topo) {
@@ -120,31 +176,33 @@ static void level_a(const Ctx& c, int d, bool topo, bool uv, const float* pin, f
 
 template <int RW, bool CREASED>
 static void level_b(const Ctx& c, int d, const float* pin, float* pout) {
-    const QuadView<RW> L = quad_view_l<RW>(c, d);
-    const int32_t Vold = c.lv[d - 1].V;
-    // V (memory-latency bound) runs beside B (issue bound) when a second
-    // stream is available: both read only kernel A's output and write
-    // disjoint vertex slots
-    const bool fork = c.side && c.forkEv && c.joinEv;
-    cudaStream_t sv = fork ? c.side : c.stream;
-    if (fork) {
-        cudaEventRecord(c.forkEv, c.stream);
-        cudaStreamWaitEvent(c.side, c.forkEv, 0);
-    }
-    c.prof->begin(sv, CCS_K_OLD_VERTICES, d, Vold);
-    k_level_v<RW, CREASED><<<nblocksL(Vold), kBlockL, 0, sv>>>(L, pin, pout, Vold);
-    c.prof->end(sv);
+    QuadView<RW> L = quad_view_l<RW>(c, d);
+    L.ostats = stats_at(c, d);
     c.prof->begin(c.stream, CCS_K_LEVEL_POINTS, d, L.H);
-    k_level_b<RW, CREASED><<<nblocksL(L.H), kBlockL, 0, c.stream>>>(L, pin, pout);
+    const unsigned nb = nblocksL(L.H);
+    if (d >= 2) k_level_b<RW, CREASED, true><<<nb, kBlockL, 0, c.stream>>>(L, pin, pout);
+    else k_level_b<RW, CREASED, false><<<nb, kBlockL, 0, c.stream>>>(L, pin, pout);
     c.prof->end(c.stream);
-    if (fork) {
-        cudaEventRecord(c.joinEv, c.side);
-        cudaStreamWaitEvent(c.stream, c.joinEv, 0);
-    }
 }
 
-// Declared in ccs_forward.cu: the vertex pass of one quad level when the
-// fixed-order (deterministic) sum is requested, and the cage step.
+// exact pass, d >= 2: older vertices on the second stream beside the rest
+// (both read only kernel A's output and write disjoint vertex slots)
+template <int RW, bool CREASED>
+static void level_b_exact(const Ctx& c, int d, const float* pin, float* pout) {
+    const QuadView<RW> L = quad_view_l<RW>(c, d);
+    const int32_t Vold = c.lv[d - 1].V;
+    Fork f(c);
+    c.prof->begin(f.stream(), CCS_K_OLD_VERTICES, d, Vold);
+    k_level_v<RW, CREASED><<<nblocksL(Vold), kBlockL, 0, f.stream()>>>(L, pin, pout, Vold);
+    c.prof->end(f.stream());
+    c.prof->begin(c.stream, CCS_K_EXACT_POINTS, d, L.H);
+    k_level_b_exact<RW, CREASED><<<nblocksL(L.H), kBlockL, 0, c.stream>>>(L, pin, pout);
+    c.prof->end(c.stream);
+    f.join();
+}
+
+// Declared in ccs_forward.cu: the one-thread-per-vertex sorted pass of one
+// quad level, and the cage step.
 cudaError_t run_vertex_det_level(const Ctx& c, int d, const float* pin, float* pout, bool creased);
 cudaError_t run_cage_step(const Ctx& c, bool topo, bool uv, const float* cagePts, float* pout, int mode, bool det);
 
@@ -153,23 +211,29 @@ static cudaError_t fused_levels(const Ctx& c, bool topo, bool uv, float* pts, bo
     for (int d = 1; d < c.D; ++d) {
         const float* pin = pts + 3 * c.lv[d].ptOff;
         float* pout = pts + 3 * c.lv[d + 1].ptOff;
-        level_a<RW, CREASED>(c, d, topo, uv, pin, pout);
-        if (det || d == 1) {
+        // with the topology: the older vertices' ring statistics of level d
+        // (read by the default pass and by the adjoint) beside kernel A
+        Fork f(c);
+        if (topo) ring_stats_level<RW>(c, d, f.stream());
+        level_a<RW, CREASED>(c, d, topo, uv, pin, pout, !det);
+        f.join();
+        if (!det) {
+            level_b<RW, CREASED>(c, d, pin, pout);
+        } else if (d >= 2) {
+            level_b_exact<RW, CREASED>(c, d, pin, pout);
+        } else {
             const cudaError_t e = run_vertex_det_level(c, d, pin, pout, CREASED);
             if (e != cudaSuccess) return e;
-        } else {
-            level_b<RW, CREASED>(c, d, pin, pout);
         }
     }
     return cudaGetLastError();
 }
 
-// `det` selects the one-thread-per-vertex sorted pass (k_vertex_det) at every
-// depth; either way the sums follow the reference's one-thread order.
+// `det` selects the exact pass (the reference's one-thread summation order).
 cudaError_t run_fused(const Ctx& c, bool topo, const float* cagePts, float* pts, int mode, bool det) {
     const bool creased = mode == CCS_POINTS_SCATTER;
     const bool uv = c.cage->U > 0 && c.rw == 4;
-    cudaError_t e = run_cage_step(c, topo, uv, cagePts, pts + 3 * c.lv[1].ptOff, mode, true);
+    cudaError_t e = run_cage_step(c, topo, uv, cagePts, pts + 3 * c.lv[1].ptOff, mode, det);
     if (e != cudaSuccess) return e;
     if (c.rw == 4) return creased ? fused_levels<4, true>(c, topo, uv, pts, det) : fused_levels<4, false>(c, topo, uv, pts, det);
     return creased ? fused_levels<3, true>(c, topo, false, pts, det) : fused_levels<3, false>(c, topo, false, pts, det);

@@ -114,6 +114,7 @@ struct LevelArgs {
     const float* __restrict__ pin;      // depth-d points
     float* __restrict__ pout;           // depth-(d+1) points
     int32_t H, V, F, E, C;              // depth-d counts
+    int zeroV;                          // clear the vertex slots the atomic pass accumulates into
 };
 
 // `tile` is BLOCK * 4 * RW ints of shared memory; every thread of the block
@@ -172,6 +173,7 @@ __device__ __forceinline__ void tile_level_a(const LevelArgs& a, int64_t h0, int
         const f3 Fp = quad_face_point(p, qb);
         const f3 pn = shfl3(p, ln);
         if (valid && k == 0) st3(a.pout + 3 * ((int64_t)a.V + f), Fp);
+        if (a.zeroV && h64 < a.V) st3(a.pout + 3 * h64, zero3());
         // edge point, by the pair's larger halfedge; the smaller one's share
         // is added first, as a one-thread reference run adds it
         if (valid && h > tw) {
@@ -255,8 +257,110 @@ __device__ __forceinline__ void order2(int32_t& ia, f3& sa, int32_t& ib, f3& sb)
 }
 
 // ---------------------------------------------------------------------------
-// quad level d >= 2, kernel B body: face-centre and edge-midpoint vertex
-// points of depth d+1 from the halfedges [h0, h0 + blockDim) of depth d.
+// quad level d >= 1, kernel B body of the default pass: vertex points of
+// depth d+1 from the halfedges [h0, h0 + blockDim) of depth d, accumulated
+// with float atomics into slots kernel A cleared.
+// ---------------------------------------------------------------------------
+// One thread per halfedge h (child k = h & 3 of a parent halfedge).  Ring
+// statistics without walks: a face centre (k = 2) and an edge midpoint
+// (k = 1, 3) from the refined structure, an older vertex (k = 0) from the
+// per-level table L.ostats (one walk per vertex when the topology was
+// refined).  STRUCT (depth >= 2, a 16-lane group holds the children of one
+// parent quad): a face centre's four shares are summed in lanes 2, 6, 10, 14
+// in increasing halfedge order and stored (no atomic); an edge midpoint's two
+// shares on this side go out as one atomic triple (two per interior vertex:
+// the two additions commute, so the result does not depend on their order);
+// an older vertex's shares as one atomic triple each.  Depth 1 (children of
+// n-gons): one atomic triple per halfedge.
+template <int RW, bool CREASED, bool STRUCT>
+__device__ __forceinline__ void tile_level_b(const QuadView<RW>& L, const float* __restrict__ pin,
+                                             float* __restrict__ pout, int64_t h0) {
+    const unsigned full = 0xffffffffu;
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int64_t h64 = h0 + tid;
+    const bool valid = h64 < L.H;
+    const int32_t h = (int32_t)h64;
+    const int k = lane & 3, qb = lane & ~3, lp = qb | ((k + 3) & 3);
+    const float* fpt = pout + 3 * (int64_t)L.V;
+    const float* ept = pout + 3 * ((int64_t)L.V + L.F);
+    int32_t tw = -1, ed = 0, vx = 0;
+    if (valid) {
+        if constexpr (RW == 4) {
+            const int4 r = __ldg(reinterpret_cast<const int4*>(L.he) + h);
+            tw = r.x; ed = r.y; vx = r.z;
+        } else {
+            tw = __ldg(L.he + 3 * h64 + 0);
+            ed = __ldg(L.he + 3 * h64 + 1);
+            vx = __ldg(L.he + 3 * h64 + 2);
+        }
+    }
+    f3 p = zero3(), Fh = zero3(), Eh = zero3();
+    float4 st = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (valid) {
+        p = ld3(pin + 3 * (int64_t)vx);
+        Fh = ld3(fpt + 3 * (int64_t)(h >> 2));
+        Eh = ld3(ept + 3 * (int64_t)ed);
+        if (k == 0 && L.ostats) st = L.ostats[vx];
+    }
+    const f3 Ep = shfl3(Eh, lp);                      // edge point of prev(h)'s edge
+    const int32_t ped = __shfl_sync(full, ed, lp);
+    const int32_t ptw = __shfl_sync(full, tw, lp);
+    f3 s = zero3();
+    if (valid) {
+        float vpre, cpre = 0.0f, avgS = 0.0f;
+        bool bnd = false;
+        if (k == 2) {
+            vpre = L.d == 1 ? (float)L.t.fsz[L.t.he[(int64_t)CH_WORDS * (h >> 2) + CH_FACE]] : 4.0f;
+        } else if (k != 0) {
+            const int32_t eh = k == 1 ? ped : ed;        // one half of the parent edge
+            bnd = (k == 1 ? ptw : tw) < 0;
+            vpre = bnd ? 2.0f : 4.0f;
+            if (CREASED) {
+                const float sa = L.sharp(eh), sb = L.sharp(eh ^ 1);
+                const bool own = k == 3;                 // the walk from h skips its own edge
+                avgS = (bnd && own) ? sb : fadd(sa, sb);
+                cpre = (bnd && own) ? fsign(sb) : fadd(fsign(sa), fsign(sb));
+            }
+        } else if (L.ostats) {
+            // whole-ring statistics; on a boundary the walk from h skips h's own edge
+            bnd = st.w != 0.0f;
+            vpre = st.x;
+            if (CREASED) {
+                const float own = L.sharp(ed);
+                avgS = bnd ? fsub(st.y, own) : st.y;
+                cpre = bnd ? fsub(st.z, fsign(own)) : st.z;
+            }
+        } else {
+            const RingStats r = creased_ring_walk(L, h);
+            vpre = r.valence; cpre = r.creaseCount; avgS = r.avgS; bnd = r.fwd < 0;
+        }
+        s = quad_vertex_rule<CREASED>(p, Fh, Eh, Ep, vpre, cpre, avgS, bnd,
+                                      CREASED ? fsign(L.sharp(ed)) : 0.0f, CREASED ? fsign(L.sharp(ped)) : 0.0f);
+    }
+    float* o = pout + 3 * (int64_t)vx;
+    if (STRUCT) {
+        const f3 s4 = shfl_down3(s, 4), s8 = shfl_down3(s, 8), s12 = shfl_down3(s, 12);
+        const int partner = (lane & ~15) | ((((lane >> 2) + 1) & 3) << 2) | 3;
+        const f3 sA2 = shfl3(s, partner);
+        if (!valid) return;
+        if ((lane & 15) == 2) {
+            st3(o, add3(add3(add3(add3(zero3(), s), s4), s8), s12));
+        } else if (k == 1) {
+            // the pair in increasing halfedge order: child 3 of next(g) is
+            // below child 1 of g only when next(g) wraps to the face's first
+            atomic_add3(o, (lane & 12) == 12 ? add3(sA2, s) : add3(s, sA2));
+        } else if (k == 0) {
+            atomic_add3(o, s);
+        }
+    } else if (valid) {
+        atomic_add3(o, s);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// quad level d >= 2, kernel B body of the exact (deterministic) pass:
+// face-centre and edge-midpoint vertex points of depth d+1 from the
+// halfedges [h0, h0 + blockDim) of depth d.
 // ---------------------------------------------------------------------------
 // At depth d >= 2 halfedge h = 16 f + 4 j + k is child k of parent halfedge
 // g = 4 f + j of the parent quad f, and a 16-lane group holds the 16 children
@@ -279,8 +383,8 @@ __device__ __forceinline__ void order2(int32_t& ia, f3& sa, int32_t& ib, f3& sb)
 // Requires H to be a multiple of 16 (true at depth >= 2) and blockDim a
 // multiple of 32 with h0 a multiple of 32.
 template <int RW, bool CREASED>
-__device__ __forceinline__ void tile_level_b(const QuadView<RW>& L, const float* __restrict__ pin,
-                                             float* __restrict__ pout, int64_t h0) {
+__device__ __forceinline__ void tile_level_b_exact(const QuadView<RW>& L, const float* __restrict__ pin,
+                                                   float* __restrict__ pout, int64_t h0) {
     const unsigned full = 0xffffffffu;
     const int tid = threadIdx.x, lane = tid & 31;
     const int64_t h64 = h0 + tid;

@@ -41,12 +41,19 @@ def kernel_bytes(kernel: str, lv: dict, rec: int = 16) -> int:
         return int(12 * V)
     if kernel == "level_fused":
         # records in + children out + creases in and out + points in + face
-        # and edge points out
-        return int(rec * H + 4 * rec * H + 36 * C + 12 * V + 12 * F + 12 * E)
+        # and edge points out + the cleared vertex slots
+        return int(rec * H + 4 * rec * H + 36 * C + 12 * V + 12 * F + 12 * E + 12 * V)
     # depth d >= 2: F(d-1) = H / 16 face centres and E(d-1) = (E - H / 4) / 2
-    # edge midpoints are the vertices kernel B takes; the rest are older
+    # edge midpoints; the rest of the V vertices are older
     nb = H // 16 + (E - H // 4) // 2
     if kernel == "level_points":
+        # records + crease records + face and edge points + points in, the
+        # older vertices' ring statistics (16 B), vertex points out
+        return int(rec * H + 12 * C + 12 * F + 12 * E + 12 * V + 16 * max(V - nb, 0) + 12 * V)
+    if kernel == "ring_stats":
+        # records of children 0 and 3 walked, statistics out
+        return int(rec * H // 2 + 16 * max(V - nb, 0))
+    if kernel == "exact_points":
         # records + crease records + face and edge points in; the points of
         # its vertices in and out
         return int(rec * H + 12 * C + 12 * F + 12 * E + 24 * nb)

@@ -95,11 +95,10 @@ enum {
     CCS_FLAG_NO_UV = 1u << 0,          /* 12-byte halfedge records (the
                                           CC_DISABLE_UV build of the record) */
     CCS_FLAG_PAGEABLE_HOST = 1u << 1,  /* host arrays from malloc, not pinned */
-    CCS_FLAG_DETERMINISTIC = 1u << 2,  /* one thread per vertex with a sorted
-                                          ring at every depth (the fused path
-                                          is already in the reference's
-                                          order); with SEPARATE_PASSES, the
-                                          fixed-order sum instead of atomics */
+    CCS_FLAG_DETERMINISTIC = 1u << 2,  /* scatter points summed per vertex in
+                                          increasing halfedge order (the
+                                          reference's one-thread order: bit-
+                                          identical) instead of float atomics */
     CCS_FLAG_NO_GRAPH = 1u << 3,       /* launch kernels one by one instead
                                           of replaying a captured CUDA graph  */
     CCS_FLAG_SEPARATE_PASSES = 1u << 4 /* run the reference's pass structure
@@ -301,8 +300,9 @@ typedef struct {
 enum {
     CCS_K_TOPOLOGY = 0, CCS_K_CREASES = 1, CCS_K_FACE_POINTS = 2, CCS_K_EDGE_POINTS = 3,
     CCS_K_VERTEX_POINTS = 4, CCS_K_CLEAR = 5, CCS_K_LEVEL_FUSED = 6, CCS_K_ADJOINT = 7,
-    CCS_K_UVS = 8, CCS_K_LEVEL_POINTS = 9, CCS_K_OLD_VERTICES = 10, CCS_K_ADJ_STATS = 11,
-    CCS_K_ADJ_EDGES = 12, CCS_K_ADJ_FACES = 13, CCS_K_ADJ_VERTICES = 14, CCS_K_COUNT = 15
+    CCS_K_UVS = 8, CCS_K_LEVEL_POINTS = 9, CCS_K_OLD_VERTICES = 10, CCS_K_RING_STATS = 11,
+    CCS_K_ADJ_EDGES = 12, CCS_K_ADJ_FACES = 13, CCS_K_ADJ_VERTICES = 14, CCS_K_EXACT_POINTS = 15,
+    CCS_K_COUNT = 16
 };
 /* When enabled, every launch of the subd is bracketed by CUDA events on its
  * stream (and CUDA graphs are not used). */
