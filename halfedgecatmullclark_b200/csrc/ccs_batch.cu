@@ -213,6 +213,7 @@ k_batch_forward(BatchArgs a, int d) {
         la.pin = a.pts + 3 * (bc.pt + lv.ptOff);
         la.pout = a.pts + 3 * (bc.pt + bc.lv[d + 1].ptOff);
         la.H = lv.H; la.V = lv.V; la.F = lv.F; la.E = lv.E; la.C = lv.C;
+        la.zeroV = 0;                    // the batched vertex pass stores every slot
         if (bc.uv) tile_level_a<kBatchBlock, 4, TOPO, true, true, CREASED>(la, lt * kBatchBlock, tile);
         else tile_level_a<kBatchBlock, 4, TOPO, false, true, CREASED>(la, lt * kBatchBlock, tile);
         __syncthreads();   // the tile's shared memory is reused by the next tile

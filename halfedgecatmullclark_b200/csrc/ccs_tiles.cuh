@@ -114,7 +114,7 @@ struct LevelArgs {
     const float* __restrict__ pin;      // depth-d points
     float* __restrict__ pout;           // depth-(d+1) points
     int32_t H, V, F, E, C;              // depth-d counts
-    int zeroV;                          // clear the vertex slots the atomic pass accumulates into
+    int zeroV = 0;                      // clear the vertex slots the atomic pass accumulates into
 };
 
 // `tile` is BLOCK * 4 * RW ints of shared memory; every thread of the block
