@@ -526,8 +526,12 @@ def main():
     by = {}
     for r in recs:
         by.setdefault((r["kernel"], r["level"]), []).append(r["ms"])
+    steps_by = {k: v for k, v in by.items() if k[0] == "step"}
+    by = {k: v for k, v in by.items() if k[0] != "step"}
     total_prof = sum(sum(v) for v in by.values())
-    dom_key = max(by, key=lambda k: sum(by[k]))
+    # the dominant kernel of the subd's own stream (ring_stats runs on the
+    # second stream beside kernel A: its events span the overlap)
+    dom_key = max((k for k in by if k[0] != "ring_stats"), key=lambda k: sum(by[k]))
     dom_ms = statistics.mean(by[dom_key])
     dom_bytes = metrics.kernel_bytes(dom_key[0], levels[dom_key[1]], rec_bytes)
     peak, peak_kind = measured_peak()
@@ -539,7 +543,12 @@ def main():
                       for k, v in by.items()), key=lambda x: -x["share"])
     per_depth = []
     for d in range(w.depth):
-        ms = sum(statistics.mean(v) for k, v in by.items() if k[1] == d)
+        # a whole step's device time (its kernels overlap on two streams);
+        # the sum of its kernels' times where no step record exists
+        if ("step", d) in steps_by:
+            ms = statistics.mean(steps_by[("step", d)])
+        else:
+            ms = sum(statistics.mean(v) for k, v in by.items() if k[1] == d)
         nb = metrics.level_bytes(levels[d], levels[d + 1], rec_bytes, subd.record_words == 4, d == 0, w.cage.U)
         per_depth.append({"depth": d + 1, "ms": ms, "refined_halfedges": levels[d + 1]["H"],
                           "halfedges_per_s": levels[d + 1]["H"] / (ms / 1e3), "alg_bytes": nb,
@@ -566,7 +575,7 @@ def main():
     e2e_total = max_over_ranks(sum(e2e_ms), world)
     h2d = 12 * w.cage.V
     d2h = 4 * subd.record_words * subd.cumH + 12 * subd.cumC + 12 * subd.cumV
-    launches = len([r for r in recs if r["kernel"] != "clear"]) // max(1, args.steps)
+    launches = len([r for r in recs if r["kernel"] not in ("clear", "step")]) // max(1, args.steps)
 
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -135,17 +135,19 @@ static bool twins_consistent(const cc_Mesh* m) {
 // ---------------------------------------------------------------------------
 // profiling
 // ---------------------------------------------------------------------------
-void Profiler::begin(cudaStream_t s, int kernel, int level, int64_t units) {
-    if (!on) return;
+int Profiler::begin(cudaStream_t s, int kernel, int level, int64_t units) {
+    if (!on) return -1;
     TimedLaunch t{kernel, level, units, nullptr, nullptr};
     cudaEventCreate(&t.a);
     cudaEventCreate(&t.b);
     cudaEventRecord(t.a, s);
     pending.push_back(t);
+    return (int)pending.size() - 1;
 }
-void Profiler::end(cudaStream_t s) {
+void Profiler::end(cudaStream_t s, int index) {
     if (!on || pending.empty()) return;
-    cudaEventRecord(pending.back().b, s);
+    if (index >= 0 && index < (int)pending.size()) cudaEventRecord(pending[(size_t)index].b, s);
+    else cudaEventRecord(pending.back().b, s);
 }
 
 // ---------------------------------------------------------------------------
@@ -668,7 +670,7 @@ int ccs_ReadProfile_cuda(cc_Subd* subd, ccs_KernelTime* out, int cap) {
 const char* ccs_KernelName_cuda(int kernel) {
     static const char* names[] = {"topology", "creases", "face_points", "edge_points", "vertex_points",
                                   "clear", "level_fused", "adjoint", "uvs", "level_points", "old_vertices",
-                                  "ring_stats", "adj_edges", "adj_faces", "adj_vertices", "exact_points"};
+                                  "ring_stats", "adj_edges", "adj_faces", "adj_vertices", "exact_points", "step"};
     static_assert(sizeof(names) / sizeof(names[0]) == CCS_K_COUNT, "one name per kernel id");
     return (kernel >= 0 && kernel < CCS_K_COUNT) ? names[kernel] : "unknown";
 }

@@ -43,8 +43,9 @@ struct TimedLaunch {
 struct Profiler {
     bool on = false;
     std::vector<TimedLaunch> pending;
-    void begin(cudaStream_t s, int kernel, int level, int64_t units);
-    void end(cudaStream_t s);
+    // begin returns the record's index; end closes that record (or the last)
+    int begin(cudaStream_t s, int kernel, int level, int64_t units);
+    void end(cudaStream_t s, int index = -1);
 };
 
 // Launch context: everything a refine pass needs.

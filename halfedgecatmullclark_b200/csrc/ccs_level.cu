@@ -50,20 +50,29 @@ static constexpr int kBlockL = 256;
 
 static inline unsigned nblocksL(int64_t n) { return (unsigned)((n + kBlockL - 1) / kBlockL); }
 
-// kernel A: blocks [0, nbH) take one tile of parent halfedges each, the
-// blocks after them refine the level's creases.
-template <int RW, bool TOPO, bool UV, bool PTS, bool CREASED>
-__global__ void __launch_bounds__(kBlockL)
-k_level_a(LevelArgs a) {
-    const int nbH = (a.H + kBlockL - 1) / kBlockL;
-    if ((int)blockIdx.x >= nbH) {
-        if (!TOPO) return;
-        const int64_t i = (int64_t)(blockIdx.x - nbH) * kBlockL + threadIdx.x;
-        if (i < a.C) crease_item(a.crIn, a.crOut, (int32_t)i);
-        return;
-    }
+// kernel A, persistent form: each block runs tiles blockIdx, blockIdx + grid,
+// ... through one shared tile; the next tile's parent records are loaded
+// while the current one is processed, and a tile's bulk store stays in
+// flight while the next tile computes.  Crease tiles follow.
+template <int RW, bool TOPO, bool UV, bool CREASED>
+__global__ void __launch_bounds__(kBlockL, 5)
+k_level_a_persist(LevelArgs a, int64_t nTiles, int64_t nCreaseTiles) {
     __shared__ __align__(128) int32_t tile[kBlockL * 4 * RW];
-    tile_level_a<kBlockL, RW, TOPO, UV, PTS, CREASED>(a, (int64_t)blockIdx.x * kBlockL, tile);
+    const int tid = threadIdx.x;
+    int64_t t = blockIdx.x;
+    ARec r = load_arec<RW>(a.in, t * kBlockL + tid, a.H);
+    for (; t < nTiles; t += gridDim.x) {
+        const ARec rn = load_arec<RW>(a.in, (t + gridDim.x) * kBlockL + tid, a.H);
+        tile_level_a_rec<kBlockL, RW, TOPO, UV, true, CREASED, true>(a, t * kBlockL, tile, r);
+        r = rn;
+    }
+    if (TOPO) {
+        for (int64_t c = blockIdx.x; c < nCreaseTiles; c += gridDim.x) {
+            const int64_t i = c * kBlockL + tid;
+            if (i < a.C) crease_item(a.crIn, a.crOut, (int32_t)i);
+        }
+        if (tid == 0) bulk_store_wait();              // the last store has read the tile
+    }
 }
 
 // default vertex pass: one tile of halfedges per block
@@ -151,6 +160,25 @@ struct Fork {
     }
 };
 
+// Persistent grid: as many blocks as fit on the device at once (occupancy of
+// the kernel, looked up once per kernel and device), never more than tiles.
+template <class K>
+static void launch_persist(K kernel, int64_t nT, int64_t nC, const LevelArgs& a, cudaStream_t s) {
+    static int cachedDev = -1, cachedGrid = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev != cachedDev || cachedGrid <= 0) {
+        int sms = 0, per = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kBlockL, 0);
+        cachedGrid = sms * (per > 0 ? per : 1);
+        cachedDev = dev;
+    }
+    const int64_t work = nT > nC ? nT : nC;
+    const unsigned grid = (unsigned)(work < cachedGrid ? (work > 0 ? work : 1) : cachedGrid);
+    kernel<<<grid, kBlockL, 0, s>>>(a, nT, nC);
+}
+
 template <int RW, bool CREASED>
 static void level_a(const Ctx& c, int d, bool topo, bool uv, const float* pin, float* pout, bool zeroV) {
     const Level& lv = c.lv[d];
@@ -163,13 +191,13 @@ static void level_a(const Ctx& c, int d, bool topo, bool uv, const float* pin, f
     a.pout = pout;
     a.H = lv.H; a.V = lv.V; a.F = lv.F; a.E = lv.E; a.C = lv.C;
     a.zeroV = zeroV ? 1 : 0;
-    const unsigned nb = nblocksL(lv.H) + (topo ? nblocksL(lv.C) : 0u);
+    const int64_t nT = nblocksL(lv.H), nC = topo ? nblocksL(lv.C) : 0;
     c.prof->begin(c.stream, topo ? CCS_K_LEVEL_FUSED : CCS_K_FACE_POINTS, d, lv.H);
     if (topo) {
-        if (RW == 4 && uv) k_level_a<RW, true, true, true, CREASED><<<nb, kBlockL, 0, c.stream>>>(a);
-        else k_level_a<RW, true, false, true, CREASED><<<nb, kBlockL, 0, c.stream>>>(a);
+        if (RW == 4 && uv) launch_persist(k_level_a_persist<RW, true, true, CREASED>, nT, nC, a, c.stream);
+        else launch_persist(k_level_a_persist<RW, true, false, CREASED>, nT, nC, a, c.stream);
     } else {
-        k_level_a<RW, false, false, true, CREASED><<<nb, kBlockL, 0, c.stream>>>(a);
+        launch_persist(k_level_a_persist<RW, false, false, CREASED>, nT, nC, a, c.stream);
     }
     c.prof->end(c.stream);
 }
@@ -211,6 +239,7 @@ static cudaError_t fused_levels(const Ctx& c, bool topo, bool uv, float* pts, bo
     for (int d = 1; d < c.D; ++d) {
         const float* pin = pts + 3 * c.lv[d].ptOff;
         float* pout = pts + 3 * c.lv[d + 1].ptOff;
+        const int step = c.prof->begin(c.stream, CCS_K_STEP, d, c.lv[d].H);
         // with the topology: the older vertices' ring statistics of level d
         // (read by the default pass and by the adjoint) beside kernel A
         Fork f(c);
@@ -225,6 +254,7 @@ static cudaError_t fused_levels(const Ctx& c, bool topo, bool uv, float* pts, bo
             const cudaError_t e = run_vertex_det_level(c, d, pin, pout, CREASED);
             if (e != cudaSuccess) return e;
         }
+        c.prof->end(c.stream, step);
     }
     return cudaGetLastError();
 }
@@ -233,7 +263,9 @@ static cudaError_t fused_levels(const Ctx& c, bool topo, bool uv, float* pts, bo
 cudaError_t run_fused(const Ctx& c, bool topo, const float* cagePts, float* pts, int mode, bool det) {
     const bool creased = mode == CCS_POINTS_SCATTER;
     const bool uv = c.cage->U > 0 && c.rw == 4;
+    const int step = c.prof->begin(c.stream, CCS_K_STEP, 0, c.lv[0].H);
     cudaError_t e = run_cage_step(c, topo, uv, cagePts, pts + 3 * c.lv[1].ptOff, mode, det);
+    c.prof->end(c.stream, step);
     if (e != cudaSuccess) return e;
     if (c.rw == 4) return creased ? fused_levels<4, true>(c, topo, uv, pts, det) : fused_levels<4, false>(c, topo, uv, pts, det);
     return creased ? fused_levels<3, true>(c, topo, false, pts, det) : fused_levels<3, false>(c, topo, false, pts, det);

@@ -36,12 +36,18 @@ __device__ __forceinline__ int32_t uv_enc_fast(float u, float v) {
 }
 
 // One thread writes `bytes` of shared memory to global memory through the
-// TMA engine (no multicast) and waits until the shared source has been read.
+// TMA engine (no multicast); with WAIT it then waits until the shared source
+// has been read, else the caller waits (bulk_store_wait) before it reuses or
+// releases the shared memory.
+template <bool WAIT = true>
 __device__ __forceinline__ void bulk_store_tile(void* gdst, const void* ssrc, uint32_t bytes) {
     const uint32_t s = (uint32_t)__cvta_generic_to_shared(ssrc);
     asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;"
                  :: "l"(gdst), "r"(s), "r"(bytes) : "memory");
     asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+    if (WAIT) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_store_wait() {
     asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
 }
 
@@ -117,32 +123,45 @@ struct LevelArgs {
     int zeroV = 0;                      // clear the vertex slots the atomic pass accumulates into
 };
 
+// One parent record (twin, edge, vertex, uv); zeros past the level's end.
+struct ARec {
+    int32_t tw, ed, vx, uv;
+};
+template <int RW>
+__device__ __forceinline__ ARec load_arec(const int32_t* __restrict__ in, int64_t h64, int64_t H) {
+    ARec r{0, 0, 0, 0};
+    if (h64 < H) {
+        if constexpr (RW == 4) {
+            const int4 q = __ldg(reinterpret_cast<const int4*>(in) + h64);
+            r.tw = q.x; r.ed = q.y; r.vx = q.z; r.uv = q.w;
+        } else {
+            r.tw = __ldg(in + 3 * h64 + 0);
+            r.ed = __ldg(in + 3 * h64 + 1);
+            r.vx = __ldg(in + 3 * h64 + 2);
+        }
+    }
+    return r;
+}
+
 // `tile` is BLOCK * 4 * RW ints of shared memory; every thread of the block
-// must call this with the same h0.
-template <int BLOCK, int RW, bool TOPO, bool UV, bool PTS, bool CREASED>
-__device__ __forceinline__ void tile_level_a(const LevelArgs& a, int64_t h0, int32_t* tile) {
+// must call this with the same h0, and `rec` = its parent record.  PERSIST:
+// the block runs many tiles through one shared tile, so the previous tile's
+// bulk store must have read it before it is rewritten, and this tile's store
+// is left in flight (the kernel waits for it before the block exits).
+template <int BLOCK, int RW, bool TOPO, bool UV, bool PTS, bool CREASED, bool PERSIST = false>
+__device__ __forceinline__ void tile_level_a_rec(const LevelArgs& a, int64_t h0, int32_t* tile, ARec rec) {
     const int tid = threadIdx.x, lane = tid & 31;
     const int64_t h64 = h0 + tid;
     const bool valid = h64 < a.H;
     const int32_t h = (int32_t)h64;
     const int k = lane & 3, qb = lane & ~3;
-    int32_t tw = 0, ed = 0, vx = 0, uv = 0;
-    if (valid) {
-        if constexpr (RW == 4) {
-            const int4 r = __ldg(reinterpret_cast<const int4*>(a.in) + h);
-            tw = r.x; ed = r.y; vx = r.z; uv = r.w;
-        } else {
-            tw = __ldg(a.in + 3 * h64 + 0);
-            ed = __ldg(a.in + 3 * h64 + 1);
-            vx = __ldg(a.in + 3 * h64 + 2);
-        }
-    }
+    const int32_t tw = rec.tw, ed = rec.ed, vx = rec.vx, uv = rec.uv;
     const int ln = qb | ((k + 1) & 3), lp = qb | ((k + 3) & 3), lo = qb | ((k + 2) & 3);
     const int32_t prev = (h & ~3) | ((k + 3) & 3), next = (h & ~3) | ((k + 1) & 3), f = h >> 2;
+    int32_t c_tw[4] = {0, 0, 0, 0}, c_ed[4] = {0, 0, 0, 0}, c_vx[4] = {0, 0, 0, 0}, uvc[4] = {uv, 0, 0, 0};
     if (TOPO) {
         const int32_t ptw = __shfl_sync(0xffffffffu, tw, lp);
         const int32_t ped = __shfl_sync(0xffffffffu, ed, lp);
-        int32_t uvc[4] = {uv, 0, 0, 0};
         if (UV) {
             const float u = uv_dec_fast((uint32_t)uv), v = uv_dec_fast((uint32_t)uv >> 16);
             const float un = __shfl_sync(0xffffffffu, u, ln), vn = __shfl_sync(0xffffffffu, v, ln);
@@ -153,20 +172,10 @@ __device__ __forceinline__ void tile_level_a(const LevelArgs& a, int64_t h0, int
                                  fquarter(fadd(fadd(fadd(v, vn), vo), vp)));
             uvc[3] = uv_enc_fast(flerp(u, up, 0.5f), flerp(v, vp, 0.5f));
         }
-        int32_t* t = tile + tid * 4 * RW;
-        const int32_t c_tw[4] = {child(qnext(tw), 3), child(next, 2), child(prev, 1), child(ptw, 0)};
-        const int32_t c_ed[4] = {2 * ed + (h > tw ? 0 : 1), 2 * a.E + h, 2 * a.E + prev,
-                                 2 * ped + (prev > ptw ? 1 : 0)};
-        const int32_t c_vx[4] = {vx, a.V + a.F + ed, a.V + f, a.V + a.F + ped};
-        if constexpr (RW == 4) {
-#pragma unroll
-            for (int m = 0; m < 4; ++m)
-                reinterpret_cast<int4*>(t)[m] = make_int4(c_tw[m], c_ed[m], c_vx[m], UV ? uvc[m] : 0);
-        } else {
-#pragma unroll
-            for (int m = 0; m < 4; ++m) { t[3 * m] = c_tw[m]; t[3 * m + 1] = c_ed[m]; t[3 * m + 2] = c_vx[m]; }
-        }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        c_tw[0] = child(qnext(tw), 3); c_tw[1] = child(next, 2); c_tw[2] = child(prev, 1); c_tw[3] = child(ptw, 0);
+        c_ed[0] = 2 * ed + (h > tw ? 0 : 1); c_ed[1] = 2 * a.E + h; c_ed[2] = 2 * a.E + prev;
+        c_ed[3] = 2 * ped + (prev > ptw ? 1 : 0);
+        c_vx[0] = vx; c_vx[1] = a.V + a.F + ed; c_vx[2] = a.V + f; c_vx[3] = a.V + a.F + ped;
     }
     if (PTS) {
         const f3 p = valid ? ld3(a.pin + 3 * (int64_t)vx) : zero3();
@@ -181,13 +190,20 @@ __device__ __forceinline__ void tile_level_a(const LevelArgs& a, int64_t h0, int
             const f3 sh_h = edge_share<CREASED>(p, pn, Fp, tw < 0, w);
             f3 E;
             if (tw >= 0) {
-                const int32_t tb = tw & ~3;
-                f3 Ft = zero3();
+                // the twin quad's face point, in its halfedge order; by the
+                // twin relation vertex(t) = vertex(next h) and vertex(next t)
+                // = vertex(h), so only its other two vertices are read
+                const int32_t tb = tw & ~3, kt = tw & 3;
+                f3 q[4];
 #pragma unroll
                 for (int i = 0; i < 4; ++i) {
-                    const int32_t tv = __ldg(a.in + (int64_t)RW * (tb + i) + 2);
-                    Ft = add3(Ft, quarter3(ld3(a.pin + 3 * (int64_t)tv)));
+                    if (i == kt) q[i] = pn;
+                    else if (i == ((kt + 1) & 3)) q[i] = p;
+                    else q[i] = ld3(a.pin + 3 * (int64_t)__ldg(a.in + (int64_t)RW * (tb + i) + 2));
                 }
+                f3 Ft = zero3();
+#pragma unroll
+                for (int i = 0; i < 4; ++i) Ft = add3(Ft, quarter3(q[i]));
                 const f3 sh_t = edge_share<CREASED>(pn, p, Ft, false, w);
                 E = add3(add3(zero3(), sh_t), sh_h);
             } else {
@@ -197,12 +213,31 @@ __device__ __forceinline__ void tile_level_a(const LevelArgs& a, int64_t h0, int
         }
     }
     if (TOPO) {
+        if (PERSIST) {
+            if (tid == 0) bulk_store_wait();            // the previous tile's store has read the tile
+            __syncthreads();
+        }
+        int32_t* t = tile + tid * 4 * RW;
+        if constexpr (RW == 4) {
+#pragma unroll
+            for (int m = 0; m < 4; ++m)
+                reinterpret_cast<int4*>(t)[m] = make_int4(c_tw[m], c_ed[m], c_vx[m], UV ? uvc[m] : 0);
+        } else {
+#pragma unroll
+            for (int m = 0; m < 4; ++m) { t[3 * m] = c_tw[m]; t[3 * m + 1] = c_ed[m]; t[3 * m + 2] = c_vx[m]; }
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (tid == 0) {
             const int64_t n = (a.H - h0) < BLOCK ? (a.H - h0) : BLOCK;
-            bulk_store_tile(a.out + 4 * RW * h0, tile, (uint32_t)(n * 16 * RW));
+            bulk_store_tile<!PERSIST>(a.out + 4 * RW * h0, tile, (uint32_t)(n * 16 * RW));
         }
     }
+}
+
+template <int BLOCK, int RW, bool TOPO, bool UV, bool PTS, bool CREASED>
+__device__ __forceinline__ void tile_level_a(const LevelArgs& a, int64_t h0, int32_t* tile) {
+    tile_level_a_rec<BLOCK, RW, TOPO, UV, PTS, CREASED>(a, h0, tile, load_arec<RW>(a.in, h0 + threadIdx.x, a.H));
 }
 
 // ---------------------------------------------------------------------------

@@ -302,7 +302,7 @@ enum {
     CCS_K_VERTEX_POINTS = 4, CCS_K_CLEAR = 5, CCS_K_LEVEL_FUSED = 6, CCS_K_ADJOINT = 7,
     CCS_K_UVS = 8, CCS_K_LEVEL_POINTS = 9, CCS_K_OLD_VERTICES = 10, CCS_K_RING_STATS = 11,
     CCS_K_ADJ_EDGES = 12, CCS_K_ADJ_FACES = 13, CCS_K_ADJ_VERTICES = 14, CCS_K_EXACT_POINTS = 15,
-    CCS_K_COUNT = 16
+    CCS_K_STEP = 16 /* a whole refinement step d -> d+1, on the subd's stream */, CCS_K_COUNT = 17
 };
 /* When enabled, every launch of the subd is bracketed by CUDA events on its
  * stream (and CUDA graphs are not used). */
