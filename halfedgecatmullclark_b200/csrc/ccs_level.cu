@@ -50,29 +50,23 @@ static constexpr int kBlockL = 256;
 
 static inline unsigned nblocksL(int64_t n) { return (unsigned)((n + kBlockL - 1) / kBlockL); }
 
-// kernel A, persistent form: each block runs tiles blockIdx, blockIdx + grid,
-// ... through one shared tile; the next tile's parent records are loaded
-// while the current one is processed, and a tile's bulk store stays in
-// flight while the next tile computes.  Crease tiles follow.
+// kernel A: blocks [0, nbH) take one tile of parent halfedges each, the
+// blocks after them refine the level's creases.  (A persistent form that
+// prefetched the next tile's records and left each bulk store in flight ran
+// 1.5x slower at depth 5: 5 resident blocks per SM instead of 8 hid less of
+// the gather latency than the extra overlap won.)
 template <int RW, bool TOPO, bool UV, bool CREASED>
-__global__ void __launch_bounds__(kBlockL, 5)
-k_level_a_persist(LevelArgs a, int64_t nTiles, int64_t nCreaseTiles) {
+__global__ void __launch_bounds__(kBlockL)
+k_level_a(LevelArgs a) {
+    const int nbH = (a.H + kBlockL - 1) / kBlockL;
+    if ((int)blockIdx.x >= nbH) {
+        if (!TOPO) return;
+        const int64_t i = (int64_t)(blockIdx.x - nbH) * kBlockL + threadIdx.x;
+        if (i < a.C) crease_item(a.crIn, a.crOut, (int32_t)i);
+        return;
+    }
     __shared__ __align__(128) int32_t tile[kBlockL * 4 * RW];
-    const int tid = threadIdx.x;
-    int64_t t = blockIdx.x;
-    ARec r = load_arec<RW>(a.in, t * kBlockL + tid, a.H);
-    for (; t < nTiles; t += gridDim.x) {
-        const ARec rn = load_arec<RW>(a.in, (t + gridDim.x) * kBlockL + tid, a.H);
-        tile_level_a_rec<kBlockL, RW, TOPO, UV, true, CREASED, true>(a, t * kBlockL, tile, r);
-        r = rn;
-    }
-    if (TOPO) {
-        for (int64_t c = blockIdx.x; c < nCreaseTiles; c += gridDim.x) {
-            const int64_t i = c * kBlockL + tid;
-            if (i < a.C) crease_item(a.crIn, a.crOut, (int32_t)i);
-        }
-        if (tid == 0) bulk_store_wait();              // the last store has read the tile
-    }
+    tile_level_a<kBlockL, RW, TOPO, UV, true, CREASED>(a, (int64_t)blockIdx.x * kBlockL, tile);
 }
 
 // default vertex pass: one tile of halfedges per block
@@ -98,12 +92,20 @@ k_level_v(QuadView<RW> L, const float* __restrict__ pin, float* __restrict__ pou
     if (v < Vold) old_vertex_item<RW, CREASED>(L, pin, pout, (int32_t)v);
 }
 
-// ring statistics of the older vertices of level d (one thread per vertex)
+// ring statistics of the older vertices of level d: shape (valence and
+// boundary, one thread per vertex, no level data read), then the creased
+// edges' sharpness (one thread per crease of the level, float atomics)
+__global__ void __launch_bounds__(kBlockL)
+k_shape_stats(CageTables t, int32_t d, float4* __restrict__ out, int32_t Vold) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < Vold) shape_stats_item(t, d, out, (int32_t)i);
+}
+
 template <int RW>
 __global__ void __launch_bounds__(kBlockL)
-k_ring_stats(QuadView<RW> L, float4* __restrict__ out, int32_t Vold) {
+k_crease_stats(QuadView<RW> L, float4* __restrict__ out, int32_t Vold) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < Vold) ring_stats_item(L, out, (int32_t)i);
+    if (i < L.C) crease_stats_item(L, Vold, out, (int32_t)i);
 }
 
 // ---------------------------------------------------------------------------
@@ -126,8 +128,10 @@ static void ring_stats_level(const Ctx& c, int d, cudaStream_t s) {
     float4* out = stats_at(c, d);
     if (!out || d < 1) return;
     const int32_t Vold = c.lv[d - 1].V;
+    const QuadView<RW> L = quad_view_l<RW>(c, d);
     c.prof->begin(s, CCS_K_RING_STATS, d, Vold);
-    k_ring_stats<RW><<<nblocksL(Vold), kBlockL, 0, s>>>(quad_view_l<RW>(c, d), out, Vold);
+    k_shape_stats<<<nblocksL(Vold), kBlockL, 0, s>>>(L.t, d, out, Vold);
+    if (L.C > 0) k_crease_stats<RW><<<nblocksL(L.C), kBlockL, 0, s>>>(L, out, Vold);
     c.prof->end(s);
 }
 
@@ -160,25 +164,6 @@ struct Fork {
     }
 };
 
-// Persistent grid: as many blocks as fit on the device at once (occupancy of
-// the kernel, looked up once per kernel and device), never more than tiles.
-template <class K>
-static void launch_persist(K kernel, int64_t nT, int64_t nC, const LevelArgs& a, cudaStream_t s) {
-    static int cachedDev = -1, cachedGrid = 0;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev != cachedDev || cachedGrid <= 0) {
-        int sms = 0, per = 0;
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kBlockL, 0);
-        cachedGrid = sms * (per > 0 ? per : 1);
-        cachedDev = dev;
-    }
-    const int64_t work = nT > nC ? nT : nC;
-    const unsigned grid = (unsigned)(work < cachedGrid ? (work > 0 ? work : 1) : cachedGrid);
-    kernel<<<grid, kBlockL, 0, s>>>(a, nT, nC);
-}
-
 template <int RW, bool CREASED>
 static void level_a(const Ctx& c, int d, bool topo, bool uv, const float* pin, float* pout, bool zeroV) {
     const Level& lv = c.lv[d];
@@ -191,13 +176,13 @@ static void level_a(const Ctx& c, int d, bool topo, bool uv, const float* pin, f
     a.pout = pout;
     a.H = lv.H; a.V = lv.V; a.F = lv.F; a.E = lv.E; a.C = lv.C;
     a.zeroV = zeroV ? 1 : 0;
-    const int64_t nT = nblocksL(lv.H), nC = topo ? nblocksL(lv.C) : 0;
+    const unsigned nb = nblocksL(lv.H) + (topo ? nblocksL(lv.C) : 0u);
     c.prof->begin(c.stream, topo ? CCS_K_LEVEL_FUSED : CCS_K_FACE_POINTS, d, lv.H);
     if (topo) {
-        if (RW == 4 && uv) launch_persist(k_level_a_persist<RW, true, true, CREASED>, nT, nC, a, c.stream);
-        else launch_persist(k_level_a_persist<RW, true, false, CREASED>, nT, nC, a, c.stream);
+        if (RW == 4 && uv) k_level_a<RW, true, true, CREASED><<<nb, kBlockL, 0, c.stream>>>(a);
+        else k_level_a<RW, true, false, CREASED><<<nb, kBlockL, 0, c.stream>>>(a);
     } else {
-        launch_persist(k_level_a_persist<RW, false, false, CREASED>, nT, nC, a, c.stream);
+        k_level_a<RW, false, false, CREASED><<<nb, kBlockL, 0, c.stream>>>(a);
     }
     c.prof->end(c.stream);
 }

@@ -900,6 +900,79 @@ __device__ __forceinline__ void ring_stats_item(const QuadView<RW>& L, float4* _
     out[v] = make_float4(n, tot, cnt, bnd ? 1.0f : 0.0f);
 }
 
+// The same statistics without walking the level: the valence and boundary of
+// an older vertex are those it was created with (refinement keeps a
+// vertex's ring), and its creased edges are found from the crease side.
+//
+// Valence (outgoing halfedges) and boundary of vertex v < V(d-1) at quad
+// level d >= 1, from the vertex numbering and the cage alone: a face centre
+// of a level >= 1 quad has 4 (interior); of a cage face, the face's size; an
+// edge midpoint 4, or 2 when its edge descends from a cage boundary edge
+// (edges created inside faces are interior); a cage vertex its cage ring.
+__device__ __forceinline__ void old_vertex_shape(const CageTables& t, int32_t v, int32_t d, int32_t& valence,
+                                                 bool& bnd) {
+    for (int32_t hd = d; hd > 1; --hd) {
+        const int32_t Vc = cnt_V(t.n, hd - 1), Fc = cnt_F(t.n, hd - 1);
+        if (v >= Vc + Fc) {                          // midpoint of edge e of level hd - 1
+            int32_t e = v - Vc - Fc, j = hd - 1;
+            for (; j >= 1 && e < 2 * cnt_E(t.n, j - 1); --j) e >>= 1;
+            bnd = j == 0 && t.he[(int64_t)CH_WORDS * t.e2h[e] + CH_TWIN] < 0;
+            valence = bnd ? 2 : 4;
+            return;
+        }
+        if (v >= Vc) { valence = 4; bnd = false; return; }
+    }
+    const CageCounts& n = t.n;
+    if (v >= n.V + n.F) {                            // midpoint of a cage edge
+        bnd = t.he[(int64_t)CH_WORDS * t.e2h[v - n.V - n.F] + CH_TWIN] < 0;
+        valence = bnd ? 2 : 4;
+        return;
+    }
+    if (v >= n.V) { valence = t.fsz[v - n.V]; bnd = false; return; }
+    // a cage vertex: its ring in the cage (twin(prev h) forward, next(twin h) back)
+    const int32_t h0 = t.v2h[v];
+    int32_t cntv = 1, x = h0, guard = 0;
+    auto tw = [&](int32_t h) { return t.he[(int64_t)CH_WORDS * h + CH_TWIN]; };
+    for (x = tw(t.he[(int64_t)CH_WORDS * h0 + CH_PREV]); x >= 0 && x != h0 && guard < kWalkCap;
+         x = tw(t.he[(int64_t)CH_WORDS * x + CH_PREV]), ++guard)
+        ++cntv;
+    if (x < 0) {
+        guard = 0;
+        for (int32_t y = tw(h0); y >= 0 && guard < kWalkCap; ++guard) {
+            y = t.he[(int64_t)CH_WORDS * y + CH_NEXT];
+            ++cntv;
+            y = tw(y);
+        }
+    }
+    valence = cntv;
+    bnd = x < 0;
+}
+
+// item = older vertex v: {valence, 0, 0, boundary}; the crease pass adds the
+// summed sharpness and crease count
+__device__ __forceinline__ void shape_stats_item(const CageTables& t, int32_t d, float4* __restrict__ out,
+                                                 int32_t v) {
+    int32_t valence;
+    bool bnd;
+    old_vertex_shape(t, v, d, valence, bnd);
+    out[v] = make_float4((float)valence, 0.0f, 0.0f, bnd ? 1.0f : 0.0f);
+}
+
+// item = crease (edge) c < C of quad level d with nonzero sharpness: one end
+// of c is an older vertex (an end of the parent edge), the other the parent
+// edge's midpoint; the older end's statistics take its sharpness and sign.
+template <int RW>
+__device__ __forceinline__ void crease_stats_item(const QuadView<RW>& L, int32_t Vold, float4* __restrict__ out,
+                                                  int32_t c) {
+    const float s = L.cr[c].sharpness;
+    if (s == 0.0f) return;
+    const int32_t h = edge_to_he(L.t, c, L.d);
+    const int32_t v0 = L.vert(h), v1 = L.vert(qnext(h));
+    float* o = reinterpret_cast<float*>(out + (v0 < Vold ? v0 : v1));
+    atomicAdd(o + 1, s);
+    atomicAdd(o + 2, fsign(s));
+}
+
 struct VCoef {
     float a, bF, cE, dE;
 };
