@@ -9,10 +9,20 @@
 //   E[e(h)]   += al P[v(h)] + be P[v(next h)] + ga F[f(h)]
 //   Vn[v(h)]  += a P[v(h)] + bF F[f(h)] + cE E[e(h)] + dE E[e(prev h)]
 //
-// (coefficients below).  Given g = dL/d(points of depth d+1) this file
-// computes dL/d(points of depth d) += S_d^T g as three gathers, so that
-// every output slot is written by exactly one thread and the result does not
-// depend on scheduling:
+// (coefficients in ccs_tiles.cuh).  Given g = dL/d(points of depth d+1) this
+// file computes dL/d(points of depth d) += S_d^T g.
+//
+// Quad levels (d >= 1, cages with the twin relation): two halfedge-parallel
+// passes with the forward's lane layout (ccs_tiles.cuh adj_quad_*):
+//   1. gE[e] += the cE / dE terms, completed by the pair's larger halfedge
+//      (its own side from the quad's lanes, the twin side's coefficients
+//      recomputed; the twin side's vertices are this side's);
+//   2. per halfedge: the face term gF + sum of bF gV + ga gE over the quad
+//      (lane reduction), then the halfedge's term of its vertex
+//      a gV + al gE + gF/4 + be(prev) gE(prev), summed into the vertex (a face
+//      centre in the warp, the others by float atomics).
+// The cage level (and cages without the twin relation) runs three gathers,
+// every output slot written by one thread:
 //
 //   1. edge gather    (one thread per edge, run by the pair's larger
 //      halfedge):  gE[e] += sum of cE / dE terms of the halfedges whose
@@ -25,8 +35,8 @@
 //
 // The coefficients of a halfedge need its vertex's ring statistics.  On quad
 // levels these are known from the structure for face centres and edge
-// midpoints; for the older vertices the gathers read the per-level table the
-// topology refinement keeps (k_ring_stats, one ring walk per vertex).
+// midpoints; for the older vertices the passes read the per-level table the
+// topology refinement keeps (ccs_level.cu k_shape_stats / k_crease_stats).
 //
 // Levels run deepest first; only the level offsets are needed (no state is
 // saved by the forward pass).
@@ -59,7 +69,31 @@ k_adj_vertices(View L, const float* __restrict__ gNew, float* __restrict__ gOld)
     if (i < L.V) adj_vertex_item(L, gNew, gOld, (int32_t)i);
 }
 
+// quad levels: two halfedge-parallel passes (ccs_tiles.cuh)
+template <int RW>
+__global__ void __launch_bounds__(kBlockA)
+k_adj_quad_edges(QuadView<RW> L, float* __restrict__ gNew) {
+    adj_quad_edge_tile<RW>(L, gNew, (int64_t)blockIdx.x * kBlockA);
+}
+
+template <int RW, bool STRUCT>
+__global__ void __launch_bounds__(kBlockA)
+k_adj_quad_points(QuadView<RW> L, const float* __restrict__ gNew, float* __restrict__ gOld) {
+    adj_quad_point_tile<RW, STRUCT>(L, gNew, gOld, (int64_t)blockIdx.x * kBlockA);
+}
+
 static CageTables cage_tables_a(const DevCage& c) { return make_cage_tables(c); }
+
+template <int RW>
+static void adjoint_quad_level(const Ctx& c, const QuadView<RW>& L, float* gNew, float* gOld) {
+    c.prof->begin(c.stream, CCS_K_ADJ_EDGES, L.d, L.H);
+    k_adj_quad_edges<RW><<<nblocksA(L.H), kBlockA, 0, c.stream>>>(L, gNew);
+    c.prof->end(c.stream);
+    c.prof->begin(c.stream, CCS_K_ADJ_VERTICES, L.d, L.H);
+    if (L.d >= 2) k_adj_quad_points<RW, true><<<nblocksA(L.H), kBlockA, 0, c.stream>>>(L, gNew, gOld);
+    else k_adj_quad_points<RW, false><<<nblocksA(L.H), kBlockA, 0, c.stream>>>(L, gNew, gOld);
+    c.prof->end(c.stream);
+}
 
 template <class View>
 static void adjoint_level(const Ctx& c, const View& L, float* gNew, float* gOld) {
@@ -99,7 +133,8 @@ cudaError_t run_adjoint(const Ctx& c, const float* gradPts, float* work, float* 
                 L.cr = c.cr + lv.crOff;
                 L.V = lv.V; L.F = lv.F; L.E = lv.E; L.H = lv.H; L.C = lv.C; L.d = d;
                 L.ostats = stats_at(c, d);
-                adjoint_level(c, L, gNew, gOld);
+                if (c.fusable) adjoint_quad_level(c, L, gNew, gOld);
+                else adjoint_level(c, L, gNew, gOld);
             } else {
                 QuadView<3> L;
                 L.t = cage_tables_a(*c.cage);
@@ -107,7 +142,8 @@ cudaError_t run_adjoint(const Ctx& c, const float* gradPts, float* work, float* 
                 L.cr = c.cr + lv.crOff;
                 L.V = lv.V; L.F = lv.F; L.E = lv.E; L.H = lv.H; L.C = lv.C; L.d = d;
                 L.ostats = stats_at(c, d);
-                adjoint_level(c, L, gNew, gOld);
+                if (c.fusable) adjoint_quad_level(c, L, gNew, gOld);
+                else adjoint_level(c, L, gNew, gOld);
             }
         }
     }

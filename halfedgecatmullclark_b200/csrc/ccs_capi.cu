@@ -185,6 +185,7 @@ struct SubdImpl {
         c.stream = s; c.prof = &prof; c.err = err;
         c.side = side; c.forkEv = forkEv; c.joinEv = joinEv;
         c.stats = stats; c.statsOff = statsOff.data();
+        c.fusable = fusable;
         return c;
     }
 };

@@ -67,6 +67,7 @@ struct Ctx {
     // stats + statsOff[d], V(d-1) entries; null = not kept
     float4* stats = nullptr;
     const int64_t* statsOff = nullptr;
+    bool fusable = true;         // the twin relation vertex(twin h) = vertex(next h) holds
 };
 
 inline float4* stats_at(const Ctx& c, int d) {

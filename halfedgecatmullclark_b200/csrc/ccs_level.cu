@@ -20,7 +20,8 @@
 //   Vertex pass, default (k_level_b, one thread per halfedge): the vertex
 //      share of its halfedge with ring statistics from the refined structure
 //      (face centres, edge midpoints) or from the per-level table of the
-//      older vertices' statistics (k_ring_stats, built with the topology);
+//      older vertices' statistics (k_shape_stats + k_crease_stats, built
+//      with the topology);
 //      a face centre's shares are summed in the warp and stored, the other
 //      shares go out as float atomics (pairs combined in the warp first).
 //   Vertex pass, deterministic (CCS_FLAG_DETERMINISTIC): every vertex summed

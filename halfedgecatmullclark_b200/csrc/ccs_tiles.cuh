@@ -1121,5 +1121,101 @@ __device__ __forceinline__ void adj_vertex_item(const View& L, const float* __re
     o[2] += acc.z;
 }
 
+// ---------------------------------------------------------------------------
+// adjoint of a quad level (d >= 1) in two halfedge-parallel passes with the
+// forward's lane structure (a face's 4 halfedges in 4 adjacent lanes); needs
+// the twin relation vertex(twin h) = vertex(next h).
+// ---------------------------------------------------------------------------
+// Pass 1, tile of halfedges [h0, h0 + blockDim): the pair's larger halfedge
+// completes gE[e] += cE(h) gV[v(h)] + dE(next h) gV[v(next h)] + the same two
+// terms of the twin side, whose vertices are v(next h) and v(h).
+template <int RW>
+__device__ __forceinline__ void adj_quad_edge_tile(const QuadView<RW>& L, float* __restrict__ gNew, int64_t h0) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31, k = lane & 3, qb = lane & ~3, ln = qb | ((k + 1) & 3);
+    const int64_t h64 = h0 + threadIdx.x;
+    const bool valid = h64 < L.H;
+    const int32_t h = (int32_t)h64;
+    const float* gV = gNew;
+    float* gE = gNew + 3 * ((int64_t)L.V + L.F);
+    int32_t tw = -1, ed = 0, vx = 0;
+    VCoef kc{0.0f, 0.0f, 0.0f, 0.0f};
+    f3 g = zero3();
+    if (valid) {
+        tw = L.twin(h); ed = L.edge(h); vx = L.vert(h);
+        kc = vertex_coef(L, h);
+        g = ld3(gV + 3 * (int64_t)vx);
+    }
+    const float dEn = __shfl_sync(full, kc.dE, ln);
+    const f3 gn = shfl3(g, ln);
+    if (!valid || !(h > tw)) return;
+    f3 acc = add3(mul3(g, kc.cE), mul3(gn, dEn));
+    if (tw >= 0) {
+        const VCoef kt = vertex_coef(L, tw), ktn = vertex_coef(L, qnext(tw));
+        acc = add3(acc, add3(mul3(gn, kt.cE), mul3(g, ktn.dE)));
+    }
+    float* o = gE + 3 * (int64_t)ed;
+    o[0] += acc.x;
+    o[1] += acc.y;
+    o[2] += acc.z;
+}
+
+// Pass 2, tile of halfedges: the face's gradient gF[f] + sum over its
+// halfedges of bF gV[v] + ga gE[e] (reduced over the quad's lanes), then
+// each halfedge's term of its vertex a gV[v] + al gE[e] + gF/4 + be(prev h)
+// gE[e(prev h)], summed into gOld[v]: STRUCT (depth >= 2) a face centre's
+// four terms in the warp (one writer), an edge midpoint's two per side and
+// an older vertex's one by float atomics; depth 1 all by atomics.
+template <int RW, bool STRUCT>
+__device__ __forceinline__ void adj_quad_point_tile(const QuadView<RW>& L, const float* __restrict__ gNew,
+                                                    float* __restrict__ gOld, int64_t h0) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31, k = lane & 3, qb = lane & ~3, lp = qb | ((k + 3) & 3);
+    const int64_t h64 = h0 + threadIdx.x;
+    const bool valid = h64 < L.H;
+    const int32_t h = (int32_t)h64;
+    const float* gV = gNew;
+    const float* gF = gNew + 3 * (int64_t)L.V;
+    const float* gE = gNew + 3 * ((int64_t)L.V + L.F);
+    int32_t vx = 0;
+    VCoef kc{0.0f, 0.0f, 0.0f, 0.0f};
+    ECoef ke{0.0f, 0.0f, 0.0f};
+    f3 gv = zero3(), ge = zero3(), gf = zero3();
+    if (valid) {
+        const int32_t ed = L.edge(h);
+        vx = L.vert(h);
+        kc = vertex_coef(L, h);
+        ke = edge_coef(L, h);
+        gv = ld3(gV + 3 * (int64_t)vx);
+        ge = ld3(gE + 3 * (int64_t)ed);
+        if (k == 0) gf = ld3(gF + 3 * (int64_t)(h >> 2));
+    }
+    f3 ft = add3(mul3(gv, kc.bF), mul3(ge, ke.ga));
+    ft = add3(ft, shfl_xor3(ft, 1));
+    ft = add3(ft, shfl_xor3(ft, 2));
+    const f3 gFt = add3(shfl3(gf, qb), ft);
+    const float bep = __shfl_sync(full, ke.be, lp);
+    const f3 gep = shfl3(ge, lp);
+    f3 s = add3(add3(mul3(gv, kc.a), mul3(ge, ke.al)), add3(mul3(gFt, 0.25f), mul3(gep, bep)));
+    float* o = gOld + 3 * (int64_t)vx;
+    if (STRUCT) {
+        const f3 s4 = shfl_down3(s, 4), s8 = shfl_down3(s, 8), s12 = shfl_down3(s, 12);
+        const int partner = (lane & ~15) | ((((lane >> 2) + 1) & 3) << 2) | 3;
+        const f3 sA2 = shfl3(s, partner);
+        if (!valid) return;
+        if ((lane & 15) == 2) {
+            const f3 t = add3(add3(s, s4), add3(s8, s12));
+            o[0] += t.x;
+            o[1] += t.y;
+            o[2] += t.z;
+        } else if (k == 1) {
+            atomic_add3(o, add3(s, sA2));
+        } else if (k == 0) {
+            atomic_add3(o, s);
+        }
+    } else if (valid) {
+        atomic_add3(o, s);
+    }
+}
 
 }  // namespace ccs
