@@ -9,12 +9,20 @@
 // stride over the tiles of one phase, meet at a grid barrier, and go on
 // with the next phase:
 //
-//   forward, d = 0:  cage topology + creases + face points | edge points
-//                    | vertex points (one thread per vertex, sorted ring)
-//   forward, d = 1:  kernel A tiles + crease tiles | vertex points (sorted ring)
-//   forward, d >= 2: kernel A tiles + crease tiles | older vertices + kernel B tiles
-//   (every vertex point summed in the reference's one-thread order: no atomics)
-//   adjoint, each d: edge gathers | face gathers | vertex gathers
+//   forward, d = 0:  cage topology + creases + face points (+ clearing)
+//                    | edge points | vertex points (+ shape statistics of level 1)
+//   forward, d >= 1: kernel A tiles + crease tiles (+ creased-edge statistics
+//                    of level d) | vertex pass tiles (+ shape statistics of
+//                    level d + 1)
+//   adjoint, d = 0:  edge gathers | face gathers | vertex gathers
+//   adjoint, d >= 1: edge pass | face + vertex pass
+//
+// The default vertex pass sums with float atomics (the single-mesh default);
+// CCS_FLAG_DETERMINISTIC selects the exact pass (older vertices one thread
+// each, face centres and edge midpoints in the warp; one thread per vertex
+// with a sorted ring at d <= 1), bit-identical to the reference.  The older
+// vertices' ring statistics are built while the topology is refined and kept
+// per level for the points-only forward and the adjoint.
 //
 // The tile bodies are the single-mesh ones (ccs_tiles.cuh).  The kernels run
 // as cooperative launches (all blocks resident), and every barrier wait is
@@ -40,16 +48,18 @@ enum Phase {
     PH_CAGE_TOPO = 0,   // 4 H0 child halfedges
     PH_CAGE_CREASE,     // E0 creases
     PH_CAGE_FACE,       // F0 faces
+    PH_CAGE_ZERO,       // V0 vertex slots of depth 1 (atomic pass)
     PH_CAGE_EDGE,       // H0 halfedges
-    PH_CAGE_VERT,       // V0 vertices
+    PH_CAGE_VERT,       // V0 vertices (sorted ring) or H0 halfedges (atomics): max of both
     PH_A,               // H_d parent halfedges
     PH_A_CREASE,        // C_d creases
-    PH_V,               // d >= 2: V_(d-1) older vertices
-    PH_B,               // d = 1: V_1 vertices; d >= 2: H_d halfedges
-    PH_ADJ_STATS,       // d >= 1: V_(d-1) older vertices (ring statistics)
+    PH_CREASE_STATS,    // C_d creases of depth d (statistics of the older vertices)
+    PH_SHAPE_NEXT,      // V_d vertices: shape statistics of depth d + 1
+    PH_V,               // d >= 2: V_(d-1) older vertices (exact pass)
+    PH_B,               // H_d halfedges; exact pass at d = 1: V_1 vertices
     PH_ADJ_EDGE,        // H_d
-    PH_ADJ_FACE,        // F_d
-    PH_ADJ_VERT,        // V_d
+    PH_ADJ_FACE,        // F_d (cage)
+    PH_ADJ_VERT,        // V_0 (cage) or H_d
     PH_COUNT
 };
 
@@ -59,7 +69,7 @@ struct BatchCage {
     int32_t uv;          // UV codes are refined
     int64_t cagePt;      // first cage point of this cage in the batch's cage-point buffer
     int64_t he, cr, pt;  // first record / crease / point of this cage's hierarchy
-    int64_t stats;       // first ring-statistics entry of this cage (adjoint)
+    int64_t stats[kMaxBatchDepth + 1];  // level d's ring statistics (V(d-1) entries), 1 <= d < depth
     Level lv[kMaxBatchDepth + 1];
 };
 
@@ -79,7 +89,7 @@ struct BatchArgs {
     float* pts;
     float* work;                         // adjoint: running gradient per refined point
     float* gradCage;                     // adjoint output
-    float4* stats;                       // adjoint: ring statistics of the older vertices
+    float4* stats;                       // ring statistics of the older vertices, every level
     GridSync* sync;
     unsigned int spinCap;                // polls before a barrier wait gives up
 };
@@ -162,11 +172,26 @@ __device__ __forceinline__ void for_tiles(const BatchArgs& a, int d, int phase, 
     }
 }
 
-template <bool TOPO, bool CREASED>
+__device__ __forceinline__ QuadView<4> batch_quad_view_stats(const BatchArgs& a, const BatchCage& bc, int d) {
+    QuadView<4> L = batch_quad_view(a, bc, d);
+    L.ostats = a.stats + bc.stats[d];
+    return L;
+}
+
+template <bool TOPO, bool CREASED, bool DET>
 __global__ void __launch_bounds__(kBatchBlock)
 k_batch_forward(BatchArgs a, int d) {
     __shared__ __align__(128) int32_t tile[kBatchBlock * 4 * 4];
     const int tid = threadIdx.x;
+    // shape statistics of depth d + 1 (valence, boundary; cage tables only)
+    auto shape_next = [&]() {
+        if (!TOPO) return;
+        for_tiles(a, d, PH_SHAPE_NEXT, [&](const BatchCage& bc, int64_t lt) {
+            const int64_t v = lt * kBatchBlock + tid;
+            if (d + 1 < bc.depth && v < bc.lv[d].V)
+                shape_stats_item(make_cage_tables(bc.cage), d + 1, a.stats + bc.stats[d + 1], (int32_t)v);
+        });
+    };
     if (d == 0) {
         if (TOPO) {
             for_tiles(a, 0, PH_CAGE_TOPO, [&](const BatchCage& bc, int64_t lt) {
@@ -187,6 +212,12 @@ k_batch_forward(BatchArgs a, int d) {
             face_point_item<CageView, false>(batch_cage_view(bc), a.cagePts + 3 * bc.cagePt,
                                              a.pts + 3 * (bc.pt + bc.lv[1].ptOff), (int32_t)i);
         });
+        if (!DET) {
+            for_tiles(a, 0, PH_CAGE_ZERO, [&](const BatchCage& bc, int64_t lt) {
+                const int64_t i = lt * kBatchBlock + tid;
+                if (i < bc.cage.V) st3(a.pts + 3 * (bc.pt + bc.lv[1].ptOff + i), zero3());
+            });
+        }
         if (!grid_sync(a.sync, a.spinCap, gridDim.x)) return;
         for_tiles(a, 0, PH_CAGE_EDGE, [&](const BatchCage& bc, int64_t lt) {
             const int64_t i = lt * kBatchBlock + tid;
@@ -197,10 +228,16 @@ k_batch_forward(BatchArgs a, int d) {
         if (!grid_sync(a.sync, a.spinCap, gridDim.x)) return;
         for_tiles(a, 0, PH_CAGE_VERT, [&](const BatchCage& bc, int64_t lt) {
             const int64_t i = lt * kBatchBlock + tid;
-            if (i < bc.cage.V)
-                vertex_det_item<CageView, CREASED>(batch_cage_view(bc), a.cagePts + 3 * bc.cagePt,
-                                                   a.pts + 3 * (bc.pt + bc.lv[1].ptOff), (int32_t)i);
+            const float* cp = a.cagePts + 3 * bc.cagePt;
+            float* pout = a.pts + 3 * (bc.pt + bc.lv[1].ptOff);
+            if (DET) {
+                if (i < bc.cage.V) vertex_det_item<CageView, CREASED>(batch_cage_view(bc), cp, pout, (int32_t)i);
+            } else {
+                // warp-collective: every lane of the tile takes part
+                vertex_atomic_item<CageView, CREASED>(batch_cage_view(bc), cp, pout, (int32_t)i, i < bc.cage.H);
+            }
         });
+        shape_next();
         return;
     }
     for_tiles(a, d, PH_A, [&](const BatchCage& bc, int64_t lt) {
@@ -213,7 +250,7 @@ k_batch_forward(BatchArgs a, int d) {
         la.pin = a.pts + 3 * (bc.pt + lv.ptOff);
         la.pout = a.pts + 3 * (bc.pt + bc.lv[d + 1].ptOff);
         la.H = lv.H; la.V = lv.V; la.F = lv.F; la.E = lv.E; la.C = lv.C;
-        la.zeroV = 0;                    // the batched vertex pass stores every slot
+        la.zeroV = DET ? 0 : 1;          // the atomic pass accumulates into cleared slots
         if (bc.uv) tile_level_a<kBatchBlock, 4, TOPO, true, true, CREASED>(la, lt * kBatchBlock, tile);
         else tile_level_a<kBatchBlock, 4, TOPO, false, true, CREASED>(la, lt * kBatchBlock, tile);
         __syncthreads();   // the tile's shared memory is reused by the next tile
@@ -224,9 +261,16 @@ k_batch_forward(BatchArgs a, int d) {
             if (i < bc.lv[d].C)
                 crease_item(a.cr + bc.cr + bc.lv[d].crOff, a.cr + bc.cr + bc.lv[d + 1].crOff, (int32_t)i);
         });
+        // creased edges of depth d into the older vertices' statistics (their
+        // shape entries were written by the previous depth's launch)
+        for_tiles(a, d, PH_CREASE_STATS, [&](const BatchCage& bc, int64_t lt) {
+            const int64_t i = lt * kBatchBlock + tid;
+            if (i < bc.lv[d].C)
+                crease_stats_item(batch_quad_view(a, bc, d), bc.lv[d - 1].V, a.stats + bc.stats[d], (int32_t)i);
+        });
     }
     if (!grid_sync(a.sync, a.spinCap, gridDim.x)) return;
-    if (d >= 2) {
+    if (DET && d >= 2) {
         for_tiles(a, d, PH_V, [&](const BatchCage& bc, int64_t lt) {
             const int64_t v = lt * kBatchBlock + tid;
             if (v < bc.lv[d - 1].V)
@@ -235,53 +279,52 @@ k_batch_forward(BatchArgs a, int d) {
         });
     }
     for_tiles(a, d, PH_B, [&](const BatchCage& bc, int64_t lt) {
-        const QuadView<4> L = batch_quad_view(a, bc, d);
         const float* pin = a.pts + 3 * (bc.pt + bc.lv[d].ptOff);
         float* pout = a.pts + 3 * (bc.pt + bc.lv[d + 1].ptOff);
-        if (d >= 2) {
-            tile_level_b_exact<4, CREASED>(L, pin, pout, lt * kBatchBlock);
+        if (!DET) {
+            const QuadView<4> L = batch_quad_view_stats(a, bc, d);
+            if (d >= 2) tile_level_b<4, CREASED, true>(L, pin, pout, lt * kBatchBlock);
+            else tile_level_b<4, CREASED, false>(L, pin, pout, lt * kBatchBlock);
+        } else if (d >= 2) {
+            tile_level_b_exact<4, CREASED>(batch_quad_view(a, bc, d), pin, pout, lt * kBatchBlock);
         } else {
+            const QuadView<4> L = batch_quad_view(a, bc, d);
             const int64_t v = lt * kBatchBlock + tid;
             if (v < L.V) vertex_det_item<QuadView<4>, CREASED>(L, pin, pout, (int32_t)v);
         }
     });
+    shape_next();
 }
 
 __global__ void __launch_bounds__(kBatchBlock)
 k_batch_adjoint(BatchArgs a, int d) {
     const int tid = threadIdx.x;
     auto gnew = [&](const BatchCage& bc) { return a.work + 3 * (bc.pt + bc.lv[d + 1].ptOff); };
-    auto qview = [&](const BatchCage& bc) {
-        QuadView<4> L = batch_quad_view(a, bc, d);
-        L.ostats = a.stats + bc.stats;
-        return L;
-    };
-    if (d >= 1) {
-        for_tiles(a, d, PH_ADJ_STATS, [&](const BatchCage& bc, int64_t lt) {
+    if (d == 0) {
+        for_tiles(a, 0, PH_ADJ_EDGE, [&](const BatchCage& bc, int64_t lt) {
             const int64_t i = lt * kBatchBlock + tid;
-            if (i < bc.lv[d - 1].V) ring_stats_item(batch_quad_view(a, bc, d), a.stats + bc.stats, (int32_t)i);
+            if (i < bc.cage.H) adj_edge_item(batch_cage_view(bc), gnew(bc), (int32_t)i);
         });
         if (!grid_sync(a.sync, a.spinCap, gridDim.x)) return;
+        for_tiles(a, 0, PH_ADJ_FACE, [&](const BatchCage& bc, int64_t lt) {
+            const int64_t i = lt * kBatchBlock + tid;
+            if (i < bc.cage.F) adj_face_item(batch_cage_view(bc), gnew(bc), (int32_t)i);
+        });
+        if (!grid_sync(a.sync, a.spinCap, gridDim.x)) return;
+        for_tiles(a, 0, PH_ADJ_VERT, [&](const BatchCage& bc, int64_t lt) {
+            const int64_t i = lt * kBatchBlock + tid;
+            if (i < bc.cage.V) adj_vertex_item(batch_cage_view(bc), gnew(bc), a.gradCage + 3 * bc.cagePt, (int32_t)i);
+        });
+        return;
     }
     for_tiles(a, d, PH_ADJ_EDGE, [&](const BatchCage& bc, int64_t lt) {
-        const int64_t i = lt * kBatchBlock + tid;
-        if (i >= bc.lv[d].H) return;
-        if (d == 0) adj_edge_item(batch_cage_view(bc), gnew(bc), (int32_t)i);
-        else adj_edge_item(qview(bc), gnew(bc), (int32_t)i);
-    });
-    if (!grid_sync(a.sync, a.spinCap, gridDim.x)) return;
-    for_tiles(a, d, PH_ADJ_FACE, [&](const BatchCage& bc, int64_t lt) {
-        const int64_t i = lt * kBatchBlock + tid;
-        if (i >= bc.lv[d].F) return;
-        if (d == 0) adj_face_item(batch_cage_view(bc), gnew(bc), (int32_t)i);
-        else adj_face_item(qview(bc), gnew(bc), (int32_t)i);
+        adj_quad_edge_tile<4>(batch_quad_view_stats(a, bc, d), gnew(bc), lt * kBatchBlock);
     });
     if (!grid_sync(a.sync, a.spinCap, gridDim.x)) return;
     for_tiles(a, d, PH_ADJ_VERT, [&](const BatchCage& bc, int64_t lt) {
-        const int64_t i = lt * kBatchBlock + tid;
-        if (i >= bc.lv[d].V) return;
-        if (d == 0) adj_vertex_item(batch_cage_view(bc), gnew(bc), a.gradCage + 3 * bc.cagePt, (int32_t)i);
-        else adj_vertex_item(qview(bc), gnew(bc), a.work + 3 * (bc.pt + bc.lv[d].ptOff), (int32_t)i);
+        float* gOld = a.work + 3 * (bc.pt + bc.lv[d].ptOff);
+        if (d >= 2) adj_quad_point_tile<4, true>(batch_quad_view_stats(a, bc, d), gnew(bc), gOld, lt * kBatchBlock);
+        else adj_quad_point_tile<4, false>(batch_quad_view_stats(a, bc, d), gnew(bc), gOld, lt * kBatchBlock);
     });
 }
 
@@ -341,16 +384,18 @@ static int64_t phase_units(const BatchCage& bc, int d, int ph) {
         case PH_CAGE_TOPO: return d == 0 ? 4 * (int64_t)lv.H : 0;
         case PH_CAGE_CREASE: return d == 0 ? lv.E : 0;
         case PH_CAGE_FACE: return d == 0 ? lv.F : 0;
+        case PH_CAGE_ZERO: return d == 0 ? lv.V : 0;
         case PH_CAGE_EDGE: return d == 0 ? lv.H : 0;
-        case PH_CAGE_VERT: return d == 0 ? lv.V : 0;
+        case PH_CAGE_VERT: return d == 0 ? (lv.H > lv.V ? lv.H : lv.V) : 0;
         case PH_A: return d >= 1 ? lv.H : 0;
         case PH_A_CREASE: return d >= 1 ? lv.C : 0;
+        case PH_CREASE_STATS: return d >= 1 ? lv.C : 0;
+        case PH_SHAPE_NEXT: return d + 1 < bc.depth ? lv.V : 0;
         case PH_V: return d >= 2 ? bc.lv[d - 1].V : 0;
-        case PH_B: return d == 1 ? lv.V : (d >= 2 ? lv.H : 0);
-        case PH_ADJ_STATS: return d >= 1 ? bc.lv[d - 1].V : 0;
+        case PH_B: return d == 1 ? (lv.H > lv.V ? lv.H : lv.V) : (d >= 2 ? lv.H : 0);
         case PH_ADJ_EDGE: return lv.H;
-        case PH_ADJ_FACE: return lv.F;
-        case PH_ADJ_VERT: return lv.V;
+        case PH_ADJ_FACE: return d == 0 ? lv.F : 0;
+        case PH_ADJ_VERT: return d == 0 ? lv.V : lv.H;
         default: return 0;
     }
 }
@@ -377,7 +422,7 @@ static int batch_create(const cc_Mesh* const* cages, const int32_t* depths, int3
                         ccs_Batch** out) {
     if (!out || !cages || !depths || count <= 0) return CCS_ERR_ARG;
     *out = nullptr;
-    if (flags & (CCS_FLAG_NO_UV | CCS_FLAG_DETERMINISTIC)) return CCS_ERR_UNSUPPORTED;
+    if (flags & CCS_FLAG_NO_UV) return CCS_ERR_UNSUPPORTED;
     ccs_Batch* b = new (std::nothrow) ccs_Batch();
     if (!b) return CCS_ERR_ALLOC;
     b->count = count;
@@ -408,8 +453,10 @@ static int batch_create(const cc_Mesh* const* cages, const int32_t* depths, int3
         bc.cage.fsz = (int32_t*)(intptr_t)oF;
         bc.cagePt = oV;
         bc.he = b->totH; bc.cr = b->totC; bc.pt = b->totV;
-        bc.stats = b->totStats;                  // entries: max over 1 <= d < D of V(d-1) = V(D-2)
-        b->totStats += D >= 2 ? lv[D - 2].V : 0;
+        for (int d = 1; d < D; ++d) {            // level d: V(d-1) older vertices
+            bc.stats[d] = b->totStats;
+            b->totStats += lv[d - 1].V;
+        }
         const Level& last = lv[D];
         b->totH += last.heOff + last.H;
         b->totC += last.crOff + last.C;
@@ -426,7 +473,7 @@ static int batch_create(const cc_Mesh* const* cages, const int32_t* depths, int3
     if (!bmalloc(&b->cHe, 7 * oHe) || !bmalloc(&b->cCr, oE) || !bmalloc(&b->cUv, 2 * oUv) ||
         !bmalloc(&b->cV2h, oV) || !bmalloc(&b->cE2h, oE) || !bmalloc(&b->cF2h, oF) || !bmalloc(&b->cFsz, oF) ||
         !bmalloc(&b->cagePts, 3 * oV) || !bmalloc(&b->he, 4 * b->totH) || !bmalloc(&b->cr, b->totC) ||
-        !bmalloc(&b->pts, 3 * b->totV) || !bmalloc(&b->sync, 1)) {
+        !bmalloc(&b->pts, 3 * b->totV) || !bmalloc(&b->sync, 1) || !bmalloc(&b->stats, b->totStats)) {
         free_batch(b);
         return CCS_ERR_ALLOC;
     }
@@ -475,13 +522,12 @@ static int batch_create(const cc_Mesh* const* cages, const int32_t* depths, int3
     return CCS_OK;
 }
 
-// gradient of every refined point, of the cage points, and the ring statistics
+// gradient of every refined point and of the cage points
 static bool adjoint_buffers(ccs_Batch* b) {
     if (b->work) return true;
-    if (bmalloc(&b->work, 3 * b->totV) && bmalloc(&b->gradCage, 3 * b->totCagePts) && bmalloc(&b->stats, b->totStats))
-        return true;
-    cudaFree(b->work); cudaFree(b->gradCage); cudaFree(b->stats);
-    b->work = nullptr; b->gradCage = nullptr; b->stats = nullptr;
+    if (bmalloc(&b->work, 3 * b->totV) && bmalloc(&b->gradCage, 3 * b->totCagePts)) return true;
+    cudaFree(b->work); cudaFree(b->gradCage);
+    b->work = nullptr; b->gradCage = nullptr;
     return false;
 }
 
@@ -531,20 +577,28 @@ static cudaError_t enqueue_batch(ccs_Batch* b, int op, bool creased) {
     if (op == BOP_ADJOINT) {
         e = cudaMemsetAsync(b->gradCage, 0, sizeof(float) * 3 * (size_t)b->totCagePts, b->stream);
         for (int d = b->maxDepth - 1; d >= 0 && e == cudaSuccess; --d) {
-            const int64_t mt = max_tiles(b, d, {PH_ADJ_STATS, PH_ADJ_EDGE, PH_ADJ_FACE, PH_ADJ_VERT});
+            const int64_t mt = max_tiles(b, d, {PH_ADJ_EDGE, PH_ADJ_FACE, PH_ADJ_VERT});
             e = launch_coop(b, k_batch_adjoint, mt, a, d);
         }
         return e;
     }
     const bool topo = op == BOP_REFINE;
+    const bool det = (b->flags & CCS_FLAG_DETERMINISTIC) != 0;
     for (int d = 0; d < b->maxDepth && e == cudaSuccess; ++d) {
-        const int64_t mt = d == 0 ? max_tiles(b, 0, {PH_CAGE_TOPO, PH_CAGE_CREASE, PH_CAGE_FACE, PH_CAGE_EDGE,
-                                                      PH_CAGE_VERT})
-                                  : max_tiles(b, d, {PH_A, PH_A_CREASE, PH_V, PH_B});
-        if (topo) e = creased ? launch_coop(b, k_batch_forward<true, true>, mt, a, d)
-                              : launch_coop(b, k_batch_forward<true, false>, mt, a, d);
-        else e = creased ? launch_coop(b, k_batch_forward<false, true>, mt, a, d)
-                         : launch_coop(b, k_batch_forward<false, false>, mt, a, d);
+        const int64_t mt = d == 0 ? max_tiles(b, 0, {PH_CAGE_TOPO, PH_CAGE_CREASE, PH_CAGE_FACE, PH_CAGE_ZERO,
+                                                      PH_CAGE_EDGE, PH_CAGE_VERT, PH_SHAPE_NEXT})
+                                  : max_tiles(b, d, {PH_A, PH_A_CREASE, PH_CREASE_STATS, PH_V, PH_B, PH_SHAPE_NEXT});
+        const int v = (topo ? 4 : 0) + (creased ? 2 : 0) + (det ? 1 : 0);
+        switch (v) {
+            case 0: e = launch_coop(b, k_batch_forward<false, false, false>, mt, a, d); break;
+            case 1: e = launch_coop(b, k_batch_forward<false, false, true>, mt, a, d); break;
+            case 2: e = launch_coop(b, k_batch_forward<false, true, false>, mt, a, d); break;
+            case 3: e = launch_coop(b, k_batch_forward<false, true, true>, mt, a, d); break;
+            case 4: e = launch_coop(b, k_batch_forward<true, false, false>, mt, a, d); break;
+            case 5: e = launch_coop(b, k_batch_forward<true, false, true>, mt, a, d); break;
+            case 6: e = launch_coop(b, k_batch_forward<true, true, false>, mt, a, d); break;
+            default: e = launch_coop(b, k_batch_forward<true, true, true>, mt, a, d); break;
+        }
     }
     return e;
 }
