@@ -59,10 +59,17 @@ __device__ __forceinline__ f3 shfl_xor3(f3 v, int m) {
     return f3{__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m),
               __shfl_xor_sync(0xffffffffu, v.z, m)};
 }
+// A 12-byte point as one 8-byte vector atomic (the aligned pair) and one
+// scalar atomic: two reductions instead of three (vector float atomics are
+// native from sm_90 on).
 __device__ __forceinline__ void atomic_add3(float* o, f3 v) {
-    atomicAdd(o + 0, v.x);
-    atomicAdd(o + 1, v.y);
-    atomicAdd(o + 2, v.z);
+    if ((reinterpret_cast<uintptr_t>(o) & 7u) == 0) {
+        atomicAdd(reinterpret_cast<float2*>(o), make_float2(v.x, v.y));
+        atomicAdd(o + 2, v.z);
+    } else {
+        atomicAdd(o, v.x);
+        atomicAdd(reinterpret_cast<float2*>(o + 1), make_float2(v.y, v.z));
+    }
 }
 
 // Face point of the quad held by lanes qb..qb+3, in halfedge order:
