@@ -428,6 +428,16 @@ def run_batch_workload(args):
         b.record(stream)
     bt.synchronize()
     batch_ms = shard.max_over_ranks(a.elapsed_time(b) / steps, world)
+    # the two halves alone (same stream, CUDA events)
+    parts = {}
+    for name, fn in (("forward_ms", bt.refine_points), ("adjoint_ms", bt.adjoint)):
+        with torch.cuda.stream(stream):
+            a.record(stream)
+            for _ in range(steps):
+                fn()
+            b.record(stream)
+        bt.synchronize()
+        parts[name] = shard.max_over_ranks(a.elapsed_time(b) / steps, world)
     agree = max(float((arr["grad_cage_points"][bt.cage_slice(i)] - ref).abs().max() /
                       max(ref.abs().max(), 1e-30))
                 for i, ref in zip((0, len(ws) // 2, len(ws) - 1), loop_sample))
@@ -451,6 +461,7 @@ def run_batch_workload(args):
             "loop": {"value": len(ws_all) / (loop_ms / 1e3), "unit": "cages/s", "ms_per_step": loop_ms,
                      "how": "Python loop of ccs_RefinePointsDevice_cuda + ccs_AdjointPointsDevice_cuda per cage"},
             "speedup_vs_loop": loop_ms / batch_ms, "topology_refine_ms": topo_ms,
+            "forward_ms": parts["forward_ms"], "adjoint_ms": parts["adjoint_ms"],
             "grad_agreement_rel": agree}
     print(json.dumps(line))
     return 0

@@ -36,18 +36,12 @@ __device__ __forceinline__ int32_t uv_enc_fast(float u, float v) {
 }
 
 // One thread writes `bytes` of shared memory to global memory through the
-// TMA engine (no multicast); with WAIT it then waits until the shared source
-// has been read, else the caller waits (bulk_store_wait) before it reuses or
-// releases the shared memory.
-template <bool WAIT = true>
+// TMA engine (no multicast) and waits until the shared source has been read.
 __device__ __forceinline__ void bulk_store_tile(void* gdst, const void* ssrc, uint32_t bytes) {
     const uint32_t s = (uint32_t)__cvta_generic_to_shared(ssrc);
     asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;"
                  :: "l"(gdst), "r"(s), "r"(bytes) : "memory");
     asm volatile("cp.async.bulk.commit_group;" ::: "memory");
-    if (WAIT) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
-}
-__device__ __forceinline__ void bulk_store_wait() {
     asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
 }
 
@@ -151,11 +145,11 @@ __device__ __forceinline__ ARec load_arec(const int32_t* __restrict__ in, int64_
 }
 
 // `tile` is BLOCK * 4 * RW ints of shared memory; every thread of the block
-// must call this with the same h0, and `rec` = its parent record.  PERSIST:
-// the block runs many tiles through one shared tile, so the previous tile's
-// bulk store must have read it before it is rewritten, and this tile's store
-// is left in flight (the kernel waits for it before the block exits).
-template <int BLOCK, int RW, bool TOPO, bool UV, bool PTS, bool CREASED, bool PERSIST = false>
+// must call this with the same h0, and `rec` = its parent record.  The child
+// records go out through the shared tile and one bulk store per block, or
+// with DIRECT as each thread's own 16-byte vector stores (its 4 children are
+// 64 (48) contiguous bytes; a warp's stores cover 2 KB without gaps).
+template <int BLOCK, int RW, bool TOPO, bool UV, bool PTS, bool CREASED, bool DIRECT = false>
 __device__ __forceinline__ void tile_level_a_rec(const LevelArgs& a, int64_t h0, int32_t* tile, ARec rec) {
     const int tid = threadIdx.x, lane = tid & 31;
     const int64_t h64 = h0 + tid;
@@ -219,11 +213,19 @@ __device__ __forceinline__ void tile_level_a_rec(const LevelArgs& a, int64_t h0,
             st3(a.pout + 3 * ((int64_t)a.V + a.F + ed), E);
         }
     }
-    if (TOPO) {
-        if (PERSIST) {
-            if (tid == 0) bulk_store_wait();            // the previous tile's store has read the tile
-            __syncthreads();
+    if (TOPO && DIRECT) {
+        if (valid) {
+            int4* dst = reinterpret_cast<int4*>(a.out + (int64_t)4 * RW * h64);
+            if constexpr (RW == 4) {
+#pragma unroll
+                for (int m = 0; m < 4; ++m) dst[m] = make_int4(c_tw[m], c_ed[m], c_vx[m], UV ? uvc[m] : 0);
+            } else {
+                dst[0] = make_int4(c_tw[0], c_ed[0], c_vx[0], c_tw[1]);
+                dst[1] = make_int4(c_ed[1], c_vx[1], c_tw[2], c_ed[2]);
+                dst[2] = make_int4(c_vx[2], c_tw[3], c_ed[3], c_vx[3]);
+            }
         }
+    } else if (TOPO) {
         int32_t* t = tile + tid * 4 * RW;
         if constexpr (RW == 4) {
 #pragma unroll
@@ -237,14 +239,15 @@ __device__ __forceinline__ void tile_level_a_rec(const LevelArgs& a, int64_t h0,
         __syncthreads();
         if (tid == 0) {
             const int64_t n = (a.H - h0) < BLOCK ? (a.H - h0) : BLOCK;
-            bulk_store_tile<!PERSIST>(a.out + 4 * RW * h0, tile, (uint32_t)(n * 16 * RW));
+            bulk_store_tile(a.out + 4 * RW * h0, tile, (uint32_t)(n * 16 * RW));
         }
     }
 }
 
-template <int BLOCK, int RW, bool TOPO, bool UV, bool PTS, bool CREASED>
+template <int BLOCK, int RW, bool TOPO, bool UV, bool PTS, bool CREASED, bool DIRECT = false>
 __device__ __forceinline__ void tile_level_a(const LevelArgs& a, int64_t h0, int32_t* tile) {
-    tile_level_a_rec<BLOCK, RW, TOPO, UV, PTS, CREASED>(a, h0, tile, load_arec<RW>(a.in, h0 + threadIdx.x, a.H));
+    tile_level_a_rec<BLOCK, RW, TOPO, UV, PTS, CREASED, DIRECT>(a, h0, tile,
+                                                               load_arec<RW>(a.in, h0 + threadIdx.x, a.H));
 }
 
 // ---------------------------------------------------------------------------
