@@ -41,8 +41,6 @@
 // then preserved by every refinement step) and uses the unfused kernels for
 // cages that break it.
 #include <cstdint>
-#include <cstdlib>
-#include <cstring>
 
 #include "ccs_host.h"
 #include "ccs_tiles.cuh"
@@ -58,7 +56,7 @@ static inline unsigned nblocksL(int64_t n) { return (unsigned)((n + kBlockL - 1)
 // prefetched the next tile's records and left each bulk store in flight ran
 // 1.5x slower at depth 5: 5 resident blocks per SM instead of 8 hid less of
 // the gather latency than the extra overlap won.)
-template <int RW, bool TOPO, bool UV, bool CREASED, bool DIRECT>
+template <int RW, bool TOPO, bool UV, bool CREASED>
 __global__ void __launch_bounds__(kBlockL)
 k_level_a(LevelArgs a) {
     const int nbH = (a.H + kBlockL - 1) / kBlockL;
@@ -68,19 +66,8 @@ k_level_a(LevelArgs a) {
         if (i < a.C) crease_item(a.crIn, a.crOut, (int32_t)i);
         return;
     }
-    __shared__ __align__(128) int32_t tile[DIRECT ? 4 : kBlockL * 4 * RW];
-    tile_level_a<kBlockL, RW, TOPO, UV, true, CREASED, DIRECT>(a, (int64_t)blockIdx.x * kBlockL, tile);
-}
-
-// Child-record store path of kernel A: the shared tile and one bulk store
-// per block (default), or each thread's own vector stores when the
-// environment variable CCS_LEVEL_A_STORE is "direct" (read once).
-static bool level_a_direct() {
-    static const int v = [] {
-        const char* e = getenv("CCS_LEVEL_A_STORE");
-        return (e && strcmp(e, "direct") == 0) ? 1 : 0;
-    }();
-    return v != 0;
+    __shared__ __align__(128) int32_t tile[kBlockL * 4 * RW];
+    tile_level_a<kBlockL, RW, TOPO, UV, true, CREASED>(a, (int64_t)blockIdx.x * kBlockL, tile);
 }
 
 // default vertex pass: one tile of halfedges per block
@@ -192,14 +179,11 @@ static void level_a(const Ctx& c, int d, bool topo, bool uv, const float* pin, f
     a.zeroV = zeroV ? 1 : 0;
     const unsigned nb = nblocksL(lv.H) + (topo ? nblocksL(lv.C) : 0u);
     c.prof->begin(c.stream, topo ? CCS_K_LEVEL_FUSED : CCS_K_FACE_POINTS, d, lv.H);
-    if (topo && level_a_direct()) {
-        if (RW == 4 && uv) k_level_a<RW, true, true, CREASED, true><<<nb, kBlockL, 0, c.stream>>>(a);
-        else k_level_a<RW, true, false, CREASED, true><<<nb, kBlockL, 0, c.stream>>>(a);
-    } else if (topo) {
-        if (RW == 4 && uv) k_level_a<RW, true, true, CREASED, false><<<nb, kBlockL, 0, c.stream>>>(a);
-        else k_level_a<RW, true, false, CREASED, false><<<nb, kBlockL, 0, c.stream>>>(a);
+    if (topo) {
+        if (RW == 4 && uv) k_level_a<RW, true, true, CREASED><<<nb, kBlockL, 0, c.stream>>>(a);
+        else k_level_a<RW, true, false, CREASED><<<nb, kBlockL, 0, c.stream>>>(a);
     } else {
-        k_level_a<RW, false, false, CREASED, false><<<nb, kBlockL, 0, c.stream>>>(a);
+        k_level_a<RW, false, false, CREASED><<<nb, kBlockL, 0, c.stream>>>(a);
     }
     c.prof->end(c.stream);
 }

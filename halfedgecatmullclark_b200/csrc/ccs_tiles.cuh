@@ -146,10 +146,9 @@ __device__ __forceinline__ ARec load_arec(const int32_t* __restrict__ in, int64_
 
 // `tile` is BLOCK * 4 * RW ints of shared memory; every thread of the block
 // must call this with the same h0, and `rec` = its parent record.  The child
-// records go out through the shared tile and one bulk store per block, or
-// with DIRECT as each thread's own 16-byte vector stores (its 4 children are
-// 64 (48) contiguous bytes; a warp's stores cover 2 KB without gaps).
-template <int BLOCK, int RW, bool TOPO, bool UV, bool PTS, bool CREASED, bool DIRECT = false>
+// records go out through the shared tile and one bulk store per block (each
+// thread's own 16-byte vector stores, measured, ran 17% slower at depth 5).
+template <int BLOCK, int RW, bool TOPO, bool UV, bool PTS, bool CREASED>
 __device__ __forceinline__ void tile_level_a_rec(const LevelArgs& a, int64_t h0, int32_t* tile, ARec rec) {
     const int tid = threadIdx.x, lane = tid & 31;
     const int64_t h64 = h0 + tid;
@@ -213,19 +212,7 @@ __device__ __forceinline__ void tile_level_a_rec(const LevelArgs& a, int64_t h0,
             st3(a.pout + 3 * ((int64_t)a.V + a.F + ed), E);
         }
     }
-    if (TOPO && DIRECT) {
-        if (valid) {
-            int4* dst = reinterpret_cast<int4*>(a.out + (int64_t)4 * RW * h64);
-            if constexpr (RW == 4) {
-#pragma unroll
-                for (int m = 0; m < 4; ++m) dst[m] = make_int4(c_tw[m], c_ed[m], c_vx[m], UV ? uvc[m] : 0);
-            } else {
-                dst[0] = make_int4(c_tw[0], c_ed[0], c_vx[0], c_tw[1]);
-                dst[1] = make_int4(c_ed[1], c_vx[1], c_tw[2], c_ed[2]);
-                dst[2] = make_int4(c_vx[2], c_tw[3], c_ed[3], c_vx[3]);
-            }
-        }
-    } else if (TOPO) {
+    if (TOPO) {
         int32_t* t = tile + tid * 4 * RW;
         if constexpr (RW == 4) {
 #pragma unroll
@@ -244,10 +231,9 @@ __device__ __forceinline__ void tile_level_a_rec(const LevelArgs& a, int64_t h0,
     }
 }
 
-template <int BLOCK, int RW, bool TOPO, bool UV, bool PTS, bool CREASED, bool DIRECT = false>
+template <int BLOCK, int RW, bool TOPO, bool UV, bool PTS, bool CREASED>
 __device__ __forceinline__ void tile_level_a(const LevelArgs& a, int64_t h0, int32_t* tile) {
-    tile_level_a_rec<BLOCK, RW, TOPO, UV, PTS, CREASED, DIRECT>(a, h0, tile,
-                                                               load_arec<RW>(a.in, h0 + threadIdx.x, a.H));
+    tile_level_a_rec<BLOCK, RW, TOPO, UV, PTS, CREASED>(a, h0, tile, load_arec<RW>(a.in, h0 + threadIdx.x, a.H));
 }
 
 // ---------------------------------------------------------------------------
