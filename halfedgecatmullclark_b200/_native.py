@@ -110,6 +110,7 @@ SIGNATURES = {
     "ccs_BatchCageInfo_cuda": ([_P, ctypes.c_int32, ctypes.POINTER(BatchCageInfo)], _I),
     "ccs_BatchSetStream_cuda": ([_P, _P], _I),
     "ccs_BatchSetSchedule_cuda": ([_P, ctypes.c_int32], _I),
+    "ccs_BatchSetLaunchMode_cuda": ([_P, ctypes.c_int32], _I),
     "ccs_BatchSynchronize_cuda": ([_P], _I),
     "ccs_BatchDownload_cuda": ([_P, ctypes.c_int32, _P], _I),
     "ccs_BarrierTimeoutSelfTest_cuda": ([], _I),

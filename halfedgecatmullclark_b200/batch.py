@@ -76,8 +76,10 @@ class Batch:
         N.check(self.L.ccs_BatchSetStream_cuda(self.ptr, ctypes.c_void_p(int(handle) if handle else 0)),
                 "ccs_BatchSetStream_cuda")
 
-    def set_schedule(self, blocks_per_sm: int) -> None:
+    def set_schedule(self, blocks_per_sm: int, split: bool | None = None) -> None:
         N.check(self.L.ccs_BatchSetSchedule_cuda(self.ptr, int(blocks_per_sm)), "ccs_BatchSetSchedule_cuda")
+        if split is not None:
+            N.check(self.L.ccs_BatchSetLaunchMode_cuda(self.ptr, 1 if split else 0), "ccs_BatchSetLaunchMode_cuda")
 
     # -- device buffers as torch tensors (no copy) ----------------------------
     def arrays(self) -> dict:
@@ -207,10 +209,12 @@ def time_fwd_adj(batch: Batch, iters: int = 5, stream=None) -> float:
     return a.elapsed_time(b) / iters
 
 
-def autotune(batch: Batch, candidates=(0, 1, 2, 3, 4, 6, 8), iters: int = 5, use_cache: bool = True,
-             stream=None) -> dict:
-    """Choose resident blocks per SM for the persistent kernels (timed on
-    `stream`, default the current torch stream; the batch stays bound to it)."""
+def autotune(batch: Batch, candidates=(0, 2, 4, 6, 8), iters: int = 5, use_cache: bool = True,
+             stream=None, modes=(False, True)) -> dict:
+    """Choose the launch schedule -- one cooperative launch per depth or one
+    launch per section (`modes`: split or not) -- and the resident blocks
+    per SM of the persistent kernels, by timing forward + adjoint on `stream`
+    (default the current torch stream; the batch stays bound to it)."""
     path = cache_path()
     key = _key(batch)
     cache = {}
@@ -221,15 +225,17 @@ def autotune(batch: Batch, candidates=(0, 1, 2, 3, 4, 6, 8), iters: int = 5, use
         except Exception:
             cache = {}
     if use_cache and key in cache:
-        batch.set_schedule(cache[key]["blocks_per_sm"])
+        batch.set_schedule(cache[key]["blocks_per_sm"], bool(cache[key].get("split", False)))
         return dict(cache[key], cached=True)
     results = {}
-    for c in candidates:
-        batch.set_schedule(c)
-        results[c] = time_fwd_adj(batch, iters, stream)
+    for split in modes:
+        for c in candidates:
+            batch.set_schedule(c, split)
+            results[(split, c)] = time_fwd_adj(batch, iters, stream)
     best = min(results, key=results.get)
-    batch.set_schedule(best)
-    entry = {"blocks_per_sm": best, "ms": results[best], "tried": {str(k): v for k, v in results.items()}}
+    batch.set_schedule(best[1], best[0])
+    entry = {"blocks_per_sm": best[1], "split": best[0], "ms": results[best],
+             "tried": {("split/%d" if k[0] else "fused/%d") % k[1]: v for k, v in results.items()}}
     cache[key] = entry
     try:
         os.makedirs(os.path.dirname(path), exist_ok=True)

@@ -178,68 +178,90 @@ __device__ __forceinline__ QuadView<4> batch_quad_view_stats(const BatchArgs& a,
     return L;
 }
 
-template <bool TOPO, bool CREASED, bool DET>
-__global__ void __launch_bounds__(kBatchBlock)
-k_batch_forward(BatchArgs a, int d) {
-    __shared__ __align__(128) int32_t tile[kBatchBlock * 4 * 4];
+// ---------------------------------------------------------------------------
+// Forward and adjoint bodies, one function per section (a section is the
+// work between two grid barriers).  The fused schedule runs all sections of a
+// depth in one cooperative launch with grid barriers between them; the split
+// schedule launches each section on its own (ordinary launches, each kernel
+// with its own register budget).
+// ---------------------------------------------------------------------------
+// shape statistics of depth d + 1 (valence, boundary; cage tables only)
+template <bool TOPO>
+__device__ __forceinline__ void fwd_shape_next(const BatchArgs& a, int d) {
+    if (!TOPO) return;
     const int tid = threadIdx.x;
-    // shape statistics of depth d + 1 (valence, boundary; cage tables only)
-    auto shape_next = [&]() {
-        if (!TOPO) return;
-        for_tiles(a, d, PH_SHAPE_NEXT, [&](const BatchCage& bc, int64_t lt) {
-            const int64_t v = lt * kBatchBlock + tid;
-            if (d + 1 < bc.depth && v < bc.lv[d].V)
-                shape_stats_item(make_cage_tables(bc.cage), d + 1, a.stats + bc.stats[d + 1], (int32_t)v);
-        });
-    };
-    if (d == 0) {
-        if (TOPO) {
-            for_tiles(a, 0, PH_CAGE_TOPO, [&](const BatchCage& bc, int64_t lt) {
-                const int64_t i = lt * kBatchBlock + tid;
-                if (i >= 4 * (int64_t)bc.cage.H) return;
-                int32_t* out = a.he + 4 * (bc.he + bc.lv[1].heOff);
-                if (bc.uv) cage_topology_item<4, true, true>(make_cage_tables(bc.cage), out, i);
-                else cage_topology_item<4, true, false>(make_cage_tables(bc.cage), out, i);
-            });
-            for_tiles(a, 0, PH_CAGE_CREASE, [&](const BatchCage& bc, int64_t lt) {
-                const int64_t i = lt * kBatchBlock + tid;
-                if (i < bc.cage.E) crease_item(bc.cage.cr, a.cr + bc.cr + bc.lv[1].crOff, (int32_t)i);
-            });
-        }
-        for_tiles(a, 0, PH_CAGE_FACE, [&](const BatchCage& bc, int64_t lt) {
+    for_tiles(a, d, PH_SHAPE_NEXT, [&](const BatchCage& bc, int64_t lt) {
+        const int64_t v = lt * kBatchBlock + tid;
+        if (d + 1 < bc.depth && v < bc.lv[d].V)
+            shape_stats_item(make_cage_tables(bc.cage), d + 1, a.stats + bc.stats[d + 1], (int32_t)v);
+    });
+}
+
+// d = 0, section 1: cage topology, creases, face points, clearing
+template <bool TOPO, bool CREASED, bool DET>
+__device__ __forceinline__ void fwd_cage_s1(const BatchArgs& a) {
+    const int tid = threadIdx.x;
+    if (TOPO) {
+        for_tiles(a, 0, PH_CAGE_TOPO, [&](const BatchCage& bc, int64_t lt) {
             const int64_t i = lt * kBatchBlock + tid;
-            if (i >= bc.cage.F) return;
-            face_point_item<CageView, false>(batch_cage_view(bc), a.cagePts + 3 * bc.cagePt,
-                                             a.pts + 3 * (bc.pt + bc.lv[1].ptOff), (int32_t)i);
+            if (i >= 4 * (int64_t)bc.cage.H) return;
+            int32_t* out = a.he + 4 * (bc.he + bc.lv[1].heOff);
+            if (bc.uv) cage_topology_item<4, true, true>(make_cage_tables(bc.cage), out, i);
+            else cage_topology_item<4, true, false>(make_cage_tables(bc.cage), out, i);
         });
-        if (!DET) {
-            for_tiles(a, 0, PH_CAGE_ZERO, [&](const BatchCage& bc, int64_t lt) {
-                const int64_t i = lt * kBatchBlock + tid;
-                if (i < bc.cage.V) st3(a.pts + 3 * (bc.pt + bc.lv[1].ptOff + i), zero3());
-            });
-        }
-        if (!grid_sync(a.sync, a.spinCap, gridDim.x)) return;
-        for_tiles(a, 0, PH_CAGE_EDGE, [&](const BatchCage& bc, int64_t lt) {
+        for_tiles(a, 0, PH_CAGE_CREASE, [&](const BatchCage& bc, int64_t lt) {
             const int64_t i = lt * kBatchBlock + tid;
-            if (i >= bc.cage.H) return;
-            edge_owner_item<CageView, CREASED>(batch_cage_view(bc), a.cagePts + 3 * bc.cagePt,
-                                               a.pts + 3 * (bc.pt + bc.lv[1].ptOff), (int32_t)i);
+            if (i < bc.cage.E) crease_item(bc.cage.cr, a.cr + bc.cr + bc.lv[1].crOff, (int32_t)i);
         });
-        if (!grid_sync(a.sync, a.spinCap, gridDim.x)) return;
-        for_tiles(a, 0, PH_CAGE_VERT, [&](const BatchCage& bc, int64_t lt) {
-            const int64_t i = lt * kBatchBlock + tid;
-            const float* cp = a.cagePts + 3 * bc.cagePt;
-            float* pout = a.pts + 3 * (bc.pt + bc.lv[1].ptOff);
-            if (DET) {
-                if (i < bc.cage.V) vertex_det_item<CageView, CREASED>(batch_cage_view(bc), cp, pout, (int32_t)i);
-            } else {
-                // warp-collective: every lane of the tile takes part
-                vertex_atomic_item<CageView, CREASED>(batch_cage_view(bc), cp, pout, (int32_t)i, i < bc.cage.H);
-            }
-        });
-        shape_next();
-        return;
     }
+    for_tiles(a, 0, PH_CAGE_FACE, [&](const BatchCage& bc, int64_t lt) {
+        const int64_t i = lt * kBatchBlock + tid;
+        if (i >= bc.cage.F) return;
+        face_point_item<CageView, false>(batch_cage_view(bc), a.cagePts + 3 * bc.cagePt,
+                                         a.pts + 3 * (bc.pt + bc.lv[1].ptOff), (int32_t)i);
+    });
+    if (!DET) {
+        for_tiles(a, 0, PH_CAGE_ZERO, [&](const BatchCage& bc, int64_t lt) {
+            const int64_t i = lt * kBatchBlock + tid;
+            if (i < bc.cage.V) st3(a.pts + 3 * (bc.pt + bc.lv[1].ptOff + i), zero3());
+        });
+    }
+}
+
+// d = 0, section 2: edge points
+template <bool CREASED>
+__device__ __forceinline__ void fwd_cage_s2(const BatchArgs& a) {
+    const int tid = threadIdx.x;
+    for_tiles(a, 0, PH_CAGE_EDGE, [&](const BatchCage& bc, int64_t lt) {
+        const int64_t i = lt * kBatchBlock + tid;
+        if (i >= bc.cage.H) return;
+        edge_owner_item<CageView, CREASED>(batch_cage_view(bc), a.cagePts + 3 * bc.cagePt,
+                                           a.pts + 3 * (bc.pt + bc.lv[1].ptOff), (int32_t)i);
+    });
+}
+
+// d = 0, section 3: vertex points (+ shape statistics of depth 1)
+template <bool TOPO, bool CREASED, bool DET>
+__device__ __forceinline__ void fwd_cage_s3(const BatchArgs& a) {
+    const int tid = threadIdx.x;
+    for_tiles(a, 0, PH_CAGE_VERT, [&](const BatchCage& bc, int64_t lt) {
+        const int64_t i = lt * kBatchBlock + tid;
+        const float* cp = a.cagePts + 3 * bc.cagePt;
+        float* pout = a.pts + 3 * (bc.pt + bc.lv[1].ptOff);
+        if (DET) {
+            if (i < bc.cage.V) vertex_det_item<CageView, CREASED>(batch_cage_view(bc), cp, pout, (int32_t)i);
+        } else {
+            // warp-collective: every lane of the tile takes part
+            vertex_atomic_item<CageView, CREASED>(batch_cage_view(bc), cp, pout, (int32_t)i, i < bc.cage.H);
+        }
+    });
+    fwd_shape_next<TOPO>(a, 0);
+}
+
+// d >= 1, section 1: kernel A tiles, crease tiles, creased-edge statistics
+template <bool TOPO, bool CREASED, bool DET>
+__device__ __forceinline__ void fwd_level_s1(const BatchArgs& a, int d, int32_t* tile) {
+    const int tid = threadIdx.x;
     for_tiles(a, d, PH_A, [&](const BatchCage& bc, int64_t lt) {
         const Level& lv = bc.lv[d];
         LevelArgs la;
@@ -269,7 +291,12 @@ k_batch_forward(BatchArgs a, int d) {
                 crease_stats_item(batch_quad_view(a, bc, d), bc.lv[d - 1].V, a.stats + bc.stats[d], (int32_t)i);
         });
     }
-    if (!grid_sync(a.sync, a.spinCap, gridDim.x)) return;
+}
+
+// d >= 1, section 2: vertex pass (+ shape statistics of depth d + 1)
+template <bool TOPO, bool CREASED, bool DET>
+__device__ __forceinline__ void fwd_level_s2(const BatchArgs& a, int d) {
+    const int tid = threadIdx.x;
     if (DET && d >= 2) {
         for_tiles(a, d, PH_V, [&](const BatchCage& bc, int64_t lt) {
             const int64_t v = lt * kBatchBlock + tid;
@@ -293,39 +320,110 @@ k_batch_forward(BatchArgs a, int d) {
             if (v < L.V) vertex_det_item<QuadView<4>, CREASED>(L, pin, pout, (int32_t)v);
         }
     });
-    shape_next();
+    fwd_shape_next<TOPO>(a, d);
+}
+
+__device__ __forceinline__ float* adj_gnew(const BatchArgs& a, const BatchCage& bc, int d) {
+    return a.work + 3 * (bc.pt + bc.lv[d + 1].ptOff);
+}
+
+// adjoint, d = 0: three gathers (sections 1-3)
+template <int S>
+__device__ __forceinline__ void adj_cage_section(const BatchArgs& a) {
+    const int tid = threadIdx.x;
+    if (S == 1) {
+        for_tiles(a, 0, PH_ADJ_EDGE, [&](const BatchCage& bc, int64_t lt) {
+            const int64_t i = lt * kBatchBlock + tid;
+            if (i < bc.cage.H) adj_edge_item(batch_cage_view(bc), adj_gnew(a, bc, 0), (int32_t)i);
+        });
+    } else if (S == 2) {
+        for_tiles(a, 0, PH_ADJ_FACE, [&](const BatchCage& bc, int64_t lt) {
+            const int64_t i = lt * kBatchBlock + tid;
+            if (i < bc.cage.F) adj_face_item(batch_cage_view(bc), adj_gnew(a, bc, 0), (int32_t)i);
+        });
+    } else {
+        for_tiles(a, 0, PH_ADJ_VERT, [&](const BatchCage& bc, int64_t lt) {
+            const int64_t i = lt * kBatchBlock + tid;
+            if (i < bc.cage.V)
+                adj_vertex_item(batch_cage_view(bc), adj_gnew(a, bc, 0), a.gradCage + 3 * bc.cagePt, (int32_t)i);
+        });
+    }
+}
+
+// adjoint, d >= 1: edge pass (section 1), point pass (section 2)
+template <int S>
+__device__ __forceinline__ void adj_level_section(const BatchArgs& a, int d) {
+    if (S == 1) {
+        for_tiles(a, d, PH_ADJ_EDGE, [&](const BatchCage& bc, int64_t lt) {
+            adj_quad_edge_tile<4>(batch_quad_view_stats(a, bc, d), adj_gnew(a, bc, d), lt * kBatchBlock);
+        });
+    } else {
+        for_tiles(a, d, PH_ADJ_VERT, [&](const BatchCage& bc, int64_t lt) {
+            float* gOld = a.work + 3 * (bc.pt + bc.lv[d].ptOff);
+            if (d >= 2) adj_quad_point_tile<4, true>(batch_quad_view_stats(a, bc, d), adj_gnew(a, bc, d), gOld, lt * kBatchBlock);
+            else adj_quad_point_tile<4, false>(batch_quad_view_stats(a, bc, d), adj_gnew(a, bc, d), gOld, lt * kBatchBlock);
+        });
+    }
+}
+
+// fused schedule: one cooperative launch per depth, grid barriers between sections
+template <bool TOPO, bool CREASED, bool DET>
+__global__ void __launch_bounds__(kBatchBlock)
+k_batch_forward(BatchArgs a, int d) {
+    __shared__ __align__(128) int32_t tile[kBatchBlock * 4 * 4];
+    if (d == 0) {
+        fwd_cage_s1<TOPO, CREASED, DET>(a);
+        if (!grid_sync(a.sync, a.spinCap, gridDim.x)) return;
+        fwd_cage_s2<CREASED>(a);
+        if (!grid_sync(a.sync, a.spinCap, gridDim.x)) return;
+        fwd_cage_s3<TOPO, CREASED, DET>(a);
+        return;
+    }
+    fwd_level_s1<TOPO, CREASED, DET>(a, d, tile);
+    if (!grid_sync(a.sync, a.spinCap, gridDim.x)) return;
+    fwd_level_s2<TOPO, CREASED, DET>(a, d);
 }
 
 __global__ void __launch_bounds__(kBatchBlock)
 k_batch_adjoint(BatchArgs a, int d) {
-    const int tid = threadIdx.x;
-    auto gnew = [&](const BatchCage& bc) { return a.work + 3 * (bc.pt + bc.lv[d + 1].ptOff); };
     if (d == 0) {
-        for_tiles(a, 0, PH_ADJ_EDGE, [&](const BatchCage& bc, int64_t lt) {
-            const int64_t i = lt * kBatchBlock + tid;
-            if (i < bc.cage.H) adj_edge_item(batch_cage_view(bc), gnew(bc), (int32_t)i);
-        });
+        adj_cage_section<1>(a);
         if (!grid_sync(a.sync, a.spinCap, gridDim.x)) return;
-        for_tiles(a, 0, PH_ADJ_FACE, [&](const BatchCage& bc, int64_t lt) {
-            const int64_t i = lt * kBatchBlock + tid;
-            if (i < bc.cage.F) adj_face_item(batch_cage_view(bc), gnew(bc), (int32_t)i);
-        });
+        adj_cage_section<2>(a);
         if (!grid_sync(a.sync, a.spinCap, gridDim.x)) return;
-        for_tiles(a, 0, PH_ADJ_VERT, [&](const BatchCage& bc, int64_t lt) {
-            const int64_t i = lt * kBatchBlock + tid;
-            if (i < bc.cage.V) adj_vertex_item(batch_cage_view(bc), gnew(bc), a.gradCage + 3 * bc.cagePt, (int32_t)i);
-        });
+        adj_cage_section<3>(a);
         return;
     }
-    for_tiles(a, d, PH_ADJ_EDGE, [&](const BatchCage& bc, int64_t lt) {
-        adj_quad_edge_tile<4>(batch_quad_view_stats(a, bc, d), gnew(bc), lt * kBatchBlock);
-    });
+    adj_level_section<1>(a, d);
     if (!grid_sync(a.sync, a.spinCap, gridDim.x)) return;
-    for_tiles(a, d, PH_ADJ_VERT, [&](const BatchCage& bc, int64_t lt) {
-        float* gOld = a.work + 3 * (bc.pt + bc.lv[d].ptOff);
-        if (d >= 2) adj_quad_point_tile<4, true>(batch_quad_view_stats(a, bc, d), gnew(bc), gOld, lt * kBatchBlock);
-        else adj_quad_point_tile<4, false>(batch_quad_view_stats(a, bc, d), gnew(bc), gOld, lt * kBatchBlock);
-    });
+    adj_level_section<2>(a, d);
+}
+
+// split schedule: one ordinary launch per section (kernel boundaries order them)
+enum Section { SEC_CAGE_1 = 0, SEC_CAGE_2, SEC_CAGE_3, SEC_LEVEL_1, SEC_LEVEL_2 };
+
+template <bool TOPO, bool CREASED, bool DET, int S>
+__global__ void __launch_bounds__(kBatchBlock)
+k_batch_forward_section(BatchArgs a, int d) {
+    if constexpr (S == SEC_CAGE_1) fwd_cage_s1<TOPO, CREASED, DET>(a);
+    else if constexpr (S == SEC_CAGE_2) fwd_cage_s2<CREASED>(a);
+    else if constexpr (S == SEC_CAGE_3) fwd_cage_s3<TOPO, CREASED, DET>(a);
+    else if constexpr (S == SEC_LEVEL_1) {
+        __shared__ __align__(128) int32_t tile[kBatchBlock * 4 * 4];
+        fwd_level_s1<TOPO, CREASED, DET>(a, d, tile);
+    } else {
+        fwd_level_s2<TOPO, CREASED, DET>(a, d);
+    }
+}
+
+template <int S>
+__global__ void __launch_bounds__(kBatchBlock)
+k_batch_adjoint_section(BatchArgs a, int d) {
+    if constexpr (S == SEC_CAGE_1) adj_cage_section<1>(a);
+    else if constexpr (S == SEC_CAGE_2) adj_cage_section<2>(a);
+    else if constexpr (S == SEC_CAGE_3) adj_cage_section<3>(a);
+    else if constexpr (S == SEC_LEVEL_1) adj_level_section<1>(a, d);
+    else adj_level_section<2>(a, d);
 }
 
 // A one-block barrier that waits for a second arrival that never comes: the
@@ -366,6 +464,7 @@ struct ccs_Batch {
     cudaStream_t stream = nullptr;
     bool ownStream = false;
     int blocksPerSM = 0;                     // 0 = as many as fit
+    bool split = false;                      // one launch per section instead of per depth
     int numSMs = 148;
     bool graphOk = true;
     bool topoReady = false;                  // ccs_BatchRefine_cuda has run
@@ -540,8 +639,12 @@ static BatchArgs batch_args(ccs_Batch* b) {
     return a;
 }
 
+// A persistent launch: as many blocks as are resident at once (capped by the
+// schedule's blocks per SM), never more than the phase's tiles.  Cooperative
+// for the fused schedule, whose kernels meet at grid barriers.
 template <class Kernel>
-static cudaError_t launch_coop(ccs_Batch* b, Kernel kernel, int64_t maxTiles, BatchArgs a, int d) {
+static cudaError_t launch_persistent(ccs_Batch* b, Kernel kernel, int64_t maxTiles, BatchArgs a, int d, bool coop) {
+    if (maxTiles <= 0) return cudaSuccess;
     int perSM = 0;
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kernel, kBatchBlock, 0);
     if (e != cudaSuccess || perSM <= 0) return e != cudaSuccess ? e : cudaErrorLaunchOutOfResources;
@@ -557,8 +660,13 @@ static cudaError_t launch_coop(ccs_Batch* b, Kernel kernel, int64_t maxTiles, Ba
     attr[0].id = cudaLaunchAttributeCooperative;
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = coop ? 1 : 0;
     return cudaLaunchKernelEx(&cfg, kernel, a, d);
+}
+
+template <class Kernel>
+static cudaError_t launch_coop(ccs_Batch* b, Kernel kernel, int64_t maxTiles, BatchArgs a, int d) {
+    return launch_persistent(b, kernel, std::max<int64_t>(maxTiles, 1), a, d, true);
 }
 
 static int64_t max_tiles(const ccs_Batch* b, int d, std::initializer_list<int> phases) {
@@ -570,6 +678,29 @@ static int64_t max_tiles(const ccs_Batch* b, int d, std::initializer_list<int> p
 
 enum BatchOp { BOP_REFINE = 0, BOP_POINTS = 1, BOP_ADJOINT = 2 };
 
+// split schedule, forward: the sections of depth d as ordinary launches
+template <bool TOPO, bool CREASED, bool DET>
+static cudaError_t forward_sections(ccs_Batch* b, const BatchArgs& a, int d) {
+    cudaError_t e;
+    if (d == 0) {
+        e = launch_persistent(b, k_batch_forward_section<TOPO, CREASED, DET, SEC_CAGE_1>,
+                              max_tiles(b, 0, {PH_CAGE_TOPO, PH_CAGE_CREASE, PH_CAGE_FACE, PH_CAGE_ZERO}), a, 0, false);
+        if (e == cudaSuccess)
+            e = launch_persistent(b, k_batch_forward_section<TOPO, CREASED, DET, SEC_CAGE_2>,
+                                  max_tiles(b, 0, {PH_CAGE_EDGE}), a, 0, false);
+        if (e == cudaSuccess)
+            e = launch_persistent(b, k_batch_forward_section<TOPO, CREASED, DET, SEC_CAGE_3>,
+                                  max_tiles(b, 0, {PH_CAGE_VERT, PH_SHAPE_NEXT}), a, 0, false);
+        return e;
+    }
+    e = launch_persistent(b, k_batch_forward_section<TOPO, CREASED, DET, SEC_LEVEL_1>,
+                          max_tiles(b, d, {PH_A, PH_A_CREASE, PH_CREASE_STATS}), a, d, false);
+    if (e == cudaSuccess)
+        e = launch_persistent(b, k_batch_forward_section<TOPO, CREASED, DET, SEC_LEVEL_2>,
+                              max_tiles(b, d, {PH_V, PH_B, PH_SHAPE_NEXT}), a, d, false);
+    return e;
+}
+
 static cudaError_t enqueue_batch(ccs_Batch* b, int op, bool creased) {
     BatchArgs a = batch_args(b);
     cudaError_t e = cudaMemsetAsync(b->sync, 0, sizeof(GridSync), b->stream);
@@ -577,13 +708,41 @@ static cudaError_t enqueue_batch(ccs_Batch* b, int op, bool creased) {
     if (op == BOP_ADJOINT) {
         e = cudaMemsetAsync(b->gradCage, 0, sizeof(float) * 3 * (size_t)b->totCagePts, b->stream);
         for (int d = b->maxDepth - 1; d >= 0 && e == cudaSuccess; --d) {
-            const int64_t mt = max_tiles(b, d, {PH_ADJ_EDGE, PH_ADJ_FACE, PH_ADJ_VERT});
-            e = launch_coop(b, k_batch_adjoint, mt, a, d);
+            if (!b->split) {
+                const int64_t mt = max_tiles(b, d, {PH_ADJ_EDGE, PH_ADJ_FACE, PH_ADJ_VERT});
+                e = launch_coop(b, k_batch_adjoint, mt, a, d);
+            } else if (d == 0) {
+                e = launch_persistent(b, k_batch_adjoint_section<SEC_CAGE_1>, max_tiles(b, 0, {PH_ADJ_EDGE}), a, 0, false);
+                if (e == cudaSuccess)
+                    e = launch_persistent(b, k_batch_adjoint_section<SEC_CAGE_2>, max_tiles(b, 0, {PH_ADJ_FACE}), a, 0, false);
+                if (e == cudaSuccess)
+                    e = launch_persistent(b, k_batch_adjoint_section<SEC_CAGE_3>, max_tiles(b, 0, {PH_ADJ_VERT}), a, 0, false);
+            } else {
+                e = launch_persistent(b, k_batch_adjoint_section<SEC_LEVEL_1>, max_tiles(b, d, {PH_ADJ_EDGE}), a, d, false);
+                if (e == cudaSuccess)
+                    e = launch_persistent(b, k_batch_adjoint_section<SEC_LEVEL_2>, max_tiles(b, d, {PH_ADJ_VERT}), a, d, false);
+            }
         }
         return e;
     }
     const bool topo = op == BOP_REFINE;
     const bool det = (b->flags & CCS_FLAG_DETERMINISTIC) != 0;
+    if (b->split) {
+        const int v = (topo ? 4 : 0) + (creased ? 2 : 0) + (det ? 1 : 0);
+        for (int d = 0; d < b->maxDepth && e == cudaSuccess; ++d) {
+            switch (v) {
+                case 0: e = forward_sections<false, false, false>(b, a, d); break;
+                case 1: e = forward_sections<false, false, true>(b, a, d); break;
+                case 2: e = forward_sections<false, true, false>(b, a, d); break;
+                case 3: e = forward_sections<false, true, true>(b, a, d); break;
+                case 4: e = forward_sections<true, false, false>(b, a, d); break;
+                case 5: e = forward_sections<true, false, true>(b, a, d); break;
+                case 6: e = forward_sections<true, true, false>(b, a, d); break;
+                default: e = forward_sections<true, true, true>(b, a, d); break;
+            }
+        }
+        return e;
+    }
     for (int d = 0; d < b->maxDepth && e == cudaSuccess; ++d) {
         const int64_t mt = d == 0 ? max_tiles(b, 0, {PH_CAGE_TOPO, PH_CAGE_CREASE, PH_CAGE_FACE, PH_CAGE_ZERO,
                                                       PH_CAGE_EDGE, PH_CAGE_VERT, PH_SHAPE_NEXT})
@@ -740,6 +899,17 @@ int ccs_BatchSetSchedule_cuda(ccs_Batch* batch, int32_t blocksPerSM) {
         for (auto& kv : batch->graphs) cudaGraphExecDestroy(kv.second);
         batch->graphs.clear();
         batch->blocksPerSM = blocksPerSM;
+    }
+    return set_last_error(CCS_OK);
+}
+
+int ccs_BatchSetLaunchMode_cuda(ccs_Batch* batch, int32_t split) {
+    if (!batch || split < 0 || split > 1) return set_last_error(CCS_ERR_ARG);
+    std::lock_guard<std::mutex> lock(batch->mu);
+    if (batch->split != (split != 0)) {
+        for (auto& kv : batch->graphs) cudaGraphExecDestroy(kv.second);
+        batch->graphs.clear();
+        batch->split = split != 0;
     }
     return set_last_error(CCS_OK);
 }

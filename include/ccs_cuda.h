@@ -263,6 +263,10 @@ int ccs_BatchCageInfo_cuda(const ccs_Batch *batch, int32_t cage, ccs_BatchCageIn
 int ccs_BatchSetStream_cuda(ccs_Batch *batch, void *stream);
 /* Persistent grid size: resident blocks per SM (0 = all that fit). */
 int ccs_BatchSetSchedule_cuda(ccs_Batch *batch, int32_t blocksPerSM);
+/* Launch schedule: 0 = one cooperative launch per depth with grid barriers
+ * between its sections (default); 1 = one launch per section, each kernel
+ * with its own register budget. */
+int ccs_BatchSetLaunchMode_cuda(ccs_Batch *batch, int32_t split);
 /* Waits for the batch's stream; CCS_ERR_TIMEOUT if a grid barrier gave up. */
 int ccs_BatchSynchronize_cuda(ccs_Batch *batch);
 /* Copies one cage's hierarchy into the host arrays of a cc_Subd made for

@@ -121,3 +121,26 @@ def test_autotune_writes_and_reuses_cache(workloads, tmp_path, monkeypatch):
         assert not first["cached"] and (tmp_path / "tune.json").exists()
         again = B.autotune(b, candidates=(0, 1, 2), iters=2)
         assert again["cached"] and again["blocks_per_sm"] == first["blocks_per_sm"]
+
+
+def test_split_schedule_matches_fused(workloads):
+    """One launch per section gives what one cooperative launch per depth gives:
+    bit for bit with the deterministic flag (topology, points, adjoint)."""
+    import torch
+    from halfedgecatmullclark_b200 import _native as N
+    from halfedgecatmullclark_b200.batch import Batch
+    outs = []
+    for split in (False, True):
+        with Batch([w.cage for w in workloads], [w.depth for w in workloads], N.FLAG_DETERMINISTIC) as b:
+            b.set_schedule(0, split)
+            b.refine()
+            arr = b.arrays()
+            gen = torch.Generator(device="cuda").manual_seed(1)
+            arr["grad_points"].copy_(torch.randn(arr["grad_points"].shape, device="cuda", generator=gen))
+            b.adjoint()
+            b.synchronize()
+            outs.append((arr["halfedges"].cpu().numpy(), arr["points"].cpu().numpy(),
+                         arr["grad_cage_points"].cpu().numpy()))
+    assert np.array_equal(outs[0][0], outs[1][0])
+    assert np.array_equal(outs[0][1].view(np.uint32), outs[1][1].view(np.uint32))
+    assert rel_err(outs[1][2], outs[0][2]) <= 1e-5
