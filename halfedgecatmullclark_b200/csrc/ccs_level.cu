@@ -7,7 +7,7 @@
 //        contiguous bytes); the face's other records come from the 3 sibling
 //        lanes through shuffles;
 //      - builds the 4 child records (topology + UV code) in shared memory;
-//        one lane per warp then writes the warp's 2 KB of it with a single
+//        one thread then writes the block's 16 KB tile with a single
 //        cp.async.bulk store (TMA engine, no multicast);
 //      - face point of its face (lanes' vertex points combined by shuffles,
 //        in halfedge order), stored by the face's first lane;
@@ -57,7 +57,7 @@ static inline unsigned nblocksL(int64_t n) { return (unsigned)((n + kBlockL - 1)
 // 1.5x slower at depth 5: 5 resident blocks per SM instead of 8 hid less of
 // the gather latency than the extra overlap won.)
 template <int RW, bool TOPO, bool UV, bool CREASED>
-__global__ void __launch_bounds__(kBlockL, 8)
+__global__ void __launch_bounds__(kBlockL)
 k_level_a(LevelArgs a) {
     const int nbH = (a.H + kBlockL - 1) / kBlockL;
     if ((int)blockIdx.x >= nbH) {

@@ -222,14 +222,11 @@ __device__ __forceinline__ void tile_level_a_rec(const LevelArgs& a, int64_t h0,
 #pragma unroll
             for (int m = 0; m < 4; ++m) { t[3 * m] = c_tw[m]; t[3 * m + 1] = c_ed[m]; t[3 * m + 2] = c_vx[m]; }
         }
-        // each warp stores its own 32 parents' children (2 KB): no block-wide
-        // barrier, and a warp's lanes only ever write its own part of the tile
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncwarp();
-        if (lane == 0) {
-            const int64_t w0 = h0 + (tid & ~31);
-            const int64_t n = (a.H - w0) < 32 ? (a.H - w0) : 32;
-            if (n > 0) bulk_store_tile(a.out + 4 * RW * w0, tile + (tid & ~31) * 4 * RW, (uint32_t)(n * 16 * RW));
+        __syncthreads();
+        if (tid == 0) {
+            const int64_t n = (a.H - h0) < BLOCK ? (a.H - h0) : BLOCK;
+            bulk_store_tile(a.out + 4 * RW * h0, tile, (uint32_t)(n * 16 * RW));
         }
     }
 }
