@@ -641,16 +641,24 @@ static BatchArgs batch_args(ccs_Batch* b) {
 
 // A persistent launch: as many blocks as are resident at once (capped by the
 // schedule's blocks per SM), never more than the phase's tiles.  Cooperative
-// for the fused schedule, whose kernels meet at grid barriers.
+// for the fused schedule, whose kernels meet at grid barriers.  The split
+// schedule with no blocks-per-SM cap launches one block per tile instead.
 template <class Kernel>
 static cudaError_t launch_persistent(ccs_Batch* b, Kernel kernel, int64_t maxTiles, BatchArgs a, int d, bool coop) {
     if (maxTiles <= 0) return cudaSuccess;
-    int perSM = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kernel, kBatchBlock, 0);
-    if (e != cudaSuccess || perSM <= 0) return e != cudaSuccess ? e : cudaErrorLaunchOutOfResources;
-    if (b->blocksPerSM > 0) perSM = std::min(perSM, b->blocksPerSM);
-    int64_t grid = (int64_t)perSM * b->numSMs;
-    grid = std::max<int64_t>(1, std::min<int64_t>(grid, maxTiles));
+    int64_t grid;
+    if (!coop && b->blocksPerSM == 0) {
+        // split schedule, default: one block per tile, so the hardware
+        // scheduler overlaps the tiles' descriptor look-ups and gathers
+        grid = std::min<int64_t>(maxTiles, 0x7fffffff);
+    } else {
+        int perSM = 0;
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kernel, kBatchBlock, 0);
+        if (e != cudaSuccess || perSM <= 0) return e != cudaSuccess ? e : cudaErrorLaunchOutOfResources;
+        if (b->blocksPerSM > 0) perSM = std::min(perSM, b->blocksPerSM);
+        grid = (int64_t)perSM * b->numSMs;
+        grid = std::max<int64_t>(1, std::min<int64_t>(grid, maxTiles));
+    }
     cudaLaunchConfig_t cfg;
     memset(&cfg, 0, sizeof cfg);
     cfg.gridDim = dim3((unsigned)grid);

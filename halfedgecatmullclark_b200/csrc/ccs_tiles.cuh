@@ -1122,10 +1122,12 @@ __device__ __forceinline__ void adj_vertex_item(const View& L, const float* __re
 // forward's lane structure (a face's 4 halfedges in 4 adjacent lanes); needs
 // the twin relation vertex(twin h) = vertex(next h).
 // ---------------------------------------------------------------------------
-// Pass 1, tile of halfedges [h0, h0 + blockDim): the pair's larger halfedge
-// completes gE[e] += cE(h) gV[v(h)] + dE(next h) gV[v(next h)] + the same two
-// terms of the twin side, whose vertices are v(next h) and v(h).
-template <int RW>
+// Pass 1, tile of halfedges [h0, h0 + blockDim): each halfedge adds its
+// side's terms cE(h) gV[v(h)] + dE(next h) gV[v(next h)] to gE[e] (next h is
+// the quad's next lane) with one float atomic triple; with PAIR instead the
+// pair's larger halfedge completes gE[e] itself, recomputing the twin side's
+// coefficients (its vertices are v(next h) and v(h)).
+template <int RW, bool PAIR = false>
 __device__ __forceinline__ void adj_quad_edge_tile(const QuadView<RW>& L, float* __restrict__ gNew, int64_t h0) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31, k = lane & 3, qb = lane & ~3, ln = qb | ((k + 1) & 3);
@@ -1144,6 +1146,10 @@ __device__ __forceinline__ void adj_quad_edge_tile(const QuadView<RW>& L, float*
     }
     const float dEn = __shfl_sync(full, kc.dE, ln);
     const f3 gn = shfl3(g, ln);
+    if (!PAIR) {
+        if (valid) atomic_add3(gE + 3 * (int64_t)ed, add3(mul3(g, kc.cE), mul3(gn, dEn)));
+        return;
+    }
     if (!valid || !(h > tw)) return;
     f3 acc = add3(mul3(g, kc.cE), mul3(gn, dEn));
     if (tw >= 0) {
