@@ -1122,6 +1122,74 @@ __device__ __forceinline__ void adj_vertex_item(const View& L, const float* __re
 // forward's lane structure (a face's 4 halfedges in 4 adjacent lanes); needs
 // the twin relation vertex(twin h) = vertex(next h).
 // ---------------------------------------------------------------------------
+// Coefficients of the quad-level vertex rule from its ring statistics
+// (vertex_coef's formulas, corner-first branch order).
+__device__ __forceinline__ VCoef coef_from_stats(float vp, float cpre, float avgS, bool bnd, float cw, float pcw) {
+    const float valence = bnd ? vp + 1.0f : vp;
+    const float creaseCount = bnd ? cpre + cw : cpre;
+    VCoef k{0.0f, 0.0f, 0.0f, 0.0f};
+    if (creaseCount >= 3.0f || valence == 2.0f) {
+        k.a = 1.0f / vp;
+    } else if (creaseCount <= 1.0f) {
+        const float inv = 1.0f / (vp * vp);
+        k.a = (vp - 3.0f) * inv;
+        k.bF = -inv;
+        k.cE = 4.0f * inv;
+    } else {
+        const float t = fsat(avgS * 0.5f);
+        k.a = (1.0f - t) / vp + t * 0.25f * (cw + (bnd ? pcw : 0.0f));
+        k.cE = t * 0.25f * cw;
+        k.dE = bnd ? t * 0.25f * pcw : 0.0f;
+    }
+    return k;
+}
+
+// The vertex coefficients of halfedge h from its own record (tw, ed), its
+// prev lane's (ptw, ped) and, for child 0, its older vertex's statistics `st`
+// -- what vertex_coef finds by reading the level.
+template <int RW>
+__device__ __forceinline__ VCoef lane_vertex_coef(const QuadView<RW>& L, int32_t h, int32_t tw, int32_t ed,
+                                                  int32_t ptw, int32_t ped, const float4& st) {
+    const int k = h & 3;
+    float vp, cpre = 0.0f, avgS = 0.0f;
+    bool bnd = false;
+    if (k == 2) {
+        vp = L.d == 1 ? (float)L.t.fsz[L.t.he[(int64_t)CH_WORDS * (h >> 2) + CH_FACE]] : 4.0f;
+    } else if (k != 0) {
+        const int32_t eh = k == 1 ? ped : ed;
+        const float sa = L.sharp(eh), sb = L.sharp(eh ^ 1);
+        bnd = (k == 1 ? ptw : tw) < 0;
+        vp = bnd ? 2.0f : 4.0f;
+        const bool own = k == 3;
+        avgS = (bnd && own) ? sb : sa + sb;
+        cpre = (bnd && own) ? fsign(sb) : fsign(sa) + fsign(sb);
+    } else if (L.ostats) {
+        bnd = st.w != 0.0f;
+        vp = st.x;
+        const float own = L.sharp(ed);
+        avgS = bnd ? st.y - own : st.y;
+        cpre = bnd ? st.z - fsign(own) : st.z;
+    } else {
+        const RingStats r = creased_ring_walk(L, h);
+        vp = r.valence; cpre = r.creaseCount; avgS = r.avgS; bnd = r.fwd < 0;
+    }
+    return coef_from_stats(vp, cpre, avgS, bnd, fsign(L.sharp(ed)), fsign(L.sharp(ped)));
+}
+
+// A lane's record of a quad level: twin, edge, vertex (one 16-byte load for
+// 4-word records).
+template <int RW>
+__device__ __forceinline__ void lane_record(const QuadView<RW>& L, int64_t h64, int32_t& tw, int32_t& ed,
+                                            int32_t& vx) {
+    if constexpr (RW == 4) {
+        const int4 r = __ldg(reinterpret_cast<const int4*>(L.he) + h64);
+        tw = r.x; ed = r.y; vx = r.z;
+    } else {
+        tw = __ldg(L.he + 3 * h64 + 0);
+        ed = __ldg(L.he + 3 * h64 + 1);
+        vx = __ldg(L.he + 3 * h64 + 2);
+    }
+}
 // Pass 1, tile of halfedges [h0, h0 + blockDim): each halfedge adds its
 // side's terms cE(h) gV[v(h)] + dE(next h) gV[v(next h)] to gE[e] (next h is
 // the quad's next lane) with one float atomic triple; with PAIR instead the
@@ -1131,19 +1199,23 @@ template <int RW, bool PAIR = false>
 __device__ __forceinline__ void adj_quad_edge_tile(const QuadView<RW>& L, float* __restrict__ gNew, int64_t h0) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31, k = lane & 3, qb = lane & ~3, ln = qb | ((k + 1) & 3);
+    const int lp = qb | ((k + 3) & 3);
     const int64_t h64 = h0 + threadIdx.x;
     const bool valid = h64 < L.H;
     const int32_t h = (int32_t)h64;
     const float* gV = gNew;
     float* gE = gNew + 3 * ((int64_t)L.V + L.F);
     int32_t tw = -1, ed = 0, vx = 0;
-    VCoef kc{0.0f, 0.0f, 0.0f, 0.0f};
+    float4 st = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     f3 g = zero3();
     if (valid) {
-        tw = L.twin(h); ed = L.edge(h); vx = L.vert(h);
-        kc = vertex_coef(L, h);
+        lane_record(L, h64, tw, ed, vx);
         g = ld3(gV + 3 * (int64_t)vx);
+        if (k == 0 && L.ostats) st = L.ostats[vx];
     }
+    const int32_t ped = __shfl_sync(full, ed, lp), ptw = __shfl_sync(full, tw, lp);
+    VCoef kc{0.0f, 0.0f, 0.0f, 0.0f};
+    if (valid) kc = lane_vertex_coef(L, h, tw, ed, ptw, ped, st);
     const float dEn = __shfl_sync(full, kc.dE, ln);
     const f3 gn = shfl3(g, ln);
     if (!PAIR) {
@@ -1179,18 +1251,27 @@ __device__ __forceinline__ void adj_quad_point_tile(const QuadView<RW>& L, const
     const float* gV = gNew;
     const float* gF = gNew + 3 * (int64_t)L.V;
     const float* gE = gNew + 3 * ((int64_t)L.V + L.F);
-    int32_t vx = 0;
-    VCoef kc{0.0f, 0.0f, 0.0f, 0.0f};
-    ECoef ke{0.0f, 0.0f, 0.0f};
+    int32_t tw = -1, ed = 0, vx = 0;
+    float4 st = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     f3 gv = zero3(), ge = zero3(), gf = zero3();
     if (valid) {
-        const int32_t ed = L.edge(h);
-        vx = L.vert(h);
-        kc = vertex_coef(L, h);
-        ke = edge_coef(L, h);
+        lane_record(L, h64, tw, ed, vx);
         gv = ld3(gV + 3 * (int64_t)vx);
         ge = ld3(gE + 3 * (int64_t)ed);
-        if (k == 0) gf = ld3(gF + 3 * (int64_t)(h >> 2));
+        if (k == 0) {
+            gf = ld3(gF + 3 * (int64_t)(h >> 2));
+            if (L.ostats) st = L.ostats[vx];
+        }
+    }
+    const int32_t ped = __shfl_sync(full, ed, lp), ptw = __shfl_sync(full, tw, lp);
+    VCoef kc{0.0f, 0.0f, 0.0f, 0.0f};
+    ECoef ke{0.0f, 0.0f, 0.0f};
+    if (valid) {
+        kc = lane_vertex_coef(L, h, tw, ed, ptw, ped, st);
+        const float w = fsat(L.sharp(ed)), b = tw < 0 ? 1.0f : 0.5f;    // edge_coef
+        ke.al = (1.0f - w) * 0.25f + w * b * 0.5f;
+        ke.be = w * b * 0.5f;
+        ke.ga = (1.0f - w) * 0.25f;
     }
     f3 ft = add3(mul3(gv, kc.bF), mul3(ge, ke.ga));
     ft = add3(ft, shfl_xor3(ft, 1));
