@@ -77,7 +77,7 @@ k_adj_quad_edges(QuadView<RW> L, float* __restrict__ gNew) {
 }
 
 template <int RW, bool STRUCT>
-__global__ void __launch_bounds__(kBlockA)
+__global__ void __launch_bounds__(kBlockA, 8)
 k_adj_quad_points(QuadView<RW> L, const float* __restrict__ gNew, float* __restrict__ gOld) {
     adj_quad_point_tile<RW, STRUCT>(L, gNew, gOld, (int64_t)blockIdx.x * kBlockA);
 }

@@ -72,7 +72,7 @@ k_level_a(LevelArgs a) {
 
 // default vertex pass: one tile of halfedges per block
 template <int RW, bool CREASED, bool STRUCT>
-__global__ void __launch_bounds__(kBlockL, 5)
+__global__ void __launch_bounds__(kBlockL, 8)
 k_level_b(QuadView<RW> L, const float* __restrict__ pin, float* __restrict__ pout) {
     tile_level_b<RW, CREASED, STRUCT>(L, pin, pout, (int64_t)blockIdx.x * kBlockL);
 }
