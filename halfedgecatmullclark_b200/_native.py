@@ -79,6 +79,9 @@ SIGNATURES = {
     "ccs_Create_cuda": ([_P, ctypes.c_int32], _P),
     "ccs_CreateEx_cuda": ([_P, ctypes.c_int32, _U, ctypes.POINTER(_P)], _I),
     "ccs_Release_cuda": ([_P], None),
+    "ccs_LoadCage_cuda": ([ctypes.c_char_p], _P),
+    "ccs_ReleaseCage_cuda": ([_P], None),
+    "ccs_SaveCage_cuda": ([_P, ctypes.c_char_p], _I),
     "ccs_Refine_Scatter_cuda": ([_P], _I),
     "ccs_Refine_Gather_cuda": ([_P], _I),
     "ccs_RefineVertexPoints_Gather_cuda": ([_P], _I),
@@ -100,6 +103,7 @@ SIGNATURES = {
     "ccs_GetDeviceArrays_cuda": ([_P, ctypes.POINTER(DeviceArrays)], _I),
     "ccs_RefinePointsDevice_cuda": ([_P, _P, _P, _I, _P], _I),
     "ccs_AdjointPointsDevice_cuda": ([_P, _P, _P, _P], _I),
+    "ccs_HalfedgeNormals_cuda": ([_P, _P, _P, ctypes.c_int, _P], _I),
     "ccs_AdjointPointsDeviceNoAlloc_cuda": ([_P, _P, _P, _P], _I),
     "ccs_BatchCreate_cuda": ([_P, _P, ctypes.c_int32, _U, ctypes.POINTER(_P)], _I),
     "ccs_BatchRelease_cuda": ([_P], None),

@@ -73,3 +73,47 @@ def save(cage: Cage, path: str) -> None:
     """Write a ``.ccm`` file (``ccm_Save``, CatmullClark.h:3227-3269)."""
     with open(path, "wb") as fh:
         fh.write(dumps(cage))
+
+
+def load_pinned(path: str) -> Cage:
+    """Read a ``.ccm`` file with the C library's loader (``ccs_LoadCage_cuda``).
+
+    The returned cage's arrays are views of one page-locked host block (plain
+    host memory where the CUDA runtime cannot pin), so ``Subd`` uploads them
+    by DMA with no staging copy.  The block is released with the cage.
+    """
+    import ctypes
+    import weakref
+
+    from . import _native as N
+    from .mesh import cc_Mesh
+
+    L = N.lib()
+    ptr = L.ccs_LoadCage_cuda(path.encode())
+    if not ptr:
+        code = L.ccs_LastError_cuda()
+        raise CcmError("cc: cannot load %s (%s)" % (path, L.ccs_ErrorString_cuda(code).decode()))
+    m = cc_Mesh.from_address(ptr)
+
+    def view(addr, dtype, n):
+        dtype = np.dtype(dtype)
+        if n == 0 or not addr:
+            return np.zeros(0, dtype)
+        return np.frombuffer((ctypes.c_char * (n * dtype.itemsize)).from_address(addr), dtype, n)
+
+    V, U, E, F, H = m.vertexCount, m.uvCount, m.edgeCount, m.faceCount, m.halfedgeCount
+    cage = Cage(view(m.vertexPoints, np.float32, 3 * V).reshape(-1, 3),
+                view(m.halfedges, HALFEDGE_DTYPE, H), view(m.creases, CREASE_DTYPE, E),
+                view(m.vertexToHalfedgeIDs, np.int32, V), view(m.edgeToHalfedgeIDs, np.int32, E),
+                view(m.faceToHalfedgeIDs, np.int32, F), view(m.uvs, np.float32, 2 * U).reshape(-1, 2))
+    weakref.finalize(cage, L.ccs_ReleaseCage_cuda, ptr)
+    return cage
+
+
+def save_native(cage: Cage, path: str) -> None:
+    """Write a ``.ccm`` file with the C library's writer (``ccs_SaveCage_cuda``)."""
+    import ctypes
+
+    from . import _native as N
+    m = cage.as_cc_mesh()
+    N.check(N.lib().ccs_SaveCage_cuda(ctypes.byref(m), path.encode()), "ccs_SaveCage_cuda")

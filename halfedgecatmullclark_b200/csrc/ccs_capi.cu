@@ -615,6 +615,15 @@ int ccs_AdjointPointsDevice_cuda(cc_Subd* subd, const float* gradPoints, float* 
     return ret(run_adjoint(c, gradPoints, s->work, gradCage, s->cumV) == cudaSuccess ? CCS_OK : CCS_ERR_CUDA);
 }
 
+int ccs_HalfedgeNormals_cuda(cc_Subd* subd, const float* points, float* normals, int smooth, void* stream) {
+    SubdImpl* s = find(subd);
+    if (!s || !normals) return ret(CCS_ERR_ARG);
+    if (!s->topo_ready) return ret(CCS_ERR_STATE);
+    DeviceGuard g(s->device);
+    Ctx c = s->ctx(stream ? (cudaStream_t)stream : s->stream);
+    return ret(run_normals(c, points ? points : s->pts, normals, smooth != 0) == cudaSuccess ? CCS_OK : CCS_ERR_CUDA);
+}
+
 int ccs_LevelCounts_cuda(const cc_Mesh* cage, int32_t maxDepth, ccs_LevelCounts* out) {
     if (!cage || !out) return ret(CCS_ERR_ARG);
     std::vector<Level> lv;

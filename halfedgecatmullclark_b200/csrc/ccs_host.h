@@ -70,6 +70,9 @@ struct Ctx {
     bool fusable = true;         // the twin relation vertex(twin h) = vertex(next h) holds
 };
 
+// Records `s` as the calling thread's ccs_LastError_cuda() status; returns s.
+int set_last_error(int s);
+
 inline float4* stats_at(const Ctx& c, int d) {
     return (c.stats && c.statsOff && d >= 1 && d < c.D) ? c.stats + c.statsOff[d] : nullptr;
 }
@@ -83,6 +86,10 @@ cudaError_t run_points(const Ctx& c, const float* cagePts, float* pts, int mode,
 // level.  topo = also refine halfedges, UVs and creases.  mode must be
 // CCS_POINTS_SCATTER or CCS_POINTS_NOCREASES_SCATTER.
 cudaError_t run_fused(const Ctx& c, bool topo, const float* cagePts, float* pts, int mode, bool deterministic);
+
+// Per-halfedge normals of the finest level (ccs_normals.cu): `pts` all
+// levels' points (cumV x 3), `out` H(D) x 3.
+cudaError_t run_normals(const Ctx& c, const float* pts, float* out, bool smooth);
 
 // Ring statistics of the older vertices of every quad level (ccs_level.cu),
 // from the refined halfedges and creases.

@@ -157,6 +157,29 @@ class Subd:
             "cage_points": torch.as_tensor(_CudaArray(d.cagePoints, (self.cage.V, 3), "<f4"), device="cuda"),
         }
 
+    def normals(self, smooth: bool = True, points=None, out=None):
+        """Per-halfedge normals of the finest level as an (H, 3) float32 CUDA
+        tensor (ccs_HalfedgeNormal / ccs_HalfedgeNormal_Fast of
+        glsl/CatmullClark_Scatter.glsl:931-960).  `points` = a (cumV, 3) CUDA
+        tensor of every depth's points (default: the subd's own).  Runs on
+        torch's current stream: after refining on the subd's own stream, call
+        ``synchronize()`` (or ``set_stream`` it to torch's) first."""
+        import torch
+        H = self.levels[-1]["H"]
+        if out is None:
+            dev = points.device if points is not None else torch.device("cuda", torch.cuda.current_device())
+            out = torch.empty((H, 3), dtype=torch.float32, device=dev)
+        assert out.is_cuda and out.dtype == torch.float32 and out.is_contiguous() and out.numel() == 3 * H
+        pp = None
+        if points is not None:
+            assert points.is_cuda and points.dtype == torch.float32 and points.is_contiguous()
+            assert points.numel() == 3 * self.cumV
+            pp = points.data_ptr()
+        stream = torch.cuda.current_stream(out.device).cuda_stream
+        N.check(self.L.ccs_HalfedgeNormals_cuda(self.ptr, pp, out.data_ptr(), 1 if smooth else 0, stream),
+                "ccs_HalfedgeNormals_cuda")
+        return out
+
     def level_slice(self, level: int, what: str = "V") -> slice:
         """Rows of depth `level` (1..depth) inside the packed arrays."""
         lv = self.levels[level]

@@ -121,6 +121,17 @@ int ccs_CreateEx_cuda(const cc_Mesh *cage, int32_t maxDepth, uint32_t flags, cc_
 /* Replaces ccs_Release (CatmullClark.h:146, :977-983). NULL is a no-op. */
 void ccs_Release_cuda(cc_Subd *subd);
 
+/* `.ccm` cage files.  ccs_LoadCage_cuda replaces ccm_Load (CatmullClark.h:
+ * 74, :3186-3220): the cage and all its arrays land in one page-locked host
+ * allocation, so ccs_Create_cuda uploads it by DMA straight from the file's
+ * buffer; NULL on failure (ccs_LastError_cuda: CCS_ERR_ARG for a missing or
+ * malformed file).  Release it with ccs_ReleaseCage_cuda (ccm_Release, :79),
+ * after every subd made from it.  ccs_SaveCage_cuda replaces ccm_Save
+ * (:80, :3227-3269) and writes the same bytes (header padding zeroed). */
+cc_Mesh *ccs_LoadCage_cuda(const char *path);
+void ccs_ReleaseCage_cuda(cc_Mesh *cage);
+int ccs_SaveCage_cuda(const cc_Mesh *cage, const char *path);
+
 /* ---------------------------------------------------------------------- */
 /* Refinement (CatmullClark.h:197-212)                                     */
 /* ---------------------------------------------------------------------- */
@@ -215,6 +226,16 @@ int ccs_AdjointPointsDevice_cuda(cc_Subd *subd, const float *gradPoints, float *
  * serialised by the caller. */
 int ccs_AdjointPointsDeviceNoAlloc_cuda(cc_Subd *subd, const float *gradPoints, float *gradCage,
                                         void *stream);
+
+/* Per-halfedge normals of the finest level, the refined-surface consumer of
+ * the reference's GLSL library (glsl/CatmullClark_Scatter.glsl:931-960,
+ * ccs_HalfedgeNormal_Fast / ccs_HalfedgeNormal): `normals` (device, H(D) x 3
+ * floats) receives, per halfedge h of depth D, the normalised cross product
+ * of its face's edges at h, or with `smooth` the normalised sum of those of
+ * every halfedge around vertex(h) (the face normal on a boundary vertex).
+ * `points` = device points of every depth as ccs_RefinePointsDevice_cuda
+ * writes them, or NULL for the subd's own.  Needs the topology refined. */
+int ccs_HalfedgeNormals_cuda(cc_Subd *subd, const float *points, float *normals, int smooth, void *stream);
 
 /* ---------------------------------------------------------------------- */
 /* Batched refinement (no reference counterpart).                          */

@@ -173,3 +173,46 @@ def level_slice(cage, depth: int, level: int, what: str = "V"):
     per = {"V": "V", "H": "H", "C": "C"}[what]
     start = cnt[key][level - 1]
     return slice(start, start + cnt[per][level])
+
+
+def halfedge_normals(he_level, pts_level, smooth: bool = True):
+    """Per-halfedge normals of one quad level, in float64.
+
+    Restates glsl/CatmullClark_Scatter.glsl:931-940 (ccs_HalfedgeNormal_Fast:
+    normalize(cross(P[v(next h)] - P[v(h)], P[v(prev h)] - P[v(h)]))) and
+    :943-960 (ccs_HalfedgeNormal: add the fast normals of the halfedges met
+    walking prev-vertex halfedges, twin(prev h), back to h and normalise; a
+    walk that meets a boundary returns the fast normal).  `he_level` holds the
+    level's records (twin, edge, vertex[, uv]) and `pts_level` its points.
+    """
+    he = np.asarray(he_level)
+    P = np.asarray(pts_level, np.float64)
+    H = he.shape[0]
+    ids = np.arange(H, dtype=np.int64)
+    nxt = (ids & ~3) | ((ids + 1) & 3)
+    prv = (ids & ~3) | ((ids - 1) & 3)
+    vert = he[:, 2].astype(np.int64)
+    twin = he[:, 0].astype(np.int64)
+
+    def unit(v):
+        return v / np.linalg.norm(v, axis=1, keepdims=True)
+
+    v0 = P[vert]
+    fast = unit(np.cross(P[vert[nxt]] - v0, P[vert[prv]] - v0))
+    if not smooth:
+        return fast
+    acc = np.zeros_like(fast)
+    it = twin[prv]                       # ccs_PrevVertexHalfedgeID (CatmullClark.h:1168-1175)
+    live = (it >= 0) & (it != ids)
+    for _ in range(H):
+        if not live.any():
+            break
+        acc[live] += fast[it[live]]
+        step = it.copy()
+        step[live] = twin[prv[it[live]]]
+        it = np.where(live, step, it)
+        live = live & (it >= 0) & (it != ids)
+    closed = it >= 0
+    out = fast.copy()
+    out[closed] = unit(fast[closed] + acc[closed])
+    return out

@@ -88,3 +88,67 @@ def test_builder_conventions_on_a_single_quad():
     # (examples/obj_to_ccm.c:219-249), so boundary creases stay self-linked
     assert list(c.creases["nextID"]) == [0, 1, 2, 3]
     assert list(c.creases["prevID"]) == [0, 1, 2, 3]
+
+
+def test_native_ccm_loader_and_writer(tmp_path):
+    """ccs_LoadCage_cuda / ccs_SaveCage_cuda against the Python reader and
+    the files' own bytes (header padding aside)."""
+    from halfedgecatmullclark_b200 import build, ccm
+    build.build()
+    paths = ccm_paths()
+    if not paths:
+        pytest.skip("sample cages not available")
+    for p in paths:
+        ref = ccm.load(p)
+        cage = ccm.load_pinned(p)
+        for _, a in FIELDS:
+            assert np.array_equal(getattr(cage, a).view(np.uint8), getattr(ref, a).view(np.uint8)), (p, a)
+        out = str(tmp_path / "native.ccm")
+        ccm.save_native(cage, out)
+        data, again = open(p, "rb").read(), open(out, "rb").read()
+        assert again[:28] == data[:28] and again[28:32] == b"\0" * 4 and again[32:] == data[32:]
+        del cage
+
+
+def test_native_ccm_loader_errors(tmp_path):
+    from halfedgecatmullclark_b200 import _native as N, build, ccm, configs
+    build.build()
+    data = ccm.dumps(configs.torus_quads().cage)
+    bad = {"magic": b"cc_MeshX" + data[8:], "short": data[:-5], "tiny": b"xx",
+           "negative": data[:8] + (-1).to_bytes(4, "little", signed=True) + data[12:]}
+    for name, blob in bad.items():
+        path = tmp_path / (name + ".ccm")
+        path.write_bytes(blob)
+        with pytest.raises(ccm.CcmError):
+            ccm.load_pinned(str(path))
+        assert N.lib().ccs_LastError_cuda() == -1          # CCS_ERR_ARG
+    with pytest.raises(ccm.CcmError):
+        ccm.load_pinned(str(tmp_path / "missing.ccm"))
+    good = tmp_path / "good.ccm"
+    good.write_bytes(data)
+    assert ccm.dumps(ccm.load_pinned(str(good))) == data
+    N.lib().ccs_ReleaseCage_cuda(None)                    # NULL is a no-op
+
+
+@pytest.mark.gpu
+def test_subd_from_pinned_cage_matches():
+    """A subd made from a ccs_LoadCage_cuda cage (DMA upload from the file's
+    page-locked block) refines exactly like one from the Python reader."""
+    from conftest import gpu_available
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+    from halfedgecatmullclark_b200 import build, ccm
+    from halfedgecatmullclark_b200.subd import Subd
+    build.build()
+    paths = ccm_paths()
+    if not paths:
+        pytest.skip("sample cages not available")
+    for p in paths[:4]:
+        res = []
+        for cage in (ccm.load(p), ccm.load_pinned(p)):
+            with Subd(cage, 2, 4) as s:                  # deterministic: bit-comparable
+                s.refine("scatter")
+                s.download()
+                res.append((s.halfedges(), s.creases(), s.points()))
+        for a, b in zip(*res):
+            assert np.array_equal(a.view(np.uint8), b.view(np.uint8)), p
