@@ -56,18 +56,46 @@ static inline unsigned nblocksL(int64_t n) { return (unsigned)((n + kBlockL - 1)
 // prefetched the next tile's records and left each bulk store in flight ran
 // 1.5x slower at depth 5: 5 resident blocks per SM instead of 8 hid less of
 // the gather latency than the extra overlap won.)
+#ifndef CCS_A_MIN_BLOCKS
+#define CCS_A_MIN_BLOCKS 8
+#endif
 template <int RW, bool TOPO, bool UV, bool CREASED>
-__global__ void __launch_bounds__(kBlockL)
+__global__ void __launch_bounds__(kBlockL, CCS_A_MIN_BLOCKS)
 k_level_a(LevelArgs a) {
     const int nbH = (a.H + kBlockL - 1) / kBlockL;
     if ((int)blockIdx.x >= nbH) {
         if (!TOPO) return;
         const int64_t i = (int64_t)(blockIdx.x - nbH) * kBlockL + threadIdx.x;
-        if (i < a.C) crease_item(a.crIn, a.crOut, (int32_t)i);
+        if (i < a.C) {
+            const float2 sh = crease_item(a.crIn, a.crOut, (int32_t)i);
+            if (a.statsNext) crease_stats_next<RW>(a, (int32_t)i, sh);
+        }
         return;
     }
     __shared__ __align__(128) int32_t tile[kBlockL * 4 * RW];
     tile_level_a<kBlockL, RW, TOPO, UV, true, CREASED>(a, (int64_t)blockIdx.x * kBlockL, tile);
+}
+
+// depth d >= 2, default pass: kernel A and the vertex pass in one launch
+// (tile_level_ab); blocks after the halfedge tiles refine the creases
+#ifndef CCS_AB_MIN_BLOCKS
+#define CCS_AB_MIN_BLOCKS 6
+#endif
+template <int RW, bool TOPO, bool UV, bool CREASED>
+__global__ void __launch_bounds__(kBlockL, CCS_AB_MIN_BLOCKS)
+k_level_ab(LevelArgs a) {
+    const int nbH = (a.H + kBlockL - 1) / kBlockL;
+    if ((int)blockIdx.x >= nbH) {
+        if (!TOPO) return;
+        const int64_t i = (int64_t)(blockIdx.x - nbH) * kBlockL + threadIdx.x;
+        if (i < a.C) {
+            const float2 sh = crease_item(a.crIn, a.crOut, (int32_t)i);
+            if (a.statsNext) crease_stats_next<RW>(a, (int32_t)i, sh);
+        }
+        return;
+    }
+    __shared__ __align__(128) int32_t tile[TOPO ? kBlockL * 4 * RW : 4];
+    tile_level_ab<kBlockL, RW, TOPO, UV, CREASED>(a, (int64_t)blockIdx.x * kBlockL, tile, (int64_t)nbH * kBlockL);
 }
 
 // default vertex pass: one tile of halfedges per block
@@ -124,16 +152,31 @@ static QuadView<RW> quad_view_l(const Ctx& c, int d) {
     return L;
 }
 
-template <int RW>
-static void ring_stats_level(const Ctx& c, int d, cudaStream_t s) {
+// The shape half needs no level data; the crease half reads the level's
+// creases and halfedges and must follow the shape half.
+static void shape_stats_level(const Ctx& c, int d, cudaStream_t s) {
     float4* out = stats_at(c, d);
     if (!out || d < 1) return;
     const int32_t Vold = c.lv[d - 1].V;
-    const QuadView<RW> L = quad_view_l<RW>(c, d);
     c.prof->begin(s, CCS_K_RING_STATS, d, Vold);
-    k_shape_stats<<<nblocksL(Vold), kBlockL, 0, s>>>(L.t, d, out, Vold);
-    if (L.C > 0) k_crease_stats<RW><<<nblocksL(L.C), kBlockL, 0, s>>>(L, out, Vold);
+    k_shape_stats<<<nblocksL(Vold), kBlockL, 0, s>>>(make_cage_tables(*c.cage), d, out, Vold);
     c.prof->end(s);
+}
+
+template <int RW>
+static void crease_stats_level(const Ctx& c, int d, cudaStream_t s) {
+    float4* out = stats_at(c, d);
+    if (!out || d < 1 || c.lv[d].C <= 0) return;
+    const QuadView<RW> L = quad_view_l<RW>(c, d);
+    c.prof->begin(s, CCS_K_RING_STATS, d, L.C);
+    k_crease_stats<RW><<<nblocksL(L.C), kBlockL, 0, s>>>(L, out, c.lv[d - 1].V);
+    c.prof->end(s);
+}
+
+template <int RW>
+static void ring_stats_level(const Ctx& c, int d, cudaStream_t s) {
+    shape_stats_level(c, d, s);
+    crease_stats_level<RW>(c, d, s);
 }
 
 cudaError_t run_ring_stats(const Ctx& c) {
@@ -149,7 +192,7 @@ cudaError_t run_ring_stats(const Ctx& c) {
 struct Fork {
     const Ctx& c;
     bool on;
-    explicit Fork(const Ctx& cx) : c(cx), on(cx.side && cx.forkEv && cx.joinEv) {
+    explicit Fork(const Ctx& cx, bool want = true) : c(cx), on(want && cx.side && cx.forkEv && cx.joinEv) {
         if (on) {
             cudaEventRecord(c.forkEv, c.stream);
             cudaStreamWaitEvent(c.side, c.forkEv, 0);
@@ -165,6 +208,47 @@ struct Fork {
     }
 };
 
+// The crease half of depth d+1's ring statistics from the crease items of
+// the step d -> d+1 (needs the shape half written first).
+static void fold_crease_stats(const Ctx& c, int d, LevelArgs& a) {
+    a.statsNext = stats_at(c, d + 1);
+    a.t = make_cage_tables(*c.cage);
+    a.d = d;
+}
+
+// Slots [0, V(d+1)) of depth d+2: where the step d+1 -> d+2 accumulates.
+static void next_slots(const Ctx& c, int d, float* pts, LevelArgs& a) {
+    if (d + 2 <= c.D) {
+        a.zeroNext = pts + 3 * c.lv[d + 2].ptOff;
+        a.zeroNextN = 3 * (int64_t)c.lv[d + 1].V;
+    }
+}
+
+template <int RW, bool CREASED>
+static void level_ab(const Ctx& c, int d, bool topo, bool uv, float* pts) {
+    const Level& lv = c.lv[d];
+    LevelArgs a;
+    a.in = c.he + (int64_t)RW * lv.heOff;
+    a.out = c.he + (int64_t)RW * c.lv[d + 1].heOff;
+    a.crIn = c.cr + lv.crOff;
+    a.crOut = c.cr + c.lv[d + 1].crOff;
+    a.pin = pts + 3 * lv.ptOff;
+    a.pout = pts + 3 * c.lv[d + 1].ptOff;
+    a.H = lv.H; a.V = lv.V; a.F = lv.F; a.E = lv.E; a.C = lv.C;
+    a.ostats = stats_at(c, d);
+    if (topo) fold_crease_stats(c, d, a);
+    next_slots(c, d, pts, a);
+    const unsigned nb = nblocksL(lv.H) + (topo ? nblocksL(lv.C) : 0u);
+    c.prof->begin(c.stream, topo ? CCS_K_LEVEL_STEP : CCS_K_LEVEL_STEP_POINTS, d, lv.H);
+    if (topo) {
+        if (RW == 4 && uv) k_level_ab<RW, true, true, CREASED><<<nb, kBlockL, 0, c.stream>>>(a);
+        else k_level_ab<RW, true, false, CREASED><<<nb, kBlockL, 0, c.stream>>>(a);
+    } else {
+        k_level_ab<RW, false, false, CREASED><<<nb, kBlockL, 0, c.stream>>>(a);
+    }
+    c.prof->end(c.stream);
+}
+
 template <int RW, bool CREASED>
 static void level_a(const Ctx& c, int d, bool topo, bool uv, const float* pin, float* pout, bool zeroV) {
     const Level& lv = c.lv[d];
@@ -177,6 +261,7 @@ static void level_a(const Ctx& c, int d, bool topo, bool uv, const float* pin, f
     a.pout = pout;
     a.H = lv.H; a.V = lv.V; a.F = lv.F; a.E = lv.E; a.C = lv.C;
     a.zeroV = zeroV ? 1 : 0;
+    if (topo) fold_crease_stats(c, d, a);
     const unsigned nb = nblocksL(lv.H) + (topo ? nblocksL(lv.C) : 0u);
     c.prof->begin(c.stream, topo ? CCS_K_LEVEL_FUSED : CCS_K_FACE_POINTS, d, lv.H);
     if (topo) {
@@ -220,18 +305,43 @@ static void level_b_exact(const Ctx& c, int d, const float* pin, float* pout) {
 cudaError_t run_vertex_det_level(const Ctx& c, int d, const float* pin, float* pout, bool creased);
 cudaError_t run_cage_step(const Ctx& c, bool topo, bool uv, const float* cagePts, float* pout, int mode, bool det);
 
+// With the topology, the older vertices' ring statistics of every level are
+// built on the way (read by the default pass and by the adjoint): the shape
+// half of all levels on the second stream from the start (`shapes`, joined
+// before the first crease half), the crease half of level 1 beside kernel A
+// of depth 1, that of level d+1 by the crease items of the step d -> d+1.  The default pass runs depth 1 as
+// kernel A + vertex pass and every deeper level as one k_level_ab launch,
+// which reads the statistics of its level and clears the slots the next
+// level accumulates into (depth 3's are cleared by a memset at depth 1).
 template <int RW, bool CREASED>
-static cudaError_t fused_levels(const Ctx& c, bool topo, bool uv, float* pts, bool det) {
+static cudaError_t fused_levels(const Ctx& c, bool topo, bool uv, float* pts, bool det, Fork& shapes) {
+#ifdef CCS_NO_LEVEL_AB
+    bool ab = false;
+#else
+    bool ab = !det;
+#endif
+    for (int d = 2; d < c.D; ++d) ab = ab && stats_at(c, d) != nullptr;
     for (int d = 1; d < c.D; ++d) {
         const float* pin = pts + 3 * c.lv[d].ptOff;
         float* pout = pts + 3 * c.lv[d + 1].ptOff;
         const int step = c.prof->begin(c.stream, CCS_K_STEP, d, c.lv[d].H);
-        // with the topology: the older vertices' ring statistics of level d
-        // (read by the default pass and by the adjoint) beside kernel A
-        Fork f(c);
-        if (topo) ring_stats_level<RW>(c, d, f.stream());
-        level_a<RW, CREASED>(c, d, topo, uv, pin, pout, !det);
-        f.join();
+        if (topo && d == 1) {
+            // level 1's creases come from the cage step: the crease half of
+            // its statistics beside kernel A (whose crease items add level 2's)
+            shapes.join();
+            Fork f(c);
+            crease_stats_level<RW>(c, 1, f.stream());
+            level_a<RW, CREASED>(c, d, topo, uv, pin, pout, !det);
+            f.join();
+        } else if (ab && d >= 2) {
+            level_ab<RW, CREASED>(c, d, topo, uv, pts);
+            c.prof->end(c.stream, step);
+            continue;
+        } else {
+            level_a<RW, CREASED>(c, d, topo, uv, pin, pout, !det);
+        }
+        if (ab && d == 1 && c.D >= 3)
+            cudaMemsetAsync(pts + 3 * c.lv[3].ptOff, 0, sizeof(float) * 3 * (size_t)c.lv[2].V, c.stream);
         if (!det) {
             level_b<RW, CREASED>(c, d, pin, pout);
         } else if (d >= 2) {
@@ -249,12 +359,23 @@ static cudaError_t fused_levels(const Ctx& c, bool topo, bool uv, float* pts, bo
 cudaError_t run_fused(const Ctx& c, bool topo, const float* cagePts, float* pts, int mode, bool det) {
     const bool creased = mode == CCS_POINTS_SCATTER;
     const bool uv = c.cage->U > 0 && c.rw == 4;
+    // the shape half of every level's ring statistics beside the cage step
+    Fork shapes(c, topo && c.stats);
+    if (topo)
+        for (int d = 1; d < c.D; ++d) shape_stats_level(c, d, shapes.stream());
     const int step = c.prof->begin(c.stream, CCS_K_STEP, 0, c.lv[0].H);
     cudaError_t e = run_cage_step(c, topo, uv, cagePts, pts + 3 * c.lv[1].ptOff, mode, det);
     c.prof->end(c.stream, step);
-    if (e != cudaSuccess) return e;
-    if (c.rw == 4) return creased ? fused_levels<4, true>(c, topo, uv, pts, det) : fused_levels<4, false>(c, topo, uv, pts, det);
-    return creased ? fused_levels<3, true>(c, topo, false, pts, det) : fused_levels<3, false>(c, topo, false, pts, det);
+    if (e == cudaSuccess) {
+        if (c.rw == 4)
+            e = creased ? fused_levels<4, true>(c, topo, uv, pts, det, shapes)
+                        : fused_levels<4, false>(c, topo, uv, pts, det, shapes);
+        else
+            e = creased ? fused_levels<3, true>(c, topo, false, pts, det, shapes)
+                        : fused_levels<3, false>(c, topo, false, pts, det, shapes);
+    }
+    shapes.join();
+    return e;
 }
 
 }  // namespace ccs

@@ -75,6 +75,14 @@ __device__ __forceinline__ f3 quad_face_point(f3 p, int qb) {
     return acc;
 }
 
+// The same face point, and in `pn` the point of the next lane of the quad
+// (taken from the face point's shuffles, none of its own).
+__device__ __forceinline__ f3 quad_face_point_next(f3 p, int qb, int k, f3& pn) {
+    const f3 q0 = shfl3(p, qb), q1 = shfl3(p, qb + 1), q2 = shfl3(p, qb + 2), q3 = shfl3(p, qb + 3);
+    pn = k == 0 ? q1 : (k == 1 ? q2 : (k == 2 ? q3 : q0));
+    return add3(add3(add3(add3(zero3(), quarter3(q0)), quarter3(q1)), quarter3(q2)), quarter3(q3));
+}
+
 // One halfedge's share of its edge point: v0 = its vertex, v1 = the next
 // vertex, F = its face point (creased rule :2194-2241, plain rule :2107-2139).
 template <bool CREASED>
@@ -91,7 +99,7 @@ __device__ __forceinline__ f3 edge_share(f3 v0, f3 v1, f3 F, bool boundary, floa
 // ---------------------------------------------------------------------------
 // creases (CatmullClark.h:2950-2983, :2992-3026): item = parent crease
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void crease_item(const cc_Crease* __restrict__ in, cc_Crease* __restrict__ out,
+__device__ __forceinline__ float2 crease_item(const cc_Crease* __restrict__ in, cc_Crease* __restrict__ out,
                                             int32_t e) {
     const cc_Crease me = in[e];
     const int32_t nx = me.nextID, pv = me.prevID;
@@ -108,6 +116,7 @@ __device__ __forceinline__ void crease_item(const cc_Crease* __restrict__ in, cc
     y.sharpness = fmax_ref(0.0f, fsub(fquarter(fadd(thisS, cn.sharpness)), 1.0f));
     out[2 * (int64_t)e + 0] = x;
     out[2 * (int64_t)e + 1] = y;
+    return make_float2(x.sharpness, y.sharpness);
 }
 
 // ---------------------------------------------------------------------------
@@ -122,7 +131,42 @@ struct LevelArgs {
     float* __restrict__ pout;           // depth-(d+1) points
     int32_t H, V, F, E, C;              // depth-d counts
     int zeroV = 0;                      // clear the vertex slots the atomic pass accumulates into
+    float* __restrict__ zeroNext = nullptr;  // floats to clear for the next level's accumulation
+    int64_t zeroNextN = 0;
+    const float4* __restrict__ ostats = nullptr;  // older vertices' ring statistics (tile_level_ab)
+    // crease half of depth d+1's ring statistics, added by the crease items
+    // (the shape half must already be there); null = not kept
+    float4* __restrict__ statsNext = nullptr;
+    CageTables t;
+    int32_t d = 0;
 };
+
+// Crease item e of depth d >= 1 that made children 2e, 2e+1 of sharpness
+// `s`: each child's sharpness and sign go to the ring statistics of its end
+// that is a depth-d vertex (crease_stats_item's rule, located without depth
+// d+1's records).  Child 0 of halfedge h runs along half 2 e(h) + (h > twin
+// ? 0 : 1) of e(h) from vertex(h); so with h0 = a halfedge of e, half b0 =
+// (h0 > twin(h0) ? 0 : 1) ends at vertex(h0) and the other half at
+// vertex(next h0).
+template <int RW>
+__device__ __forceinline__ void crease_stats_next(const LevelArgs& a, int32_t e, float2 s) {
+    if (s.x == 0.0f && s.y == 0.0f) return;
+    const int32_t h0 = edge_to_he(a.t, e, a.d);
+    const int32_t tw0 = __ldg(a.in + (int64_t)RW * h0 + 0);
+    const int32_t v0 = __ldg(a.in + (int64_t)RW * h0 + 2);
+    const int32_t v1 = __ldg(a.in + (int64_t)RW * qnext(h0) + 2);
+    const int b0 = h0 > tw0 ? 0 : 1;
+    if (s.x != 0.0f) {
+        float* o = reinterpret_cast<float*>(a.statsNext + (b0 == 0 ? v0 : v1));
+        atomicAdd(o + 1, s.x);
+        atomicAdd(o + 2, fsign(s.x));
+    }
+    if (s.y != 0.0f) {
+        float* o = reinterpret_cast<float*>(a.statsNext + (b0 == 1 ? v0 : v1));
+        atomicAdd(o + 1, s.y);
+        atomicAdd(o + 2, fsign(s.y));
+    }
+}
 
 // One parent record (twin, edge, vertex, uv); zeros past the level's end.
 struct ARec {
@@ -142,6 +186,36 @@ __device__ __forceinline__ ARec load_arec(const int32_t* __restrict__ in, int64_
         }
     }
     return r;
+}
+
+// Writes a thread's four child records to its 16 * RW-byte slot of the shared
+// tile with 16-byte stores free of bank conflicts.  RW = 4: the slots are 64
+// bytes apart, so lanes start at different children (lane pair u of each
+// quarter-warp at child u): the eight stores of a quarter-warp then cover
+// the 32 banks once.  RW = 3: the three 16-byte words of 48-byte slots are
+// conflict-free as they are (48 / 16 = 3 is odd).
+template <int RW, bool UV>
+__device__ __forceinline__ void put_children(int32_t* tile, int tid, int lane, const int32_t (&tw)[4],
+                                             const int32_t (&ed)[4], const int32_t (&vx)[4],
+                                             const int32_t (&uv)[4]) {
+    int4* t4 = reinterpret_cast<int4*>(tile) + tid * RW;
+    if constexpr (RW == 4) {
+        int4 r0 = make_int4(tw[0], ed[0], vx[0], UV ? uv[0] : 0);
+        int4 r1 = make_int4(tw[1], ed[1], vx[1], UV ? uv[1] : 0);
+        int4 r2 = make_int4(tw[2], ed[2], vx[2], UV ? uv[2] : 0);
+        int4 r3 = make_int4(tw[3], ed[3], vx[3], UV ? uv[3] : 0);
+        const int r = (lane >> 1) & 3;
+        if (r & 1) { const int4 x = r0; r0 = r1; r1 = r2; r2 = r3; r3 = x; }
+        if (r & 2) { int4 x = r0; r0 = r2; r2 = x; x = r1; r1 = r3; r3 = x; }
+        t4[r] = r0;
+        t4[(r + 1) & 3] = r1;
+        t4[(r + 2) & 3] = r2;
+        t4[(r + 3) & 3] = r3;
+    } else {
+        t4[0] = make_int4(tw[0], ed[0], vx[0], tw[1]);
+        t4[1] = make_int4(ed[1], vx[1], tw[2], ed[2]);
+        t4[2] = make_int4(vx[2], tw[3], ed[3], vx[3]);
+    }
 }
 
 // `tile` is BLOCK * 4 * RW ints of shared memory; every thread of the block
@@ -179,8 +253,8 @@ __device__ __forceinline__ void tile_level_a_rec(const LevelArgs& a, int64_t h0,
     }
     if (PTS) {
         const f3 p = valid ? ld3(a.pin + 3 * (int64_t)vx) : zero3();
-        const f3 Fp = quad_face_point(p, qb);
-        const f3 pn = shfl3(p, ln);
+        f3 pn;
+        const f3 Fp = quad_face_point_next(p, qb, k, pn);
         if (valid && k == 0) st3(a.pout + 3 * ((int64_t)a.V + f), Fp);
         if (a.zeroV && h64 < a.V) st3(a.pout + 3 * h64, zero3());
         // edge point, by the pair's larger halfedge; the smaller one's share
@@ -213,15 +287,7 @@ __device__ __forceinline__ void tile_level_a_rec(const LevelArgs& a, int64_t h0,
         }
     }
     if (TOPO) {
-        int32_t* t = tile + tid * 4 * RW;
-        if constexpr (RW == 4) {
-#pragma unroll
-            for (int m = 0; m < 4; ++m)
-                reinterpret_cast<int4*>(t)[m] = make_int4(c_tw[m], c_ed[m], c_vx[m], UV ? uvc[m] : 0);
-        } else {
-#pragma unroll
-            for (int m = 0; m < 4; ++m) { t[3 * m] = c_tw[m]; t[3 * m + 1] = c_ed[m]; t[3 * m + 2] = c_vx[m]; }
-        }
+        put_children<RW, UV>(tile, tid, lane, c_tw, c_ed, c_vx, uvc);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (tid == 0) {
@@ -384,6 +450,155 @@ __device__ __forceinline__ void tile_level_b(const QuadView<RW>& L, const float*
             atomic_add3(o, s);
         }
     } else if (valid) {
+        atomic_add3(o, s);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// quad level d >= 2, one pass for the whole default step d -> d+1: kernel A's
+// body (child records, face and edge points) and the default vertex pass's
+// body (tile_level_b with STRUCT) over the same tile of depth-d halfedges.
+// ---------------------------------------------------------------------------
+// The vertex share of halfedge h needs its face point (the quad's lanes), its
+// own edge point and that of prev(h) (a lane of the quad), its vertex point
+// and the ring statistics; only the last come from memory (the older
+// vertices' table `ostats`; face centres and edge midpoints from the
+// structure).  So every halfedge evaluates its own edge point, not only the
+// pair's owner.  The twin face of an edge interior to a parent quad (child 1
+// or 2, whose twin is child 2 or 1 of a sibling quad in the same 16-lane
+// group) is read from that quad's lanes; across a parent edge (children 0
+// and 3) it is rebuilt from the twin quad's records as kernel A does.  Both
+// halves evaluate (0 + share(smaller halfedge)) + share(larger halfedge), so
+// both hold the owner's value bit for bit; the owner stores it.
+// The vertex slots [0, V) of depth d+1 must be zero on entry; the tile also
+// clears its share of `zeroNext` (the slots the next level accumulates into).
+// Requires BLOCK a multiple of 32 and h0 a multiple of 16.
+template <int BLOCK, int RW, bool TOPO, bool UV, bool CREASED>
+__device__ __forceinline__ void tile_level_ab(const LevelArgs& a, int64_t h0, int32_t* tile, int64_t zeroStride) {
+    const unsigned full = 0xffffffffu;
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int64_t h64 = h0 + tid;
+    const bool valid = h64 < a.H;
+    const int32_t h = (int32_t)h64;
+    const ARec rec = load_arec<RW>(a.in, h64, a.H);
+    const int k = lane & 3, qb = lane & ~3, j = (lane >> 2) & 3;
+    const int32_t tw = rec.tw, ed = rec.ed, vx = rec.vx;
+    const int ln = qb | ((k + 1) & 3), lp = qb | ((k + 3) & 3);
+    const int32_t f = h >> 2;
+    const int32_t ptw = __shfl_sync(full, tw, lp);
+    const int32_t ped = __shfl_sync(full, ed, lp);
+    if (TOPO) {
+        const int lo = qb | ((k + 2) & 3);
+        const int32_t prev = (h & ~3) | ((k + 3) & 3), next = (h & ~3) | ((k + 1) & 3);
+        int32_t c_tw[4], c_ed[4], c_vx[4], uvc[4] = {rec.uv, 0, 0, 0};
+        if (UV) {
+            const float u = uv_dec_fast((uint32_t)rec.uv), v = uv_dec_fast((uint32_t)rec.uv >> 16);
+            const float un = __shfl_sync(full, u, ln), vn = __shfl_sync(full, v, ln);
+            const float uo = __shfl_sync(full, u, lo), vo = __shfl_sync(full, v, lo);
+            const float up = __shfl_sync(full, u, lp), vp = __shfl_sync(full, v, lp);
+            uvc[1] = uv_enc_fast(flerp(u, un, 0.5f), flerp(v, vn, 0.5f));
+            uvc[2] = uv_enc_fast(fquarter(fadd(fadd(fadd(u, un), uo), up)),
+                                 fquarter(fadd(fadd(fadd(v, vn), vo), vp)));
+            uvc[3] = uv_enc_fast(flerp(u, up, 0.5f), flerp(v, vp, 0.5f));
+        }
+        c_tw[0] = child(qnext(tw), 3); c_tw[1] = child(next, 2); c_tw[2] = child(prev, 1); c_tw[3] = child(ptw, 0);
+        c_ed[0] = 2 * ed + (h > tw ? 0 : 1); c_ed[1] = 2 * a.E + h; c_ed[2] = 2 * a.E + prev;
+        c_ed[3] = 2 * ped + (prev > ptw ? 1 : 0);
+        c_vx[0] = vx; c_vx[1] = a.V + a.F + ed; c_vx[2] = a.V + f; c_vx[3] = a.V + a.F + ped;
+        put_children<RW, UV>(tile, tid, lane, c_tw, c_ed, c_vx, uvc);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            const int64_t n = (a.H - h0) < BLOCK ? (a.H - h0) : BLOCK;
+            bulk_store_tile(a.out + 4 * RW * h0, tile, (uint32_t)(n * 16 * RW));
+        }
+    }
+    // clear this thread's share of the next level's accumulation slots
+    for (int64_t i = h64; i < a.zeroNextN; i += zeroStride) a.zeroNext[i] = 0.0f;
+
+    const f3 p = valid ? ld3(a.pin + 3 * (int64_t)vx) : zero3();
+    f3 pn;
+    const f3 Fp = quad_face_point_next(p, qb, k, pn);
+    if (valid && k == 0) st3(a.pout + 3 * ((int64_t)a.V + f), Fp);
+    const float sOwn = CREASED ? (valid && ed < a.C ? a.crIn[ed].sharpness : 0.0f) : 0.0f;
+    // the twin face of an edge inside the parent quad: a sibling quad's lanes
+    const int sib = (lane & ~15) | (k == 1 ? ((((j + 1) & 3) << 2) | 2) : ((((j + 3) & 3) << 2) | 1));
+    const f3 Fsib = shfl3(Fp, sib);
+    f3 E = zero3();
+    if (valid) {
+        const float w = CREASED ? fsat(sOwn) : 0.0f;
+        const f3 sh_h = edge_share<CREASED>(p, pn, Fp, tw < 0, w);
+        if (tw >= 0) {
+            const int32_t sibTw = k == 1 ? ((h & ~15) | ((((j + 1) & 3) << 2) | 2))
+                                         : ((h & ~15) | ((((j + 3) & 3) << 2) | 1));
+            f3 Ft;
+            if ((k == 1 || k == 2) && tw == sibTw) {
+                Ft = Fsib;
+            } else {
+                const int32_t tb = tw & ~3, kt = tw & 3;
+                f3 q[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    if (i == kt) q[i] = pn;
+                    else if (i == ((kt + 1) & 3)) q[i] = p;
+                    else q[i] = ld3(a.pin + 3 * (int64_t)__ldg(a.in + (int64_t)RW * (tb + i) + 2));
+                }
+                Ft = zero3();
+#pragma unroll
+                for (int i = 0; i < 4; ++i) Ft = add3(Ft, quarter3(q[i]));
+            }
+            const f3 sh_t = edge_share<CREASED>(pn, p, Ft, false, w);
+            E = h > tw ? add3(add3(zero3(), sh_t), sh_h) : add3(add3(zero3(), sh_h), sh_t);
+        } else {
+            E = add3(zero3(), sh_h);
+        }
+        if (h > tw) st3(a.pout + 3 * ((int64_t)a.V + a.F + ed), E);
+    }
+
+    // vertex share of h (tile_level_b, STRUCT)
+    const f3 Ep = shfl3(E, lp);
+    const float sPrev = __shfl_sync(full, sOwn, lp);
+    float4 st = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (valid && k == 0) st = a.ostats[vx];
+    f3 s = zero3();
+    if (valid) {
+        float vpre, cpre = 0.0f, avgS = 0.0f;
+        bool bnd = false;
+        if (k == 2) {
+            vpre = 4.0f;
+        } else if (k != 0) {
+            bnd = (k == 1 ? ptw : tw) < 0;
+            vpre = bnd ? 2.0f : 4.0f;
+            if (CREASED) {
+                const int32_t eh = k == 1 ? ped : ed;    // one half of the parent edge
+                const float sa = k == 1 ? sPrev : sOwn;
+                const int32_t eo = eh ^ 1;
+                const float sb = eo < a.C ? a.crIn[eo].sharpness : 0.0f;
+                const bool own = k == 3;                 // the walk from h skips its own edge
+                avgS = (bnd && own) ? sb : fadd(sa, sb);
+                cpre = (bnd && own) ? fsign(sb) : fadd(fsign(sa), fsign(sb));
+            }
+        } else {
+            bnd = st.w != 0.0f;
+            vpre = st.x;
+            if (CREASED) {
+                avgS = bnd ? fsub(st.y, sOwn) : st.y;
+                cpre = bnd ? fsub(st.z, fsign(sOwn)) : st.z;
+            }
+        }
+        s = quad_vertex_rule<CREASED>(p, Fp, E, Ep, vpre, cpre, avgS, bnd, CREASED ? fsign(sOwn) : 0.0f,
+                                      CREASED ? fsign(sPrev) : 0.0f);
+    }
+    float* o = a.pout + 3 * (int64_t)vx;
+    const f3 s4 = shfl_down3(s, 4), s8 = shfl_down3(s, 8), s12 = shfl_down3(s, 12);
+    const int partner = (lane & ~15) | ((((lane >> 2) + 1) & 3) << 2) | 3;
+    const f3 sA2 = shfl3(s, partner);
+    if (!valid) return;
+    if ((lane & 15) == 2) {
+        st3(o, add3(add3(add3(add3(zero3(), s), s4), s8), s12));
+    } else if (k == 1) {
+        atomic_add3(o, (lane & 12) == 12 ? add3(sA2, s) : add3(s, sA2));
+    } else if (k == 0) {
         atomic_add3(o, s);
     }
 }

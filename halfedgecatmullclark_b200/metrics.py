@@ -50,6 +50,14 @@ def kernel_bytes(kernel: str, lv: dict, rec: int = 16) -> int:
         # records + crease records + face and edge points + points in, the
         # older vertices' ring statistics (16 B), vertex points out
         return int(rec * H + 12 * C + 12 * F + 12 * E + 12 * V + 16 * max(V - nb, 0) + 12 * V)
+    if kernel in ("level_step", "level_step_points"):
+        # one launch for the whole default step: records in (+ children out
+        # and the creases with the topology), points in, face, edge and
+        # vertex points out, the older vertices' ring statistics and the
+        # level's crease records; the slots cleared for the next level are
+        # not counted (none at the last level)
+        topo = 4 * rec * H + 36 * C if kernel == "level_step" else 12 * C
+        return int(rec * H + topo + 12 * V + 12 * F + 12 * E + 12 * V + 16 * max(V - nb, 0))
     if kernel == "ring_stats":
         # records of children 0 and 3 walked, statistics out
         return int(rec * H // 2 + 16 * max(V - nb, 0))

@@ -327,7 +327,9 @@ enum {
     CCS_K_VERTEX_POINTS = 4, CCS_K_CLEAR = 5, CCS_K_LEVEL_FUSED = 6, CCS_K_ADJOINT = 7,
     CCS_K_UVS = 8, CCS_K_LEVEL_POINTS = 9, CCS_K_OLD_VERTICES = 10, CCS_K_RING_STATS = 11,
     CCS_K_ADJ_EDGES = 12, CCS_K_ADJ_FACES = 13, CCS_K_ADJ_VERTICES = 14, CCS_K_EXACT_POINTS = 15,
-    CCS_K_STEP = 16 /* a whole refinement step d -> d+1, on the subd's stream */, CCS_K_COUNT = 17
+    CCS_K_STEP = 16 /* a whole refinement step d -> d+1, on the subd's stream */,
+    CCS_K_LEVEL_STEP = 17 /* depth >= 2: topology, creases and all points in one launch */,
+    CCS_K_LEVEL_STEP_POINTS = 18 /* depth >= 2: all points of a step in one launch */, CCS_K_COUNT = 19
 };
 /* When enabled, every launch of the subd is bracketed by CUDA events on its
  * stream (and CUDA graphs are not used). */
