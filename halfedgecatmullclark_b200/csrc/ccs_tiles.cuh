@@ -487,6 +487,110 @@ __device__ __forceinline__ void tile_level_ab(const LevelArgs& a, int64_t h0, in
     const int32_t f = h >> 2;
     const int32_t ptw = __shfl_sync(full, tw, lp);
     const int32_t ped = __shfl_sync(full, ed, lp);
+
+    // every load that needs only the record, issued before any is used
+    const int sibK = k == 1 ? ((((j + 1) & 3) << 2) | 2) : ((((j + 3) & 3) << 2) | 1);
+    const bool inner = (k == 1 || k == 2) && tw == ((h & ~15) | sibK);
+    const bool gatherTwin = valid && tw >= 0 && !inner;
+    const f3 p = valid ? ld3(a.pin + 3 * (int64_t)vx) : zero3();
+    const float sOwn = CREASED ? (valid && ed < a.C ? a.crIn[ed].sharpness : 0.0f) : 0.0f;
+    float sOther = 0.0f;                                 // the other half of the parent edge (k = 1, 3)
+    if (CREASED && valid && (k & 1)) {
+        const int32_t eo = (k == 1 ? ped : ed) ^ 1;
+        sOther = eo < a.C ? a.crIn[eo].sharpness : 0.0f;
+    }
+    const float4 st = (valid && k == 0) ? a.ostats[vx] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    // the twin quad's two vertices other than vertex(h) and vertex(next h)
+    const int32_t kt = tw & 3;
+    f3 qa = zero3(), qc = zero3();
+    if (gatherTwin) {
+        const int32_t tb = tw & ~3;
+        const int32_t va = __ldg(a.in + (int64_t)RW * (tb + ((kt + 2) & 3)) + 2);
+        const int32_t vc = __ldg(a.in + (int64_t)RW * (tb + ((kt + 3) & 3)) + 2);
+        qa = ld3(a.pin + 3 * (int64_t)va);
+        qc = ld3(a.pin + 3 * (int64_t)vc);
+    }
+
+    // face point, and the next vertex's point from its shuffles
+    f3 pn;
+    const f3 Fp = quad_face_point_next(p, qb, k, pn);
+    if (valid && k == 0) st3(a.pout + 3 * ((int64_t)a.V + f), Fp);
+    const f3 Fsib = shfl3(Fp, (lane & ~15) | sibK);      // a sibling quad's face point
+    // edge point of h's edge, by both halves
+    f3 E = zero3();
+    if (valid) {
+        const float w = CREASED ? fsat(sOwn) : 0.0f;
+        const f3 sh_h = edge_share<CREASED>(p, pn, Fp, tw < 0, w);
+        if (tw >= 0) {
+            f3 Ft;
+            if (gatherTwin) {
+                // twin quad positions kt, kt+1, kt+2, kt+3 hold vertex(next h),
+                // vertex(h), qa, qc (the twin relation); sum in position order
+                f3 r0 = pn, r1 = p, r2 = qa, r3 = qc;         // r_i at position (kt + i) & 3
+                // rotate so that r_i sits at position i
+                if (kt & 1) { const f3 x = r3; r3 = r2; r2 = r1; r1 = r0; r0 = x; }
+                if (kt & 2) { f3 x = r0; r0 = r2; r2 = x; x = r1; r1 = r3; r3 = x; }
+                Ft = add3(add3(add3(add3(zero3(), quarter3(r0)), quarter3(r1)), quarter3(r2)), quarter3(r3));
+            } else {
+                Ft = Fsib;
+            }
+            const f3 sh_t = edge_share<CREASED>(pn, p, Ft, false, w);
+            E = h > tw ? add3(add3(zero3(), sh_t), sh_h) : add3(add3(zero3(), sh_h), sh_t);
+        } else {
+            E = add3(zero3(), sh_h);
+        }
+        if (h > tw) st3(a.pout + 3 * ((int64_t)a.V + a.F + ed), E);
+    }
+
+    // vertex share of h (tile_level_b, STRUCT)
+    const f3 Ep = shfl3(E, lp);
+    const float sPrev = __shfl_sync(full, sOwn, lp);
+    f3 s = zero3();
+    if (valid) {
+        float vpre, cpre = 0.0f, avgS = 0.0f;
+        bool bnd = false;
+        if (k == 2) {
+            vpre = 4.0f;
+        } else if (k != 0) {
+            bnd = (k == 1 ? ptw : tw) < 0;
+            vpre = bnd ? 2.0f : 4.0f;
+            if (CREASED) {
+                const float sa = k == 1 ? sPrev : sOwn;  // this side's half of the parent edge
+                const bool own = k == 3;                 // the walk from h skips its own edge
+                avgS = (bnd && own) ? sOther : fadd(sa, sOther);
+                cpre = (bnd && own) ? fsign(sOther) : fadd(fsign(sa), fsign(sOther));
+            }
+        } else {
+            bnd = st.w != 0.0f;
+            vpre = st.x;
+            if (CREASED) {
+                avgS = bnd ? fsub(st.y, sOwn) : st.y;
+                cpre = bnd ? fsub(st.z, fsign(sOwn)) : st.z;
+            }
+        }
+        s = quad_vertex_rule<CREASED>(p, Fp, E, Ep, vpre, cpre, avgS, bnd, CREASED ? fsign(sOwn) : 0.0f,
+                                      CREASED ? fsign(sPrev) : 0.0f);
+    }
+    {
+        float* o = a.pout + 3 * (int64_t)vx;
+        const f3 s4 = shfl_down3(s, 4), s8 = shfl_down3(s, 8), s12 = shfl_down3(s, 12);
+        const int partner = (lane & ~15) | ((((lane >> 2) + 1) & 3) << 2) | 3;
+        const f3 sA2 = shfl3(s, partner);
+        if (valid) {
+            if ((lane & 15) == 2) {
+                st3(o, add3(add3(add3(add3(zero3(), s), s4), s8), s12));
+            } else if (k == 1) {
+                atomic_add3(o, (lane & 12) == 12 ? add3(sA2, s) : add3(s, sA2));
+            } else if (k == 0) {
+                atomic_add3(o, s);
+            }
+        }
+    }
+
+    // clear this thread's share of the next level's accumulation slots
+    for (int64_t i = h64; i < a.zeroNextN; i += zeroStride) a.zeroNext[i] = 0.0f;
+
+    // child records through the shared tile and one bulk store
     if (TOPO) {
         const int lo = qb | ((k + 2) & 3);
         const int32_t prev = (h & ~3) | ((k + 3) & 3), next = (h & ~3) | ((k + 1) & 3);
@@ -512,94 +616,6 @@ __device__ __forceinline__ void tile_level_ab(const LevelArgs& a, int64_t h0, in
             const int64_t n = (a.H - h0) < BLOCK ? (a.H - h0) : BLOCK;
             bulk_store_tile(a.out + 4 * RW * h0, tile, (uint32_t)(n * 16 * RW));
         }
-    }
-    // clear this thread's share of the next level's accumulation slots
-    for (int64_t i = h64; i < a.zeroNextN; i += zeroStride) a.zeroNext[i] = 0.0f;
-
-    const f3 p = valid ? ld3(a.pin + 3 * (int64_t)vx) : zero3();
-    f3 pn;
-    const f3 Fp = quad_face_point_next(p, qb, k, pn);
-    if (valid && k == 0) st3(a.pout + 3 * ((int64_t)a.V + f), Fp);
-    const float sOwn = CREASED ? (valid && ed < a.C ? a.crIn[ed].sharpness : 0.0f) : 0.0f;
-    // the twin face of an edge inside the parent quad: a sibling quad's lanes
-    const int sib = (lane & ~15) | (k == 1 ? ((((j + 1) & 3) << 2) | 2) : ((((j + 3) & 3) << 2) | 1));
-    const f3 Fsib = shfl3(Fp, sib);
-    f3 E = zero3();
-    if (valid) {
-        const float w = CREASED ? fsat(sOwn) : 0.0f;
-        const f3 sh_h = edge_share<CREASED>(p, pn, Fp, tw < 0, w);
-        if (tw >= 0) {
-            const int32_t sibTw = k == 1 ? ((h & ~15) | ((((j + 1) & 3) << 2) | 2))
-                                         : ((h & ~15) | ((((j + 3) & 3) << 2) | 1));
-            f3 Ft;
-            if ((k == 1 || k == 2) && tw == sibTw) {
-                Ft = Fsib;
-            } else {
-                const int32_t tb = tw & ~3, kt = tw & 3;
-                f3 q[4];
-#pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    if (i == kt) q[i] = pn;
-                    else if (i == ((kt + 1) & 3)) q[i] = p;
-                    else q[i] = ld3(a.pin + 3 * (int64_t)__ldg(a.in + (int64_t)RW * (tb + i) + 2));
-                }
-                Ft = zero3();
-#pragma unroll
-                for (int i = 0; i < 4; ++i) Ft = add3(Ft, quarter3(q[i]));
-            }
-            const f3 sh_t = edge_share<CREASED>(pn, p, Ft, false, w);
-            E = h > tw ? add3(add3(zero3(), sh_t), sh_h) : add3(add3(zero3(), sh_h), sh_t);
-        } else {
-            E = add3(zero3(), sh_h);
-        }
-        if (h > tw) st3(a.pout + 3 * ((int64_t)a.V + a.F + ed), E);
-    }
-
-    // vertex share of h (tile_level_b, STRUCT)
-    const f3 Ep = shfl3(E, lp);
-    const float sPrev = __shfl_sync(full, sOwn, lp);
-    float4 st = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    if (valid && k == 0) st = a.ostats[vx];
-    f3 s = zero3();
-    if (valid) {
-        float vpre, cpre = 0.0f, avgS = 0.0f;
-        bool bnd = false;
-        if (k == 2) {
-            vpre = 4.0f;
-        } else if (k != 0) {
-            bnd = (k == 1 ? ptw : tw) < 0;
-            vpre = bnd ? 2.0f : 4.0f;
-            if (CREASED) {
-                const int32_t eh = k == 1 ? ped : ed;    // one half of the parent edge
-                const float sa = k == 1 ? sPrev : sOwn;
-                const int32_t eo = eh ^ 1;
-                const float sb = eo < a.C ? a.crIn[eo].sharpness : 0.0f;
-                const bool own = k == 3;                 // the walk from h skips its own edge
-                avgS = (bnd && own) ? sb : fadd(sa, sb);
-                cpre = (bnd && own) ? fsign(sb) : fadd(fsign(sa), fsign(sb));
-            }
-        } else {
-            bnd = st.w != 0.0f;
-            vpre = st.x;
-            if (CREASED) {
-                avgS = bnd ? fsub(st.y, sOwn) : st.y;
-                cpre = bnd ? fsub(st.z, fsign(sOwn)) : st.z;
-            }
-        }
-        s = quad_vertex_rule<CREASED>(p, Fp, E, Ep, vpre, cpre, avgS, bnd, CREASED ? fsign(sOwn) : 0.0f,
-                                      CREASED ? fsign(sPrev) : 0.0f);
-    }
-    float* o = a.pout + 3 * (int64_t)vx;
-    const f3 s4 = shfl_down3(s, 4), s8 = shfl_down3(s, 8), s12 = shfl_down3(s, 12);
-    const int partner = (lane & ~15) | ((((lane >> 2) + 1) & 3) << 2) | 3;
-    const f3 sA2 = shfl3(s, partner);
-    if (!valid) return;
-    if ((lane & 15) == 2) {
-        st3(o, add3(add3(add3(add3(zero3(), s), s4), s8), s12));
-    } else if (k == 1) {
-        atomic_add3(o, (lane & 12) == 12 ? add3(sA2, s) : add3(s, sA2));
-    } else if (k == 0) {
-        atomic_add3(o, s);
     }
 }
 
