@@ -80,6 +80,7 @@ SIGNATURES = {
     "ccs_CreateEx_cuda": ([_P, ctypes.c_int32, _U, ctypes.POINTER(_P)], _I),
     "ccs_Release_cuda": ([_P], None),
     "ccs_LoadCage_cuda": ([ctypes.c_char_p], _P),
+    "ccs_BuildCage_cuda": ([_P, _P, _P], _I),
     "ccs_ReleaseCage_cuda": ([_P], None),
     "ccs_SaveCage_cuda": ([_P, ctypes.c_char_p], _I),
     "ccs_Refine_Scatter_cuda": ([_P], _I),

@@ -27,6 +27,7 @@ per vertex), which is what every generator in this package produces.
 """
 from __future__ import annotations
 
+import ctypes
 from typing import Iterable, Sequence
 
 import numpy as np
@@ -206,3 +207,62 @@ def obj_text(points: np.ndarray, faces: Sequence[Sequence[int]],
     for a, b, s in crease_tags:
         out.append("t crease 2/1/0 %d %d %.9g" % (a, b, np.float32(s)))
     return "\n".join(out) + "\n"
+
+
+class _PolygonMesh(ctypes.Structure):
+    """ctypes mirror of ``ccs_PolygonMesh`` (include/ccs_cuda.h)."""
+    _fields_ = [("vertexCount", ctypes.c_int32), ("uvCount", ctypes.c_int32),
+                ("faceCount", ctypes.c_int32), ("creaseTagCount", ctypes.c_int32),
+                ("faceOffsets", ctypes.c_void_p), ("faceVertices", ctypes.c_void_p),
+                ("faceUvs", ctypes.c_void_p), ("vertexPoints", ctypes.c_void_p),
+                ("uvs", ctypes.c_void_p), ("creaseVertices", ctypes.c_void_p),
+                ("creaseSharpness", ctypes.c_void_p)]
+
+
+def build_cage_device(points: np.ndarray, faces: Sequence[Sequence[int]] | None = None,
+                      uvs: np.ndarray | None = None,
+                      face_uvs: Sequence[Sequence[int]] | None = None,
+                      crease_tags: Iterable[tuple[int, int, float]] = (),
+                      offsets: np.ndarray | None = None, corners: np.ndarray | None = None,
+                      corner_uvs: np.ndarray | None = None, stream=None) -> Cage:
+    """``build_cage`` on the GPU (``ccs_BuildCage_cuda``): the same cage, byte
+    for byte, with arrays in one page-locked block.
+
+    Faces come either as vertex lists (``faces``, ``face_uvs``) or flattened
+    (``offsets`` of length F + 1 and ``corners`` / ``corner_uvs``).  Raises
+    ``ValueError`` where the library refuses the input (a face with fewer than
+    3 corners or two consecutive corners on one vertex, an index out of
+    range, a directed edge used twice).
+    """
+    from . import _native as N
+    from .mesh import cage_of_block
+
+    points = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+    if offsets is None:
+        sizes = np.fromiter((len(f) for f in faces), np.int64, len(faces))
+        offsets = np.zeros(len(faces) + 1, np.int64)
+        np.cumsum(sizes, out=offsets[1:])
+        corners = np.fromiter((v for f in faces for v in f), np.int64, int(offsets[-1]))
+        if face_uvs is not None:
+            corner_uvs = np.fromiter((u for f in face_uvs for u in f), np.int64, int(offsets[-1]))
+    if int(offsets[-1]) >= 2**31:
+        raise ValueError("cage too large for int32 indices")
+    off = np.ascontiguousarray(offsets, np.int32)
+    fv = np.ascontiguousarray(corners, np.int32)
+    fu = None if corner_uvs is None else np.ascontiguousarray(corner_uvs, np.int32)
+    uv = None if uvs is None else np.ascontiguousarray(uvs, np.float32).reshape(-1, 2)
+    tags = list(crease_tags)
+    tv = np.ascontiguousarray([(int(a), int(b)) for a, b, _ in tags], np.int32).reshape(-1, 2)
+    ts = np.ascontiguousarray([s for _, _, s in tags], np.float32)
+    m = _PolygonMesh(points.shape[0], 0 if uv is None else uv.shape[0], off.shape[0] - 1, len(tags),
+                     off.ctypes.data, fv.ctypes.data, None if fu is None else fu.ctypes.data,
+                     points.ctypes.data, None if uv is None or uv.size == 0 else uv.ctypes.data,
+                     tv.ctypes.data if len(tags) else None, ts.ctypes.data if len(tags) else None)
+    out = ctypes.c_void_p()
+    handle = getattr(stream, "cuda_stream", stream)
+    code = N.lib().ccs_BuildCage_cuda(ctypes.byref(m), ctypes.byref(out),
+                                      ctypes.c_void_p(int(handle) if handle else 0))
+    if code == -1:
+        raise ValueError("ccs_BuildCage_cuda refused the polygon mesh")
+    N.check(code, "ccs_BuildCage_cuda")
+    return cage_of_block(out.value)

@@ -82,32 +82,15 @@ def load_pinned(path: str) -> Cage:
     host memory where the CUDA runtime cannot pin), so ``Subd`` uploads them
     by DMA with no staging copy.  The block is released with the cage.
     """
-    import ctypes
-    import weakref
-
     from . import _native as N
-    from .mesh import cc_Mesh
+    from .mesh import cage_of_block
 
     L = N.lib()
     ptr = L.ccs_LoadCage_cuda(path.encode())
     if not ptr:
         code = L.ccs_LastError_cuda()
         raise CcmError("cc: cannot load %s (%s)" % (path, L.ccs_ErrorString_cuda(code).decode()))
-    m = cc_Mesh.from_address(ptr)
-
-    def view(addr, dtype, n):
-        dtype = np.dtype(dtype)
-        if n == 0 or not addr:
-            return np.zeros(0, dtype)
-        return np.frombuffer((ctypes.c_char * (n * dtype.itemsize)).from_address(addr), dtype, n)
-
-    V, U, E, F, H = m.vertexCount, m.uvCount, m.edgeCount, m.faceCount, m.halfedgeCount
-    cage = Cage(view(m.vertexPoints, np.float32, 3 * V).reshape(-1, 3),
-                view(m.halfedges, HALFEDGE_DTYPE, H), view(m.creases, CREASE_DTYPE, E),
-                view(m.vertexToHalfedgeIDs, np.int32, V), view(m.edgeToHalfedgeIDs, np.int32, E),
-                view(m.faceToHalfedgeIDs, np.int32, F), view(m.uvs, np.float32, 2 * U).reshape(-1, 2))
-    weakref.finalize(cage, L.ccs_ReleaseCage_cuda, ptr)
-    return cage
+    return cage_of_block(ptr)
 
 
 def save_native(cage: Cage, path: str) -> None:

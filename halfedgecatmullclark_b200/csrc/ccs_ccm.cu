@@ -66,6 +66,56 @@ static void free_block(CageBlock* b) {
     else free(b);
 }
 
+// One block for a cage of these counts: the cc_Mesh with its counts set and
+// its array pointers into the block (uvs NULL when U = 0).
+cc_Mesh* alloc_cage_block(int32_t V, int32_t U, int32_t H, int32_t E, int32_t F) {
+    FileHeader h;
+    h.V = V; h.U = U; h.H = H; h.E = E; h.F = F;
+    int64_t sz[7];
+    array_bytes(h, sz);
+    int64_t total = up(sizeof(CageBlock)) + up(sizeof(cc_Mesh));
+    for (int i = 0; i < 7; ++i) total += up(sz[i]);
+    char* base = nullptr;
+    int pinned = 0;
+    if (cudaHostAlloc(reinterpret_cast<void**>(&base), (size_t)total, cudaHostAllocDefault) == cudaSuccess) {
+        pinned = 1;
+    } else {
+        cudaGetLastError();  // clear the failed call's status
+        base = static_cast<char*>(malloc((size_t)total));
+    }
+    if (!base) return nullptr;
+    CageBlock* b = reinterpret_cast<CageBlock*>(base);
+    b->magic = kBlockMagic;
+    b->pinned = pinned;
+    b->pad = 0;
+    b->bytes = total;
+    cc_Mesh* m = reinterpret_cast<cc_Mesh*>(base + up(sizeof(CageBlock)));
+    char* p = reinterpret_cast<char*>(m) + up(sizeof(cc_Mesh));
+    char* arr[7];
+    for (int i = 0; i < 7; ++i) {
+        arr[i] = p;
+        p += up(sz[i]);
+    }
+    m->vertexCount = V;
+    m->uvCount = U;
+    m->halfedgeCount = H;
+    m->edgeCount = E;
+    m->faceCount = F;
+    m->vertexToHalfedgeIDs = reinterpret_cast<int32_t*>(arr[0]);
+    m->edgeToHalfedgeIDs = reinterpret_cast<int32_t*>(arr[1]);
+    m->faceToHalfedgeIDs = reinterpret_cast<int32_t*>(arr[2]);
+    m->vertexPoints = reinterpret_cast<cc_VertexPoint*>(arr[3]);
+    m->uvs = U > 0 ? reinterpret_cast<cc_VertexUv*>(arr[4]) : nullptr;
+    m->creases = reinterpret_cast<cc_Crease*>(arr[5]);
+    m->halfedges = reinterpret_cast<cc_Halfedge*>(arr[6]);
+    return m;
+}
+
+void free_cage_block(cc_Mesh* m) {
+    CageBlock* b = block_of(m);
+    if (b) free_block(b);
+}
+
 }  // namespace ccs
 
 using namespace ccs;
@@ -83,61 +133,30 @@ cc_Mesh* ccs_LoadCage_cuda(const char* path) {
         fclose(f);
         return nullptr;
     }
-    int64_t sz[7];
-    array_bytes(h, sz);
-    int64_t total = up(sizeof(CageBlock)) + up(sizeof(cc_Mesh));
-    for (int i = 0; i < 7; ++i) total += up(sz[i]);
-    char* base = nullptr;
-    int pinned = 0;
-    if (cudaHostAlloc(reinterpret_cast<void**>(&base), (size_t)total, cudaHostAllocDefault) == cudaSuccess) {
-        pinned = 1;
-    } else {
-        cudaGetLastError();  // clear the failed call's status
-        base = static_cast<char*>(malloc((size_t)total));
-    }
-    if (!base) {
+    cc_Mesh* m = alloc_cage_block(h.V, h.U, h.H, h.E, h.F);
+    if (!m) {
         fclose(f);
         set_last_error(CCS_ERR_ALLOC);
         return nullptr;
     }
-    CageBlock* b = reinterpret_cast<CageBlock*>(base);
-    b->magic = kBlockMagic;
-    b->pinned = pinned;
-    b->pad = 0;
-    b->bytes = total;
-    cc_Mesh* m = reinterpret_cast<cc_Mesh*>(base + up(sizeof(CageBlock)));
-    char* p = reinterpret_cast<char*>(m) + up(sizeof(cc_Mesh));
-    char* arr[7];
+    // file order: v2h, e2h, f2h, points, uvs, creases, halfedges
+    void* dst[7] = {m->vertexToHalfedgeIDs, m->edgeToHalfedgeIDs, m->faceToHalfedgeIDs, m->vertexPoints,
+                    m->uvs, m->creases, m->halfedges};
+    int64_t sz[7];
+    array_bytes(h, sz);
     for (int i = 0; i < 7; ++i) {
-        arr[i] = p;
-        if (sz[i] > 0 && fread(p, 1, (size_t)sz[i], f) != (size_t)sz[i]) {
+        if (sz[i] > 0 && fread(dst[i], 1, (size_t)sz[i], f) != (size_t)sz[i]) {
             fclose(f);
-            free_block(b);
+            free_cage_block(m);
             return nullptr;
         }
-        p += up(sz[i]);
     }
     fclose(f);
-    m->vertexCount = h.V;
-    m->uvCount = h.U;
-    m->halfedgeCount = h.H;
-    m->edgeCount = h.E;
-    m->faceCount = h.F;
-    m->vertexToHalfedgeIDs = reinterpret_cast<int32_t*>(arr[0]);
-    m->edgeToHalfedgeIDs = reinterpret_cast<int32_t*>(arr[1]);
-    m->faceToHalfedgeIDs = reinterpret_cast<int32_t*>(arr[2]);
-    m->vertexPoints = reinterpret_cast<cc_VertexPoint*>(arr[3]);
-    m->uvs = h.U > 0 ? reinterpret_cast<cc_VertexUv*>(arr[4]) : nullptr;
-    m->creases = reinterpret_cast<cc_Crease*>(arr[5]);
-    m->halfedges = reinterpret_cast<cc_Halfedge*>(arr[6]);
     set_last_error(CCS_OK);
     return m;
 }
 
-void ccs_ReleaseCage_cuda(cc_Mesh* cage) {
-    CageBlock* b = block_of(cage);
-    if (b) free_block(b);
-}
+void ccs_ReleaseCage_cuda(cc_Mesh* cage) { free_cage_block(cage); }
 
 int ccs_SaveCage_cuda(const cc_Mesh* m, const char* path) {
     if (!m || !path || m->vertexCount < 0 || m->uvCount < 0 || m->halfedgeCount < 0 || m->edgeCount < 0 ||

@@ -70,6 +70,11 @@ struct Ctx {
     bool fusable = true;         // the twin relation vertex(twin h) = vertex(next h) holds
 };
 
+// A cage and all its arrays in one page-locked (else malloc'd) host block
+// (ccs_ccm.cu); NULL when out of memory.  free_cage_block takes such a cage.
+cc_Mesh* alloc_cage_block(int32_t V, int32_t U, int32_t H, int32_t E, int32_t F);
+void free_cage_block(cc_Mesh* m);
+
 // Records `s` as the calling thread's ccs_LastError_cuda() status; returns s.
 int set_last_error(int s);
 

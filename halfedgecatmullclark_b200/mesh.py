@@ -151,3 +151,27 @@ class Cage:
         return Cage(pts, arr(m.halfedges, H, HALFEDGE_DTYPE), arr(m.creases, E, CREASE_DTYPE),
                     arr(m.vertexToHalfedgeIDs, V, np.int32), arr(m.edgeToHalfedgeIDs, E, np.int32),
                     arr(m.faceToHalfedgeIDs, F, np.int32), uvs)
+
+
+def cage_of_block(ptr: int) -> "Cage":
+    """A ``Cage`` whose arrays are views of a single-block ``cc_Mesh`` made by
+    the C library (``ccs_LoadCage_cuda``, ``ccs_BuildCage_cuda``); the block
+    is released (``ccs_ReleaseCage_cuda``) with the cage."""
+    import weakref
+
+    from . import _native as N
+    m = cc_Mesh.from_address(ptr)
+
+    def view(addr, dtype, n):
+        dtype = np.dtype(dtype)
+        if n == 0 or not addr:
+            return np.zeros(0, dtype)
+        return np.frombuffer((ctypes.c_char * (n * dtype.itemsize)).from_address(addr), dtype, n)
+
+    V, U, E, F, H = m.vertexCount, m.uvCount, m.edgeCount, m.faceCount, m.halfedgeCount
+    cage = Cage(view(m.vertexPoints, np.float32, 3 * V).reshape(-1, 3),
+                view(m.halfedges, HALFEDGE_DTYPE, H), view(m.creases, CREASE_DTYPE, E),
+                view(m.vertexToHalfedgeIDs, np.int32, V), view(m.edgeToHalfedgeIDs, np.int32, E),
+                view(m.faceToHalfedgeIDs, np.int32, F), view(m.uvs, np.float32, 2 * U).reshape(-1, 2))
+    weakref.finalize(cage, N.lib().ccs_ReleaseCage_cuda, ptr)
+    return cage

@@ -132,6 +132,33 @@ cc_Mesh *ccs_LoadCage_cuda(const char *path);
 void ccs_ReleaseCage_cuda(cc_Mesh *cage);
 int ccs_SaveCage_cuda(const cc_Mesh *cage, const char *path);
 
+/* A polygon mesh: what the reference's OBJ converter reads (examples/
+ * obj_to_ccm.c LoadObj :666-752), as arrays.  Face f's corners are
+ * faceOffsets[f] .. faceOffsets[f + 1] - 1 (faceOffsets[0] = 0) of
+ * faceVertices (0-based vertex IDs) and of faceUvs (0-based texture IDs, or
+ * NULL: every uvID 0, as LoadObj for faces without `vt`).  creaseVertices
+ * holds creaseTagCount pairs (v0, v1) with creaseSharpness[t]: the
+ * `t crease 2/1/0 v0 v1 s` tags.  Arrays may be host or device memory. */
+typedef struct {
+    int32_t vertexCount, uvCount, faceCount, creaseTagCount;
+    const int32_t *faceOffsets;
+    const int32_t *faceVertices;
+    const int32_t *faceUvs;
+    const float *vertexPoints;   /* vertexCount x 3 */
+    const float *uvs;            /* uvCount x 2 */
+    const int32_t *creaseVertices;
+    const float *creaseSharpness;
+} ccs_PolygonMesh;
+
+/* Builds the halfedge cage of `mesh` on the GPU -- twins, edge, vertex and
+ * face maps, creases, boundary sharpness 16 and crease chains, numbered as
+ * LoadObj numbers them (obj_to_ccm.c:88-450, :538-561) -- into one
+ * page-locked block like ccs_LoadCage_cuda's (release it with
+ * ccs_ReleaseCage_cuda).  CCS_ERR_ARG for a face with fewer than 3 corners
+ * or two consecutive corners on one vertex, an index out of range, or a
+ * directed edge used twice.  Waits for the GPU before returning. */
+int ccs_BuildCage_cuda(const ccs_PolygonMesh *mesh, cc_Mesh **out, void *stream);
+
 /* ---------------------------------------------------------------------- */
 /* Refinement (CatmullClark.h:197-212)                                     */
 /* ---------------------------------------------------------------------- */

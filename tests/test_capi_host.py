@@ -113,6 +113,14 @@ def test_create_without_gpu_reports_cuda_error(lib):
     assert not out.value
 
 
+def test_build_cage_without_gpu_reports_an_error(lib):
+    if gpu_available():
+        pytest.skip("a GPU is present")
+    from halfedgecatmullclark_b200.cage import build_cage_device
+    with pytest.raises(Exception):
+        build_cage_device(np.zeros((4, 3), np.float32), [[0, 1, 2, 3]])
+
+
 def test_level_counts_api(lib):
     from halfedgecatmullclark_b200 import _native as N
     from halfedgecatmullclark_b200 import configs
