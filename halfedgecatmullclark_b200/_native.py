@@ -105,6 +105,7 @@ SIGNATURES = {
     "ccs_RefinePointsDevice_cuda": ([_P, _P, _P, _I, _P], _I),
     "ccs_AdjointPointsDevice_cuda": ([_P, _P, _P, _P], _I),
     "ccs_HalfedgeNormals_cuda": ([_P, _P, _P, ctypes.c_int, _P], _I),
+    "ccs_ExportObj_cuda": ([_P, ctypes.c_int32, ctypes.c_char_p], _I),
     "ccs_AdjointPointsDeviceNoAlloc_cuda": ([_P, _P, _P, _P], _I),
     "ccs_BatchCreate_cuda": ([_P, _P, ctypes.c_int32, _U, ctypes.POINTER(_P)], _I),
     "ccs_BatchRelease_cuda": ([_P], None),

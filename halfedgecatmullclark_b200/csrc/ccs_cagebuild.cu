@@ -28,6 +28,7 @@
 
 #include "ccs_host.h"
 #include "ccs_internal.cuh"
+#include "ccs_scan.cuh"
 
 namespace ccs {
 namespace {
@@ -36,89 +37,6 @@ constexpr int kB = 256;
 enum : int { BE_FACE = 1, BE_VERTEX = 2, BE_UV = 4, BE_DUP = 8 };
 
 inline unsigned nblk(int64_t n, int per = kB) { return (unsigned)((n + per - 1) / per); }
-
-// ---------------------------------------------------------------------------
-// exclusive scan of int32 counts (sums below 2^31)
-// ---------------------------------------------------------------------------
-constexpr int kScanItems = 4;                       // per thread
-constexpr int kScanTile = kB * kScanItems;          // per block
-
-__device__ __forceinline__ int32_t block_exclusive(int32_t x, int32_t* warpSums, int32_t& total) {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    int32_t incl = x;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const int32_t y = __shfl_up_sync(0xffffffffu, incl, d);
-        if (lane >= d) incl += y;
-    }
-    if (lane == 31) warpSums[w] = incl;
-    __syncthreads();
-    if (w == 0) {
-        int32_t s = lane < kB / 32 ? warpSums[lane] : 0;
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const int32_t y = __shfl_up_sync(0xffffffffu, s, d);
-            if (lane >= d) s += y;
-        }
-        if (lane < kB / 32) warpSums[lane] = s;     // inclusive over warps
-    }
-    __syncthreads();
-    total = warpSums[kB / 32 - 1];
-    const int32_t before = w > 0 ? warpSums[w - 1] : 0;
-    __syncthreads();
-    return before + incl - x;
-}
-
-__global__ void __launch_bounds__(kB) k_scan_tiles(const int32_t* __restrict__ in, int32_t* __restrict__ out,
-                                                   int32_t* __restrict__ tileSums, int64_t n) {
-    __shared__ int32_t warpSums[kB / 32];
-    const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
-    int32_t v[kScanItems], sum = 0;
-#pragma unroll
-    for (int i = 0; i < kScanItems; ++i) {
-        v[i] = base + i < n ? in[base + i] : 0;
-        sum += v[i];
-    }
-    int32_t total;
-    int32_t run = block_exclusive(sum, warpSums, total);
-#pragma unroll
-    for (int i = 0; i < kScanItems; ++i) {
-        if (base + i < n) out[base + i] = run;
-        run += v[i];
-    }
-    if (threadIdx.x == 0) tileSums[blockIdx.x] = total;
-}
-
-// one block: exclusive scan of the tile sums in place, grand total to *total
-__global__ void __launch_bounds__(kB) k_scan_sums(int32_t* __restrict__ sums, int64_t nt, int32_t* __restrict__ total) {
-    __shared__ int32_t warpSums[kB / 32];
-    int32_t carry = 0;
-    for (int64_t c = 0; c < nt; c += kB) {
-        const int64_t i = c + threadIdx.x;
-        const int32_t x = i < nt ? sums[i] : 0;
-        int32_t chunk;
-        const int32_t ex = block_exclusive(x, warpSums, chunk);
-        if (i < nt) sums[i] = carry + ex;
-        carry += chunk;
-    }
-    if (threadIdx.x == 0) *total = carry;
-}
-
-__global__ void __launch_bounds__(kB) k_scan_add(int32_t* __restrict__ out, const int32_t* __restrict__ tileSums,
-                                                 int64_t n) {
-    const int64_t i = (int64_t)blockIdx.x * kB + threadIdx.x;
-    if (i < n) out[i] += tileSums[i / kScanTile];
-}
-
-// out[0..n) = exclusive scan of in[0..n); *total = sum (device)
-cudaError_t exclusive_scan(const int32_t* in, int32_t* out, int64_t n, int32_t* scratch, int32_t* total,
-                           cudaStream_t s) {
-    const int64_t nt = (n + kScanTile - 1) / kScanTile;
-    if (nt > 0) k_scan_tiles<<<(unsigned)nt, kB, 0, s>>>(in, out, scratch, n);
-    k_scan_sums<<<1, kB, 0, s>>>(scratch, nt, total);
-    if (n > 0) k_scan_add<<<nblk(n), kB, 0, s>>>(out, scratch, n);
-    return cudaGetLastError();
-}
 
 // ---------------------------------------------------------------------------
 // build kernels; `he` is the cc_Halfedge array as CH_WORDS int32 per record
@@ -314,7 +232,7 @@ int build(const ccs_PolygonMesh* m, cc_Mesh** out, cudaStream_t s) {
         return CCS_ERR_CUDA;
     if (H < 3 * (int64_t)F) return CCS_ERR_ARG;
 
-    const int64_t nTiles = (H > V ? H : V) / kScanTile + 2;
+    const int64_t nTiles = scan_tiles(H > V ? H : V);
     const size_t i4 = sizeof(int32_t);
     Arena sc;
     if (!sc.reserve(Arena::sz(i4 * H) * (m->faceUvs ? 9 : 8) + Arena::sz(i4 * CH_WORDS * (size_t)H) +
@@ -364,12 +282,12 @@ int build(const ccs_PolygonMesh* m, cc_Mesh** out, cudaStream_t s) {
     if (hostErr) return CCS_ERR_ARG;      // every record is written and every index in range past here
 
     // vertex buckets of outgoing halfedges: start[v] .. start[v + 1]
-    if (exclusive_scan(count, start, (int64_t)V + 1, tiles, total, s) != cudaSuccess) return CCS_ERR_CUDA;
+    if (exclusive_scan<int32_t>(count, start, (int64_t)V + 1, tiles, total, s) != cudaSuccess) return CCS_ERR_CUDA;
     k_bucket_fill<<<nblk(H), kB, 0, s>>>(he, H, start, cursor, bucket);
     k_twins<<<nblk(H), kB, 0, s>>>(he, H, start, bucket, err);
     // edges
     k_edge_bits<<<nblk(H), kB, 0, s>>>(he, H, bits);
-    if (exclusive_scan(bits, pre, H, tiles, total + 1, s) != cudaSuccess) return CCS_ERR_CUDA;
+    if (exclusive_scan<int32_t>(bits, pre, H, tiles, total + 1, s) != cudaSuccess) return CCS_ERR_CUDA;
     k_edges<<<nblk(H), kB, 0, s>>>(he, H, pre, e2h);
     k_v2h_max<<<nblk(H), kB, 0, s>>>(he, H, v2h);
     k_v2h_boundary<<<nblk(H), kB, 0, s>>>(he, H, v2h);

@@ -440,6 +440,15 @@ int adjoint_into(const cc_Subd* subd, const float* gradPoints, float* gradCage, 
 
 int set_last_error(int status) { return ret(status); }
 
+bool subd_view(const cc_Subd* subd, SubdView* v) {
+    SubdImpl* s = find(subd);
+    if (!s || !v) return false;
+    v->cage = &s->dc; v->D = s->D; v->rw = s->rw; v->lv = s->lv.data();
+    v->he = s->he; v->pts = s->pts; v->stream = s->stream; v->device = s->device;
+    v->topo = s->topo_ready;
+    return true;
+}
+
 // Used by the batched path (ccs_batch.cu).
 int level_counts_ex(const cc_Mesh* cage, int32_t D, std::vector<Level>* out) { return level_counts(cage, D, out); }
 int validate_cage_ex(const cc_Mesh* m) { return validate_cage(m); }

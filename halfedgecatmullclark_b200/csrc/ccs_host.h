@@ -75,6 +75,19 @@ struct Ctx {
 cc_Mesh* alloc_cage_block(int32_t V, int32_t U, int32_t H, int32_t E, int32_t F);
 void free_cage_block(cc_Mesh* m);
 
+// Read-only view of a subd for the exporters (ccs_export.cu).
+struct SubdView {
+    const DevCage* cage;
+    int32_t D, rw;
+    const Level* lv;             // D + 1 entries
+    const int32_t* he;           // refined halfedges (all levels)
+    const float* pts;            // refined points (all levels)
+    cudaStream_t stream;
+    int device;
+    bool topo;                   // topology refined
+};
+bool subd_view(const cc_Subd* subd, SubdView* out);
+
 // Records `s` as the calling thread's ccs_LastError_cuda() status; returns s.
 int set_last_error(int s);
 

@@ -180,6 +180,13 @@ class Subd:
                 "ccs_HalfedgeNormals_cuda")
         return out
 
+    def export_obj(self, path: str, depth: int | None = None) -> None:
+        """Write one depth (default: the finest; 0 = the cage) as an OBJ file,
+        formatted on the GPU (ccs_ExportObj_cuda; ExportToObj of
+        examples/subd_cpu.c:22-115, byte for byte)."""
+        d = self.depth if depth is None else int(depth)
+        N.check(self.L.ccs_ExportObj_cuda(self.ptr, d, path.encode()), "ccs_ExportObj_cuda")
+
     def level_slice(self, level: int, what: str = "V") -> slice:
         """Rows of depth `level` (1..depth) inside the packed arrays."""
         lv = self.levels[level]

@@ -264,6 +264,15 @@ int ccs_AdjointPointsDeviceNoAlloc_cuda(cc_Subd *subd, const float *gradPoints, 
  * writes them, or NULL for the subd's own.  Needs the topology refined. */
 int ccs_HalfedgeNormals_cuda(cc_Subd *subd, const float *points, float *normals, int smooth, void *stream);
 
+/* Writes depth `depth` (0 = the cage) of a subd as an OBJ file with the bytes
+ * of the reference's ExportToObj (examples/subd_cpu.c:22-115), formatted on
+ * the GPU from the device arrays (no ccs_Download_cuda needed): "v" lines,
+ * "vt" lines (per halfedge at depth >= 1; none with 12-byte records, as the
+ * CC_DISABLE_UV build), "f" lines.  Waits for the subd's stream.  With
+ * 16-byte records and a cage without UVs the reference prints uninitialised
+ * uvIDs; here they are 0. */
+int ccs_ExportObj_cuda(const cc_Subd *subd, int32_t depth, const char *path);
+
 /* ---------------------------------------------------------------------- */
 /* Batched refinement (no reference counterpart).                          */
 /*                                                                         */

@@ -216,3 +216,54 @@ def halfedge_normals(he_level, pts_level, smooth: bool = True):
     out = fast.copy()
     out[closed] = unit(fast[closed] + acc[closed])
     return out
+
+
+def export_obj_text(cage, depth: int, halfedges=None, points=None, uv: bool = True) -> bytes:
+    """The bytes of ExportToObj (examples/subd_cpu.c:22-115) for one depth.
+
+    Depth 0 prints the cage; depth >= 1 the level's rows of the packed
+    `halfedges` (twin, edge, vertex[, uv]) and `points`.  Floats print as C's
+    "%f" (exact value rounded to 6 decimals, ties to even: Python's "%f" on
+    the float64 value of the float32 agrees); texture coordinates at depth
+    >= 1 decode the uvID as (x & 0xFFFF) / 65535.0f in float32 (:374-383).
+    """
+    out = ["# Vertices\n"]
+    f6 = lambda x: "%f" % float(x)
+    if depth == 0:
+        for p in np.asarray(cage.vertex_points, np.float32):
+            out.append("v %s %s %s\n" % (f6(p[0]), f6(p[1]), f6(p[2])))
+        for t in np.asarray(cage.uvs, np.float32).reshape(-1, 2):
+            out.append("vt %s %s\n" % (f6(t[0]), f6(t[1])))
+        out.append("\n# Topology\n")
+        he = cage.halfedges
+        for f in range(cage.F):
+            h0 = int(cage.f2h[f])
+            corners = [h0]
+            h = int(he["nextID"][h0])
+            while h != h0:
+                corners.append(h)
+                h = int(he["nextID"][h])
+            out.append("f " + " ".join("%d/%d" % (he["vertexID"][c] + 1, he["uvID"][c] + 1) for c in corners) + "\n")
+        return "".join(out).encode()
+    hs = level_slice(cage, depth, depth, "H")
+    vs = level_slice(cage, depth, depth, "V")
+    rec = np.asarray(halfedges)[hs]
+    P = np.asarray(points, np.float32)[vs]
+    for p in P:
+        out.append("v %s %s %s\n" % (f6(p[0]), f6(p[1]), f6(p[2])))
+    if uv:
+        x = rec[:, 3].astype(np.int64) & 0xFFFFFFFF
+        u = (x & 0xFFFF).astype(np.float32) / np.float32(65535.0)
+        v = ((x >> 16) & 0xFFFF).astype(np.float32) / np.float32(65535.0)
+        for a, b in zip(u, v):
+            out.append("vt %s %s\n" % (f6(a), f6(b)))
+    out.append("\n# Topology\n")
+    vert = rec[:, 2] + 1
+    for f in range(rec.shape[0] // 4):
+        if uv:
+            out.append("f %d/%d %d/%d %d/%d %d/%d\n" % (vert[4 * f], 4 * f + 1, vert[4 * f + 1], 4 * f + 2,
+                                                       vert[4 * f + 2], 4 * f + 3, vert[4 * f + 3], 4 * f + 4))
+        else:
+            out.append("f %d %d %d %d\n" % tuple(vert[4 * f:4 * f + 4]))
+    out.append("\n")
+    return "".join(out).encode()

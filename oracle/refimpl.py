@@ -242,3 +242,26 @@ def refine(cage, depth: int, mode: str = "scatter", fp64: bool = False):
         return s.halfedges(), s.creases(), s.points()
     finally:
         s.close()
+
+
+EXPORT_SO = os.path.join(HERE, "_ref", "libccexport.so")
+EXPORT_NOUV_SO = os.path.join(HERE, "_ref", "libccexport_nouv.so")
+
+
+def export_available() -> bool:
+    return os.path.exists(EXPORT_SO) and os.path.exists(EXPORT_NOUV_SO)
+
+
+def export_obj(cage, depth: int, max_depth: int, halfedges, points, path: str, uv: bool = True) -> None:
+    """The reference's ExportToObj (examples/subd_cpu.c:22-115) on a subd
+    whose packed arrays are `halfedges` (16-byte records with `uv`, else 12)
+    and `points`, over `cage` (a halfedgecatmullclark_b200 Cage)."""
+    so = EXPORT_SO if uv else EXPORT_NOUV_SO
+    L = ctypes.CDLL(so)
+    L.ccref_export_obj.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_char_p]
+    L.ccref_export_obj.restype = None
+    m = cage.as_cc_mesh()
+    he = np.ascontiguousarray(halfedges, np.int32)
+    pts = np.ascontiguousarray(points, np.float32)
+    s = cc_Subd(ctypes.addressof(m), pts.ctypes.data, he.ctypes.data, None, max_depth)
+    L.ccref_export_obj(ctypes.byref(s), depth, path.encode())
