@@ -428,6 +428,11 @@ def run_batch_workload(args):
         b.record(stream)
     bt.synchronize()
     batch_ms = shard.max_over_ranks(a.elapsed_time(b) / steps, world)
+    # gradients of the last full step (the adjoint consumes its input, so
+    # before the halves are timed alone)
+    agree = max(float((arr["grad_cage_points"][bt.cage_slice(i)] - ref).abs().max() /
+                      max(ref.abs().max(), 1e-30))
+                for i, ref in zip((0, len(ws) // 2, len(ws) - 1), loop_sample))
     # the two halves alone (same stream, CUDA events)
     parts = {}
     for name, fn in (("forward_ms", bt.refine_points), ("adjoint_ms", bt.adjoint)):
@@ -438,9 +443,6 @@ def run_batch_workload(args):
             b.record(stream)
         bt.synchronize()
         parts[name] = shard.max_over_ranks(a.elapsed_time(b) / steps, world)
-    agree = max(float((arr["grad_cage_points"][bt.cage_slice(i)] - ref).abs().max() /
-                      max(ref.abs().max(), 1e-30))
-                for i, ref in zip((0, len(ws) // 2, len(ws) - 1), loop_sample))
     agree = shard.max_over_ranks(agree, world)
     sh = int(shard.sum_over_ranks(sum(inf["halfedgeCount"] for inf in bt.info), world))
     topo_ms = shard.max_over_ranks(topo_ms, world)
