@@ -96,6 +96,19 @@ __device__ __forceinline__ f3 edge_share(f3 v0, f3 v1, f3 F, bool boundary, floa
     return lerp3(mul3(F, 0.5f), lerp3(mul3(v0, wh), mul3(v1, wh), 0.5f), wh);
 }
 
+// edge_share with a shortcut for an uncreased edge of the creased rule: with
+// w = 0 the rule's lerp(smoothP, sharpP, 0) = smoothP + 0 * (sharpP - smoothP)
+// is smoothP bit for bit unless a coordinate of smoothP is a zero (the sign
+// of a zero sum can differ), which takes the full rule.
+template <bool CREASED>
+__device__ __forceinline__ f3 edge_share_fast(f3 v0, f3 v1, f3 F, bool boundary, float w) {
+    if (CREASED && w == 0.0f) {
+        const f3 sm = mul3(lerp3(v0, F, 0.5f), 0.5f);
+        if (sm.x != 0.0f && sm.y != 0.0f && sm.z != 0.0f) return sm;
+    }
+    return edge_share<CREASED>(v0, v1, F, boundary, w);
+}
+
 // ---------------------------------------------------------------------------
 // creases (CatmullClark.h:2950-2983, :2992-3026): item = parent crease
 // ---------------------------------------------------------------------------
@@ -520,7 +533,7 @@ __device__ __forceinline__ void tile_level_ab(const LevelArgs& a, int64_t h0, in
     f3 E = zero3();
     if (valid) {
         const float w = CREASED ? fsat(sOwn) : 0.0f;
-        const f3 sh_h = edge_share<CREASED>(p, pn, Fp, tw < 0, w);
+        const f3 sh_h = edge_share_fast<CREASED>(p, pn, Fp, tw < 0, w);
         if (tw >= 0) {
             f3 Ft;
             if (gatherTwin) {
@@ -534,7 +547,7 @@ __device__ __forceinline__ void tile_level_ab(const LevelArgs& a, int64_t h0, in
             } else {
                 Ft = Fsib;
             }
-            const f3 sh_t = edge_share<CREASED>(pn, p, Ft, false, w);
+            const f3 sh_t = edge_share_fast<CREASED>(pn, p, Ft, false, w);
             E = h > tw ? add3(add3(zero3(), sh_t), sh_h) : add3(add3(zero3(), sh_h), sh_t);
         } else {
             E = add3(zero3(), sh_h);
