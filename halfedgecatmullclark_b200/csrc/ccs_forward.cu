@@ -141,6 +141,16 @@ k_face_points(View L, const float* __restrict__ pin, float* __restrict__ pout) {
     if (i < L.F) face_point_item<View, GATHER_SEM>(L, pin, pout, (int32_t)i);
 }
 
+// face points and the cleared vertex slots of the atomic pass in one launch
+// (grid over max(F, V); the two write disjoint ranges of pout)
+template <class View>
+__global__ void __launch_bounds__(kBlock)
+k_face_points_clear(View L, const float* __restrict__ pin, float* __restrict__ pout) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < L.F) face_point_item<View, false>(L, pin, pout, (int32_t)i);
+    if (i < L.V) st3(pout + 3 * i, zero3());
+}
+
 template <class View, bool CREASED>
 __global__ void __launch_bounds__(kBlock)
 k_edge_owner(View L, const float* __restrict__ pin, float* __restrict__ pout) {
@@ -380,22 +390,44 @@ static void points_level(const Ctx& c, const View& L, const float* pin, float* p
     }
 }
 
-// The cage step of the fused pipeline: topology (+UV) and creases of depth 1,
-// then the cage's face, edge and vertex points.
-cudaError_t run_cage_step(const Ctx& c, bool topo, bool uv, const float* cagePts, float* pout, int mode, bool det) {
+// The cage step of the fused pipeline: topology (+UV) and creases of depth 1
+// on `topoStream` (the points do not read them), and the cage's face, edge
+// and vertex points on the subd's stream -- for the atomic scatter, face
+// points and the cleared vertex slots in one launch.
+cudaError_t run_cage_step(const Ctx& c, bool topo, bool uv, const float* cagePts, float* pout, int mode, bool det,
+                          cudaStream_t topoStream) {
     if (topo) {
+        Ctx ct = c;
+        ct.stream = topoStream ? topoStream : c.stream;
         if (c.rw == 4) {
-            if (uv) launch_topology_level<4, true, true>(c, 0);
-            else launch_topology_level<4, true, false>(c, 0);
+            if (uv) launch_topology_level<4, true, true>(ct, 0);
+            else launch_topology_level<4, true, false>(ct, 0);
         } else {
-            launch_topology_level<3, true, false>(c, 0);
+            launch_topology_level<3, true, false>(ct, 0);
         }
         const int32_t C = c.lv[0].C;
-        c.prof->begin(c.stream, CCS_K_CREASES, 0, C);
-        k_creases<<<nblocks(C), kBlock, 0, c.stream>>>(c.cage->cr, c.cr + c.lv[1].crOff, C);
-        c.prof->end(c.stream);
+        c.prof->begin(ct.stream, CCS_K_CREASES, 0, C);
+        k_creases<<<nblocks(C), kBlock, 0, ct.stream>>>(c.cage->cr, c.cr + c.lv[1].crOff, C);
+        c.prof->end(ct.stream);
     }
-    points_level(c, cage_view(c), cagePts, pout, mode, det);
+    const bool atomic = !det && (mode == CCS_POINTS_SCATTER || mode == CCS_POINTS_NOCREASES_SCATTER);
+    if (!atomic) {
+        points_level(c, cage_view(c), cagePts, pout, mode, det);
+        return cudaGetLastError();
+    }
+    const CageView L = cage_view(c);
+    const bool creased = mode == CCS_POINTS_SCATTER;
+    c.prof->begin(c.stream, CCS_K_FACE_POINTS, 0, L.H);
+    k_face_points_clear<CageView><<<nblocks(L.F > L.V ? L.F : L.V), kBlock, 0, c.stream>>>(L, cagePts, pout);
+    c.prof->end(c.stream);
+    c.prof->begin(c.stream, CCS_K_EDGE_POINTS, 0, L.H);
+    if (creased) k_edge_owner<CageView, true><<<nblocks(L.H), kBlock, 0, c.stream>>>(L, cagePts, pout);
+    else k_edge_owner<CageView, false><<<nblocks(L.H), kBlock, 0, c.stream>>>(L, cagePts, pout);
+    c.prof->end(c.stream);
+    c.prof->begin(c.stream, CCS_K_VERTEX_POINTS, 0, L.H);
+    if (creased) k_vertex_atomic<CageView, true><<<nblocks(L.H), kBlock, 0, c.stream>>>(L, cagePts, pout);
+    else k_vertex_atomic<CageView, false><<<nblocks(L.H), kBlock, 0, c.stream>>>(L, cagePts, pout);
+    c.prof->end(c.stream);
     return cudaGetLastError();
 }
 

@@ -303,7 +303,8 @@ static void level_b_exact(const Ctx& c, int d, const float* pin, float* pout) {
 // Declared in ccs_forward.cu: the one-thread-per-vertex sorted pass of one
 // quad level, and the cage step.
 cudaError_t run_vertex_det_level(const Ctx& c, int d, const float* pin, float* pout, bool creased);
-cudaError_t run_cage_step(const Ctx& c, bool topo, bool uv, const float* cagePts, float* pout, int mode, bool det);
+cudaError_t run_cage_step(const Ctx& c, bool topo, bool uv, const float* cagePts, float* pout, int mode, bool det,
+                          cudaStream_t topoStream);
 
 // With the topology, the older vertices' ring statistics of every level are
 // built on the way (read by the default pass and by the adjoint): the shape
@@ -359,12 +360,13 @@ static cudaError_t fused_levels(const Ctx& c, bool topo, bool uv, float* pts, bo
 cudaError_t run_fused(const Ctx& c, bool topo, const float* cagePts, float* pts, int mode, bool det) {
     const bool creased = mode == CCS_POINTS_SCATTER;
     const bool uv = c.cage->U > 0 && c.rw == 4;
-    // the shape half of every level's ring statistics beside the cage step
+    // beside the cage step's points: its topology and creases, then the shape
+    // half of every level's ring statistics
     Fork shapes(c, topo && c.stats);
     if (topo)
         for (int d = 1; d < c.D; ++d) shape_stats_level(c, d, shapes.stream());
     const int step = c.prof->begin(c.stream, CCS_K_STEP, 0, c.lv[0].H);
-    cudaError_t e = run_cage_step(c, topo, uv, cagePts, pts + 3 * c.lv[1].ptOff, mode, det);
+    cudaError_t e = run_cage_step(c, topo, uv, cagePts, pts + 3 * c.lv[1].ptOff, mode, det, shapes.stream());
     c.prof->end(c.stream, step);
     if (e == cudaSuccess) {
         if (c.rw == 4)
