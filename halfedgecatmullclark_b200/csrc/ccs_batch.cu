@@ -60,6 +60,8 @@ enum Phase {
     PH_ADJ_EDGE,        // H_d
     PH_ADJ_FACE,        // F_d (cage)
     PH_ADJ_VERT,        // V_0 (cage) or H_d
+    PH_ZERO3,           // d = 1: V_2 vertex slots of depth 3 (the one-pass step of depth 2)
+    PH_CREASE_STATS_NEXT,  // C_(d+1) creases of depth d + 1 (their statistics, before depth d + 1)
     PH_COUNT
 };
 
@@ -258,45 +260,99 @@ __device__ __forceinline__ void fwd_cage_s3(const BatchArgs& a) {
     fwd_shape_next<TOPO>(a, 0);
 }
 
-// d >= 1, section 1: kernel A tiles, crease tiles, creased-edge statistics
+// Quad levels.  Deterministic pass, every depth d >= 1: section 1 = kernel A
+// tiles, crease tiles, creased-edge statistics of depth d; section 2 = the
+// exact vertex pass + shape statistics of depth d + 1.  Default (atomic)
+// pass: depth 1 as the deterministic schedule plus the clearing of depth 3's
+// slots, and a section 3 with the creased-edge statistics of depth 2; depth
+// d >= 2: section 1 = one-pass step tiles (tile_level_ab, which clear depth
+// d + 2's slots), crease tiles, shape statistics of depth d + 1; section 2 =
+// the creased-edge statistics of depth d + 1 (after its shape entries).
+__device__ __forceinline__ LevelArgs batch_level_args(const BatchArgs& a, const BatchCage& bc, int d) {
+    const Level& lv = bc.lv[d];
+    LevelArgs la;
+    la.in = a.he + 4 * (bc.he + lv.heOff);
+    la.out = a.he + 4 * (bc.he + bc.lv[d + 1].heOff);
+    la.crIn = a.cr + bc.cr + lv.crOff;
+    la.crOut = a.cr + bc.cr + bc.lv[d + 1].crOff;
+    la.pin = a.pts + 3 * (bc.pt + lv.ptOff);
+    la.pout = a.pts + 3 * (bc.pt + bc.lv[d + 1].ptOff);
+    la.H = lv.H; la.V = lv.V; la.F = lv.F; la.E = lv.E; la.C = lv.C;
+    return la;
+}
+
+template <bool TOPO>
+__device__ __forceinline__ void fwd_crease_tiles(const BatchArgs& a, int d) {
+    if (!TOPO) return;
+    const int tid = threadIdx.x;
+    for_tiles(a, d, PH_A_CREASE, [&](const BatchCage& bc, int64_t lt) {
+        const int64_t i = lt * kBatchBlock + tid;
+        if (i < bc.lv[d].C)
+            crease_item(a.cr + bc.cr + bc.lv[d].crOff, a.cr + bc.cr + bc.lv[d + 1].crOff, (int32_t)i);
+    });
+}
+
+// creased edges of depth dd into the older vertices' statistics (their shape
+// entries must be written)
+__device__ __forceinline__ void fwd_crease_stats(const BatchArgs& a, int d, int phase, int dd) {
+    const int tid = threadIdx.x;
+    for_tiles(a, d, phase, [&](const BatchCage& bc, int64_t lt) {
+        const int64_t i = lt * kBatchBlock + tid;
+        if (dd < bc.depth && i < bc.lv[dd].C)
+            crease_stats_item(batch_quad_view(a, bc, dd), bc.lv[dd - 1].V, a.stats + bc.stats[dd], (int32_t)i);
+    });
+}
+
+// default pass, depth d >= 2, section 1
+template <bool TOPO, bool CREASED>
+__device__ __forceinline__ void fwd_level_ab(const BatchArgs& a, int d, int32_t* tile) {
+        for_tiles(a, d, PH_A, [&](const BatchCage& bc, int64_t lt) {
+            LevelArgs la = batch_level_args(a, bc, d);
+            la.ostats = a.stats + bc.stats[d];
+            if (d + 2 <= bc.depth) {
+                la.zeroNext = a.pts + 3 * (bc.pt + bc.lv[d + 2].ptOff);
+                la.zeroNextN = 3 * (int64_t)bc.lv[d + 1].V;
+            }
+            const int64_t stride = (((int64_t)bc.lv[d].H + kBatchBlock - 1) / kBatchBlock) * kBatchBlock;
+            if (bc.uv) tile_level_ab<kBatchBlock, 4, TOPO, true, CREASED>(la, lt * kBatchBlock, tile, stride);
+            else tile_level_ab<kBatchBlock, 4, TOPO, false, CREASED>(la, lt * kBatchBlock, tile, stride);
+            __syncthreads();   // the tile's shared memory is reused by the next tile
+        });
+        fwd_crease_tiles<TOPO>(a, d);
+        fwd_shape_next<TOPO>(a, d);
+}
+
+// section 1 of depth 1, and of every depth in the deterministic pass
 template <bool TOPO, bool CREASED, bool DET>
 __device__ __forceinline__ void fwd_level_s1(const BatchArgs& a, int d, int32_t* tile) {
     const int tid = threadIdx.x;
     for_tiles(a, d, PH_A, [&](const BatchCage& bc, int64_t lt) {
-        const Level& lv = bc.lv[d];
-        LevelArgs la;
-        la.in = a.he + 4 * (bc.he + lv.heOff);
-        la.out = a.he + 4 * (bc.he + bc.lv[d + 1].heOff);
-        la.crIn = a.cr + bc.cr + lv.crOff;
-        la.crOut = a.cr + bc.cr + bc.lv[d + 1].crOff;
-        la.pin = a.pts + 3 * (bc.pt + lv.ptOff);
-        la.pout = a.pts + 3 * (bc.pt + bc.lv[d + 1].ptOff);
-        la.H = lv.H; la.V = lv.V; la.F = lv.F; la.E = lv.E; la.C = lv.C;
+        LevelArgs la = batch_level_args(a, bc, d);
         la.zeroV = DET ? 0 : 1;          // the atomic pass accumulates into cleared slots
         if (bc.uv) tile_level_a<kBatchBlock, 4, TOPO, true, true, CREASED>(la, lt * kBatchBlock, tile);
         else tile_level_a<kBatchBlock, 4, TOPO, false, true, CREASED>(la, lt * kBatchBlock, tile);
         __syncthreads();   // the tile's shared memory is reused by the next tile
     });
-    if (TOPO) {
-        for_tiles(a, d, PH_A_CREASE, [&](const BatchCage& bc, int64_t lt) {
+    fwd_crease_tiles<TOPO>(a, d);
+    if (TOPO) fwd_crease_stats(a, d, PH_CREASE_STATS, d);
+    if (!DET) {
+        for_tiles(a, d, PH_ZERO3, [&](const BatchCage& bc, int64_t lt) {
             const int64_t i = lt * kBatchBlock + tid;
-            if (i < bc.lv[d].C)
-                crease_item(a.cr + bc.cr + bc.lv[d].crOff, a.cr + bc.cr + bc.lv[d + 1].crOff, (int32_t)i);
-        });
-        // creased edges of depth d into the older vertices' statistics (their
-        // shape entries were written by the previous depth's launch)
-        for_tiles(a, d, PH_CREASE_STATS, [&](const BatchCage& bc, int64_t lt) {
-            const int64_t i = lt * kBatchBlock + tid;
-            if (i < bc.lv[d].C)
-                crease_stats_item(batch_quad_view(a, bc, d), bc.lv[d - 1].V, a.stats + bc.stats[d], (int32_t)i);
+            if (bc.depth >= 3 && i < bc.lv[2].V) st3(a.pts + 3 * (bc.pt + bc.lv[3].ptOff + i), zero3());
         });
     }
 }
 
-// d >= 1, section 2: vertex pass (+ shape statistics of depth d + 1)
+// section 2: the vertex pass + shape statistics of depth d + 1 (depth 1 or the
+// deterministic pass); the creased-edge statistics of depth d + 1 (d >= 2,
+// default pass)
 template <bool TOPO, bool CREASED, bool DET>
 __device__ __forceinline__ void fwd_level_s2(const BatchArgs& a, int d) {
     const int tid = threadIdx.x;
+    if (!DET && d >= 2) {
+        if (TOPO) fwd_crease_stats(a, d, PH_CREASE_STATS_NEXT, d + 1);
+        return;
+    }
     if (DET && d >= 2) {
         for_tiles(a, d, PH_V, [&](const BatchCage& bc, int64_t lt) {
             const int64_t v = lt * kBatchBlock + tid;
@@ -321,6 +377,12 @@ __device__ __forceinline__ void fwd_level_s2(const BatchArgs& a, int d) {
         }
     });
     fwd_shape_next<TOPO>(a, d);
+}
+
+// section 3 (default pass, depth 1): the creased-edge statistics of depth 2
+template <bool TOPO>
+__device__ __forceinline__ void fwd_level_s3(const BatchArgs& a, int d) {
+    if (TOPO) fwd_crease_stats(a, d, PH_CREASE_STATS_NEXT, d + 1);
 }
 
 __device__ __forceinline__ float* adj_gnew(const BatchArgs& a, const BatchCage& bc, int d) {
@@ -379,9 +441,14 @@ k_batch_forward(BatchArgs a, int d) {
         fwd_cage_s3<TOPO, CREASED, DET>(a);
         return;
     }
-    fwd_level_s1<TOPO, CREASED, DET>(a, d, tile);
+    if (!DET && d >= 2) fwd_level_ab<TOPO, CREASED>(a, d, tile);
+    else fwd_level_s1<TOPO, CREASED, DET>(a, d, tile);
     if (!grid_sync(a.sync, a.spinCap, gridDim.x)) return;
     fwd_level_s2<TOPO, CREASED, DET>(a, d);
+    if (TOPO && !DET && d == 1) {
+        if (!grid_sync(a.sync, a.spinCap, gridDim.x)) return;
+        fwd_level_s3<TOPO>(a, d);
+    }
 }
 
 __global__ void __launch_bounds__(kBatchBlock)
@@ -400,7 +467,7 @@ k_batch_adjoint(BatchArgs a, int d) {
 }
 
 // split schedule: one ordinary launch per section (kernel boundaries order them)
-enum Section { SEC_CAGE_1 = 0, SEC_CAGE_2, SEC_CAGE_3, SEC_LEVEL_1, SEC_LEVEL_2 };
+enum Section { SEC_CAGE_1 = 0, SEC_CAGE_2, SEC_CAGE_3, SEC_LEVEL_1, SEC_LEVEL_2, SEC_LEVEL_3 };
 
 template <bool TOPO, bool CREASED, bool DET, int S>
 __global__ void __launch_bounds__(kBatchBlock)
@@ -411,9 +478,20 @@ k_batch_forward_section(BatchArgs a, int d) {
     else if constexpr (S == SEC_LEVEL_1) {
         __shared__ __align__(128) int32_t tile[kBatchBlock * 4 * 4];
         fwd_level_s1<TOPO, CREASED, DET>(a, d, tile);
-    } else {
+    } else if constexpr (S == SEC_LEVEL_2) {
         fwd_level_s2<TOPO, CREASED, DET>(a, d);
+    } else {
+        fwd_level_s3<TOPO>(a, d);
     }
+}
+
+// split schedule, default pass, depth d >= 2: section 1 on its own register
+// budget (the single-mesh one-pass step's)
+template <bool TOPO, bool CREASED>
+__global__ void __launch_bounds__(kBatchBlock, 6)
+k_batch_level_ab(BatchArgs a, int d) {
+    __shared__ __align__(128) int32_t tile[kBatchBlock * 4 * 4];
+    fwd_level_ab<TOPO, CREASED>(a, d, tile);
 }
 
 template <int S>
@@ -495,6 +573,8 @@ static int64_t phase_units(const BatchCage& bc, int d, int ph) {
         case PH_ADJ_EDGE: return lv.H;
         case PH_ADJ_FACE: return d == 0 ? lv.F : 0;
         case PH_ADJ_VERT: return d == 0 ? lv.V : lv.H;
+        case PH_ZERO3: return d == 1 && bc.depth >= 3 ? bc.lv[2].V : 0;
+        case PH_CREASE_STATS_NEXT: return d >= 1 && d + 1 < bc.depth ? bc.lv[d + 1].C : 0;
         default: return 0;
     }
 }
@@ -701,11 +781,22 @@ static cudaError_t forward_sections(ccs_Batch* b, const BatchArgs& a, int d) {
                                   max_tiles(b, 0, {PH_CAGE_VERT, PH_SHAPE_NEXT}), a, 0, false);
         return e;
     }
+    if (!DET && d >= 2) {
+        e = launch_persistent(b, k_batch_level_ab<TOPO, CREASED>,
+                              max_tiles(b, d, {PH_A, PH_A_CREASE, PH_SHAPE_NEXT}), a, d, false);
+        if (e == cudaSuccess && TOPO)
+            e = launch_persistent(b, k_batch_forward_section<TOPO, CREASED, DET, SEC_LEVEL_2>,
+                                  max_tiles(b, d, {PH_CREASE_STATS_NEXT}), a, d, false);
+        return e;
+    }
     e = launch_persistent(b, k_batch_forward_section<TOPO, CREASED, DET, SEC_LEVEL_1>,
-                          max_tiles(b, d, {PH_A, PH_A_CREASE, PH_CREASE_STATS}), a, d, false);
+                          max_tiles(b, d, {PH_A, PH_A_CREASE, PH_CREASE_STATS, PH_ZERO3}), a, d, false);
     if (e == cudaSuccess)
         e = launch_persistent(b, k_batch_forward_section<TOPO, CREASED, DET, SEC_LEVEL_2>,
                               max_tiles(b, d, {PH_V, PH_B, PH_SHAPE_NEXT}), a, d, false);
+    if (e == cudaSuccess && TOPO && !DET && d == 1)
+        e = launch_persistent(b, k_batch_forward_section<TOPO, CREASED, DET, SEC_LEVEL_3>,
+                              max_tiles(b, d, {PH_CREASE_STATS_NEXT}), a, d, false);
     return e;
 }
 
@@ -754,7 +845,8 @@ static cudaError_t enqueue_batch(ccs_Batch* b, int op, bool creased) {
     for (int d = 0; d < b->maxDepth && e == cudaSuccess; ++d) {
         const int64_t mt = d == 0 ? max_tiles(b, 0, {PH_CAGE_TOPO, PH_CAGE_CREASE, PH_CAGE_FACE, PH_CAGE_ZERO,
                                                       PH_CAGE_EDGE, PH_CAGE_VERT, PH_SHAPE_NEXT})
-                                  : max_tiles(b, d, {PH_A, PH_A_CREASE, PH_CREASE_STATS, PH_V, PH_B, PH_SHAPE_NEXT});
+                                  : max_tiles(b, d, {PH_A, PH_A_CREASE, PH_CREASE_STATS, PH_V, PH_B, PH_SHAPE_NEXT,
+                                                     PH_ZERO3, PH_CREASE_STATS_NEXT});
         const int v = (topo ? 4 : 0) + (creased ? 2 : 0) + (det ? 1 : 0);
         switch (v) {
             case 0: e = launch_coop(b, k_batch_forward<false, false, false>, mt, a, d); break;
