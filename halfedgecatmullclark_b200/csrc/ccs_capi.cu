@@ -176,6 +176,8 @@ struct SubdImpl {
     bool pinned = true;
     bool topo_ready = false, creases_ready = false;
     bool fusable = true;           // twin relation holds: fused kernels allowed
+    std::vector<CUtensorMap> childMaps;  // per level d: TMA map of the child records it writes
+    std::vector<uint8_t> childMapOk;
     Profiler prof;
     std::map<int, cudaGraphExec_t> graphs;
 
@@ -186,6 +188,7 @@ struct SubdImpl {
         c.side = side; c.forkEv = forkEv; c.joinEv = joinEv;
         c.stats = stats; c.statsOff = statsOff.data();
         c.fusable = fusable;
+        if (!childMaps.empty()) { c.childMaps = childMaps.data(); c.childMapOk = childMapOk.data(); }
         return c;
     }
 };
@@ -333,6 +336,13 @@ static int create(const cc_Mesh* cage, int32_t D, uint32_t flags, cc_Subd** out)
     }
     st = upload_cage(s, cage);
     if (st != CCS_OK) { free_impl(s); return st; }
+    if (s->rw == 4) {
+        s->childMaps.resize((size_t)D + 1);
+        s->childMapOk.assign((size_t)D + 1, 0);
+        for (int d = 1; d < D; ++d)
+            s->childMapOk[(size_t)d] = encode_child_map(&s->childMaps[(size_t)d], s->he + 4 * lv[(size_t)d + 1].heOff,
+                                                        lv[(size_t)d].H) ? 1 : 0;
+    }
     {
         std::lock_guard<std::mutex> lock(g_mu);
         g_reg[s->host] = s;
@@ -439,6 +449,41 @@ int adjoint_into(const cc_Subd* subd, const float* gradPoints, float* gradCage, 
 }
 
 int set_last_error(int status) { return ret(status); }
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library)
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            p = nullptr;
+        }
+        return reinterpret_cast<EncodeTiledFn>(p);
+    }();
+    return fn;
+}
+
+bool encode_child_map(CUtensorMap* map, int32_t* levelRecords, int64_t parentHalfedges) {
+    const EncodeTiledFn fn = encode_tiled();
+    if (!fn || parentHalfedges < 2 || (parentHalfedges & 1) || (reinterpret_cast<uintptr_t>(levelRecords) & 15))
+        return false;
+    // rows of 32 int32 (128 bytes: the four 16-byte children of two parent
+    // halfedges), one row per two parents; boxes of 128 rows (256 parents)
+    const cuuint64_t dims[2] = {32, (cuuint64_t)(parentHalfedges / 2)};
+    const cuuint64_t strides[1] = {128};
+    const cuuint32_t box[2] = {32, 128};
+    const cuuint32_t elem[2] = {1, 1};
+    return fn(map, CU_TENSOR_MAP_DATA_TYPE_INT32, 2, levelRecords, dims, strides, box, elem,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
 
 bool subd_view(const cc_Subd* subd, SubdView* v) {
     SubdImpl* s = find(subd);

@@ -3,6 +3,7 @@
 
 #include <cstdint>
 #include <vector>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "ccs_cuda.h"
@@ -68,7 +69,17 @@ struct Ctx {
     float4* stats = nullptr;
     const int64_t* statsOff = nullptr;
     bool fusable = true;         // the twin relation vertex(twin h) = vertex(next h) holds
+    // TMA tensor maps of the child records each level d writes (level d+1's
+    // records as rows of 128 bytes), indexed by d; null / 0 = not available
+    const CUtensorMap* childMaps = nullptr;
+    const uint8_t* childMapOk = nullptr;
 };
+
+// Encodes the tensor map of the child records written by the step d -> d+1
+// (rows of 128 bytes over level d+1's 16-byte records, 128-row boxes,
+// 128-byte swizzle); false when the driver entry point is missing or the
+// encoding is refused.
+bool encode_child_map(CUtensorMap* map, int32_t* levelRecords, int64_t parentHalfedges);
 
 // A cage and all its arrays in one page-locked (else malloc'd) host block
 // (ccs_ccm.cu); NULL when out of memory.  free_cage_block takes such a cage.

@@ -41,6 +41,7 @@
 // then preserved by every refinement step) and uses the unfused kernels for
 // cages that break it.
 #include <cstdint>
+#include <cstring>
 
 #include "ccs_host.h"
 #include "ccs_tiles.cuh"
@@ -81,9 +82,9 @@ k_level_a(LevelArgs a) {
 #ifndef CCS_AB_MIN_BLOCKS
 #define CCS_AB_MIN_BLOCKS 6
 #endif
-template <int RW, bool TOPO, bool UV, bool CREASED>
+template <int RW, bool TOPO, bool UV, bool CREASED, bool TMAP>
 __global__ void __launch_bounds__(kBlockL, CCS_AB_MIN_BLOCKS)
-k_level_ab(LevelArgs a) {
+k_level_ab(LevelArgs a, const __grid_constant__ CUtensorMap childMap) {
     const int nbH = (a.H + kBlockL - 1) / kBlockL;
     if ((int)blockIdx.x >= nbH) {
         if (!TOPO) return;
@@ -94,8 +95,9 @@ k_level_ab(LevelArgs a) {
         }
         return;
     }
-    __shared__ __align__(128) int32_t tile[TOPO ? kBlockL * 4 * RW : 4];
-    tile_level_ab<kBlockL, RW, TOPO, UV, CREASED>(a, (int64_t)blockIdx.x * kBlockL, tile, (int64_t)nbH * kBlockL);
+    __shared__ __align__(1024) int32_t tile[TOPO ? kBlockL * 4 * RW : 4];
+    tile_level_ab<kBlockL, RW, TOPO, UV, CREASED, TMAP>(a, (int64_t)blockIdx.x * kBlockL, tile,
+                                                        (int64_t)nbH * kBlockL, &childMap);
 }
 
 // default vertex pass: one tile of halfedges per block
@@ -240,11 +242,18 @@ static void level_ab(const Ctx& c, int d, bool topo, bool uv, float* pts) {
     next_slots(c, d, pts, a);
     const unsigned nb = nblocksL(lv.H) + (topo ? nblocksL(lv.C) : 0u);
     c.prof->begin(c.stream, topo ? CCS_K_LEVEL_STEP : CCS_K_LEVEL_STEP_POINTS, d, lv.H);
-    if (topo) {
-        if (RW == 4 && uv) k_level_ab<RW, true, true, CREASED><<<nb, kBlockL, 0, c.stream>>>(a);
-        else k_level_ab<RW, true, false, CREASED><<<nb, kBlockL, 0, c.stream>>>(a);
+    const bool tmap = RW == 4 && topo && c.childMaps && c.childMapOk && c.childMapOk[d];
+    CUtensorMap none;
+    memset(&none, 0, sizeof none);
+    const CUtensorMap& map = tmap ? c.childMaps[d] : none;
+    if (topo && tmap) {
+        if (uv) k_level_ab<RW, true, true, CREASED, RW == 4><<<nb, kBlockL, 0, c.stream>>>(a, map);
+        else k_level_ab<RW, true, false, CREASED, RW == 4><<<nb, kBlockL, 0, c.stream>>>(a, map);
+    } else if (topo) {
+        if (RW == 4 && uv) k_level_ab<RW, true, true, CREASED, false><<<nb, kBlockL, 0, c.stream>>>(a, map);
+        else k_level_ab<RW, true, false, CREASED, false><<<nb, kBlockL, 0, c.stream>>>(a, map);
     } else {
-        k_level_ab<RW, false, false, CREASED><<<nb, kBlockL, 0, c.stream>>>(a);
+        k_level_ab<RW, false, false, CREASED, false><<<nb, kBlockL, 0, c.stream>>>(a, map);
     }
     c.prof->end(c.stream);
 }

@@ -45,6 +45,18 @@ __device__ __forceinline__ void bulk_store_tile(void* gdst, const void* ssrc, ui
     asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
 }
 
+// One thread writes a 256-halfedge tile of child records (128 rows of 128
+// bytes, 128-byte swizzled in shared memory) to rows [row, row + 128) of the
+// tensor `tmap` describes (TMA tensor store, no multicast; rows past the
+// tensor's end are not written) and waits until the tile has been read.
+__device__ __forceinline__ void tensor_store_tile(const void* tmap, const void* ssrc, int32_t row) {
+    const uint32_t s = (uint32_t)__cvta_generic_to_shared(ssrc);
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];"
+                 :: "l"(tmap), "r"(0), "r"(row), "r"(s) : "memory");
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+    asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+
 __device__ __forceinline__ f3 shfl3(f3 v, int src) {
     return f3{__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src),
               __shfl_sync(0xffffffffu, v.z, src)};
@@ -486,8 +498,15 @@ __device__ __forceinline__ void tile_level_b(const QuadView<RW>& L, const float*
 // The vertex slots [0, V) of depth d+1 must be zero on entry; the tile also
 // clears its share of `zeroNext` (the slots the next level accumulates into).
 // Requires BLOCK a multiple of 32 and h0 a multiple of 16.
-template <int BLOCK, int RW, bool TOPO, bool UV, bool CREASED>
-__device__ __forceinline__ void tile_level_ab(const LevelArgs& a, int64_t h0, int32_t* tile, int64_t zeroStride) {
+// TMAP (16-byte records, BLOCK = 256): the child records go out through the
+// TMA tensor store of `tmap` (rows of 128 bytes = the children of two parent
+// halfedges) from a 128-byte swizzled tile (1024-byte aligned): 16-byte chunk
+// c of row r sits at chunk c ^ (r & 7), which also spreads every
+// quarter-warp's stores over the 32 banks.
+template <int BLOCK, int RW, bool TOPO, bool UV, bool CREASED, bool TMAP = false>
+__device__ __forceinline__ void tile_level_ab(const LevelArgs& a, int64_t h0, int32_t* tile, int64_t zeroStride,
+                                              const void* tmap = nullptr) {
+    static_assert(!TMAP || (RW == 4 && BLOCK == 256), "tensor-store tiles are 256 sixteen-byte records wide");
     const unsigned full = 0xffffffffu;
     const int tid = threadIdx.x, lane = tid & 31;
     const int64_t h64 = h0 + tid;
@@ -622,12 +641,23 @@ __device__ __forceinline__ void tile_level_ab(const LevelArgs& a, int64_t h0, in
         c_ed[0] = 2 * ed + (h > tw ? 0 : 1); c_ed[1] = 2 * a.E + h; c_ed[2] = 2 * a.E + prev;
         c_ed[3] = 2 * ped + (prev > ptw ? 1 : 0);
         c_vx[0] = vx; c_vx[1] = a.V + a.F + ed; c_vx[2] = a.V + f; c_vx[3] = a.V + a.F + ped;
-        put_children<RW, UV>(tile, tid, lane, c_tw, c_ed, c_vx, uvc);
+        if constexpr (TMAP) {
+            const int r = tid >> 1, sw = r & 7, cb = (tid & 1) << 2;
+            int4* row = reinterpret_cast<int4*>(tile) + 8 * r;
+#pragma unroll
+            for (int m = 0; m < 4; ++m) row[(cb + m) ^ sw] = make_int4(c_tw[m], c_ed[m], c_vx[m], UV ? uvc[m] : 0);
+        } else {
+            put_children<RW, UV>(tile, tid, lane, c_tw, c_ed, c_vx, uvc);
+        }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (tid == 0) {
-            const int64_t n = (a.H - h0) < BLOCK ? (a.H - h0) : BLOCK;
-            bulk_store_tile(a.out + 4 * RW * h0, tile, (uint32_t)(n * 16 * RW));
+            if constexpr (TMAP) {
+                tensor_store_tile(tmap, tile, (int32_t)(h0 >> 1));
+            } else {
+                const int64_t n = (a.H - h0) < BLOCK ? (a.H - h0) : BLOCK;
+                bulk_store_tile(a.out + 4 * RW * h0, tile, (uint32_t)(n * 16 * RW));
+            }
         }
     }
 }
