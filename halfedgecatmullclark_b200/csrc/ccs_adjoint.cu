@@ -12,8 +12,11 @@
 // (coefficients in ccs_tiles.cuh).  Given g = dL/d(points of depth d+1) this
 // file computes dL/d(points of depth d) += S_d^T g.
 //
-// Quad levels (d >= 1, cages with the twin relation): two halfedge-parallel
-// passes with the forward's lane layout (ccs_tiles.cuh adj_quad_*):
+// Quad levels d >= 2 (cages with the twin relation, ring statistics kept):
+// one halfedge-parallel pass, adj_quad_step_tile, which completes each
+// edge's gradient in both of its halves and then adds the vertex terms.
+// Depth 1: two halfedge-parallel passes with the forward's lane layout
+// (ccs_tiles.cuh adj_quad_*):
 //   1. gE[e] += the cE / dE terms, completed by the pair's larger halfedge
 //      (its own side from the quad's lanes, the twin side's coefficients
 //      recomputed; the twin side's vertices are this side's);
@@ -76,6 +79,16 @@ k_adj_quad_edges(QuadView<RW> L, float* __restrict__ gNew) {
     adj_quad_edge_tile<RW>(L, gNew, (int64_t)blockIdx.x * kBlockA);
 }
 
+// quad levels d >= 2 with the older vertices' statistics: one pass
+#ifndef CCS_ADJ_STEP_MIN_BLOCKS
+#define CCS_ADJ_STEP_MIN_BLOCKS 5
+#endif
+template <int RW>
+__global__ void __launch_bounds__(kBlockA, CCS_ADJ_STEP_MIN_BLOCKS)
+k_adj_quad_step(QuadView<RW> L, const float* __restrict__ gNew, float* __restrict__ gOld) {
+    adj_quad_step_tile<RW>(L, gNew, gOld, (int64_t)blockIdx.x * kBlockA);
+}
+
 template <int RW, bool STRUCT>
 __global__ void __launch_bounds__(kBlockA, 8)
 k_adj_quad_points(QuadView<RW> L, const float* __restrict__ gNew, float* __restrict__ gOld) {
@@ -86,6 +99,14 @@ static CageTables cage_tables_a(const DevCage& c) { return make_cage_tables(c); 
 
 template <int RW>
 static void adjoint_quad_level(const Ctx& c, const QuadView<RW>& L, float* gNew, float* gOld) {
+#ifndef CCS_NO_ADJ_STEP
+    if (L.d >= 2 && L.ostats) {
+        c.prof->begin(c.stream, CCS_K_ADJ_STEP, L.d, L.H);
+        k_adj_quad_step<RW><<<nblocksA(L.H), kBlockA, 0, c.stream>>>(L, gNew, gOld);
+        c.prof->end(c.stream);
+        return;
+    }
+#endif
     c.prof->begin(c.stream, CCS_K_ADJ_EDGES, L.d, L.H);
     k_adj_quad_edges<RW><<<nblocksA(L.H), kBlockA, 0, c.stream>>>(L, gNew);
     c.prof->end(c.stream);

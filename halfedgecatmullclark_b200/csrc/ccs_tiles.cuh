@@ -1575,4 +1575,125 @@ __device__ __forceinline__ void adj_quad_point_tile(const QuadView<RW>& L, const
     }
 }
 
+// One pass for a quad level d >= 2 of the adjoint (tile of halfedges
+// [h0, h0 + blockDim), the forward's lane layout): pass 1's edge gradient is
+// completed by both halves of every edge instead of accumulated by atomics,
+// then pass 2's vertex terms follow in the same thread.
+//   gEt[e(h)] = gE[e] + cE(h) gV[v(h)] + dE(next h) gV[v(next h)]      (own side)
+//                     + cE(t) gV[v(t)] + dE(next t) gV[v(next t)]      (twin t)
+// with v(t) = v(next h), v(next t) = v(h).  The twin side:
+//   * inside the parent quad (children 1, 2): the twin lane's own side;
+//   * across a parent edge, child 0 of g (twin t = child 3 of next(twin g)):
+//     cE(t) at the parent edge's midpoint, an interior vertex of valence 4
+//     whose only creased edges are the parent edge's two halves; dE(next t)
+//     at the older vertex v(h), non-zero only on a boundary in the crease
+//     branch (the only case that reads next t's edge);
+//   * child 3 of g (twin t = child 0 of twin(prev g)): cE(t) at the older
+//     vertex v(next h) (its statistics from the quad's child-0 lane, the
+//     boundary correction with t's edge, which is h's); dE(next t) = 0, at
+//     the interior midpoint of prev(g)'s edge;
+//   * anything else: the coefficients by ring walks (vertex_coef).
+// Both halves of an edge evaluate the same terms; gE is read, not written.
+template <int RW>
+__device__ __forceinline__ void adj_quad_step_tile(const QuadView<RW>& L, const float* __restrict__ gNew,
+                                                   float* __restrict__ gOld, int64_t h0) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31, k = lane & 3, qb = lane & ~3, j = (lane >> 2) & 3;
+    const int ln = qb | ((k + 1) & 3), lp = qb | ((k + 3) & 3);
+    const int64_t h64 = h0 + threadIdx.x;
+    const bool valid = h64 < L.H;
+    const int32_t h = (int32_t)h64;
+    const float* gV = gNew;
+    const float* gF = gNew + 3 * (int64_t)L.V;
+    const float* gE = gNew + 3 * ((int64_t)L.V + L.F);
+    int32_t tw = -1, ed = 0, vx = 0;
+    float4 st = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    f3 gv = zero3(), ge = zero3(), gf = zero3();
+    float sOwn = 0.0f, sOther = 0.0f;
+    if (valid) {
+        lane_record(L, h64, tw, ed, vx);
+        gv = ld3(gV + 3 * (int64_t)vx);
+        ge = ld3(gE + 3 * (int64_t)ed);
+        sOwn = L.sharp(ed);
+        if (k == 0) {
+            gf = ld3(gF + 3 * (int64_t)(h >> 2));
+            st = L.ostats[vx];
+            sOther = L.sharp(ed ^ 1);
+        }
+    }
+    const int32_t ped = __shfl_sync(full, ed, lp), ptw = __shfl_sync(full, tw, lp);
+    VCoef kc{0.0f, 0.0f, 0.0f, 0.0f};
+    ECoef ke{0.0f, 0.0f, 0.0f};
+    if (valid) {
+        kc = lane_vertex_coef(L, h, tw, ed, ptw, ped, st);
+        const float w = fsat(sOwn), b = tw < 0 ? 1.0f : 0.5f;    // edge_coef
+        ke.al = (1.0f - w) * 0.25f + w * b * 0.5f;
+        ke.be = w * b * 0.5f;
+        ke.ga = (1.0f - w) * 0.25f;
+    }
+    const float dEn = __shfl_sync(full, kc.dE, ln);
+    const f3 gn = shfl3(gv, ln);
+    const f3 own = add3(mul3(gv, kc.cE), mul3(gn, dEn));
+    // the older vertex's statistics of the quad (its child-0 lane)
+    const float4 sq = make_float4(__shfl_sync(full, st.x, qb), __shfl_sync(full, st.y, qb),
+                                  __shfl_sync(full, st.z, qb), __shfl_sync(full, st.w, qb));
+    const int sibK = k == 1 ? ((((j + 1) & 3) << 2) | 2) : ((((j + 3) & 3) << 2) | 1);
+    const f3 ownSib = shfl3(own, (lane & ~15) | sibK);
+    f3 twinSide = zero3();
+    if (valid && tw >= 0) {
+        const int kt = tw & 3;
+        if ((k == 1 || k == 2) && tw == ((h & ~15) | sibK)) {
+            twinSide = ownSib;
+        } else if (k == 0 && kt == 3) {
+            // cE(t) at the midpoint (interior, valence 4)
+            const VCoef ct = coef_from_stats(4.0f, fsign(sOwn) + fsign(sOther), sOwn + sOther, false, fsign(sOwn), 0.0f);
+            // dE(next t) at the older vertex v(h) = this lane's
+            float dEt = 0.0f;
+            const bool bnd = st.w != 0.0f;
+            const float valence = bnd ? st.x + 1.0f : st.x;
+            if (bnd && !(st.z >= 3.0f || valence == 2.0f) && !(st.z <= 1.0f) && sOwn != 0.0f) {
+                const int32_t en = L.edge(tw & ~3);      // next(t) = child 0 of t's quad
+                const float sn = L.sharp(en);
+                const float t = fsat((st.y - sn) * 0.5f);
+                dEt = t * 0.25f * fsign(sOwn);
+            }
+            twinSide = add3(mul3(gn, ct.cE), mul3(gv, dEt));
+        } else if (k == 3 && kt == 0) {
+            // cE(t) at the older vertex v(next h), seen from t (its edge is h's)
+            const bool bnd = sq.w != 0.0f;
+            const float avgS = bnd ? sq.y - sOwn : sq.y;
+            const float cpre = bnd ? sq.z - fsign(sOwn) : sq.z;
+            const VCoef ct = coef_from_stats(sq.x, cpre, avgS, bnd, fsign(sOwn), 0.0f);
+            twinSide = mul3(gn, ct.cE);
+        } else {
+            const VCoef a = vertex_coef(L, tw), an = vertex_coef(L, qnext(tw));
+            twinSide = add3(mul3(gn, a.cE), mul3(gv, an.dE));
+        }
+    }
+    const f3 gEt = add3(add3(ge, own), twinSide);
+    // pass 2: face gradient over the quad, then this halfedge's vertex term
+    f3 ft = add3(mul3(gv, kc.bF), mul3(gEt, ke.ga));
+    ft = add3(ft, shfl_xor3(ft, 1));
+    ft = add3(ft, shfl_xor3(ft, 2));
+    const f3 gFt = add3(shfl3(gf, qb), ft);
+    const float bep = __shfl_sync(full, ke.be, lp);
+    const f3 gep = shfl3(gEt, lp);
+    const f3 s = add3(add3(mul3(gv, kc.a), mul3(gEt, ke.al)), add3(mul3(gFt, 0.25f), mul3(gep, bep)));
+    float* o = gOld + 3 * (int64_t)vx;
+    const f3 s4 = shfl_down3(s, 4), s8 = shfl_down3(s, 8), s12 = shfl_down3(s, 12);
+    const int partner = (lane & ~15) | ((((lane >> 2) + 1) & 3) << 2) | 3;
+    const f3 sA2 = shfl3(s, partner);
+    if (!valid) return;
+    if ((lane & 15) == 2) {
+        const f3 t = add3(add3(s, s4), add3(s8, s12));
+        o[0] += t.x;
+        o[1] += t.y;
+        o[2] += t.z;
+    } else if (k == 1) {
+        atomic_add3(o, add3(s, sA2));
+    } else if (k == 0) {
+        atomic_add3(o, s);
+    }
+}
+
 }  // namespace ccs

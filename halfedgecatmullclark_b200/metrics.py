@@ -58,6 +58,11 @@ def kernel_bytes(kernel: str, lv: dict, rec: int = 16) -> int:
         # not counted (none at the last level)
         topo = 4 * rec * H + 36 * C if kernel == "level_step" else 12 * C
         return int(rec * H + topo + 12 * V + 12 * F + 12 * E + 12 * V + 16 * max(V - nb, 0))
+    if kernel == "adj_step":
+        # one adjoint pass of a step: records, the gradients of depth d+1
+        # (vertex, face and edge slots), the older vertices' statistics and
+        # the crease records in; the gradients of depth d out
+        return int(rec * H + 12 * (V + F + E) + 16 * max(V - nb, 0) + 12 * C + 12 * V)
     if kernel == "ring_stats":
         # records of children 0 and 3 walked, statistics out
         return int(rec * H // 2 + 16 * max(V - nb, 0))

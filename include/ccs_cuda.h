@@ -365,7 +365,8 @@ enum {
     CCS_K_ADJ_EDGES = 12, CCS_K_ADJ_FACES = 13, CCS_K_ADJ_VERTICES = 14, CCS_K_EXACT_POINTS = 15,
     CCS_K_STEP = 16 /* a whole refinement step d -> d+1, on the subd's stream */,
     CCS_K_LEVEL_STEP = 17 /* depth >= 2: topology, creases and all points in one launch */,
-    CCS_K_LEVEL_STEP_POINTS = 18 /* depth >= 2: all points of a step in one launch */, CCS_K_COUNT = 19
+    CCS_K_LEVEL_STEP_POINTS = 18 /* depth >= 2: all points of a step in one launch */,
+    CCS_K_ADJ_STEP = 19 /* adjoint of a depth >= 2 step in one launch */, CCS_K_COUNT = 20
 };
 /* When enabled, every launch of the subd is bracketed by CUDA events on its
  * stream (and CUDA graphs are not used). */

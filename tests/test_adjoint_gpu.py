@@ -141,3 +141,81 @@ def test_cage_fitting_adam_converges():
         opt.step()
         first = first if first is not None else float(loss)
     assert float(loss) < 0.1 * first
+
+
+def _boundary_crease_cage():
+    """Open 8x6 quad grid whose boundary is smooth except for one semi-sharp
+    segment on the left side, ending at the vertex where a semi-sharp
+    interior chain (a full row of edges) starts: an older boundary vertex in
+    the crease branch with a creased interior edge.  (Cages built with the
+    OBJ converter's conventions sharpen every boundary edge, which puts such
+    a vertex in the corner branch; a caller's own cage need not.)"""
+    from halfedgecatmullclark_b200.cage import build_cage
+    nx, ny = 8, 6
+    rng = np.random.default_rng(11)
+    x, y = np.meshgrid(np.arange(nx + 1), np.arange(ny + 1), indexing="ij")
+    pts = np.stack([x, y, 0.3 * rng.normal(size=x.shape)], -1).reshape(-1, 3).astype(np.float32)
+    vid = lambda i, j: i * (ny + 1) + j
+    faces = [[vid(i, j), vid(i + 1, j), vid(i + 1, j + 1), vid(i, j + 1)] for i in range(nx) for j in range(ny)]
+    tags = [(vid(i, 3), vid(i + 1, 3), 5.0) for i in range(nx)]
+    cage = build_cage(pts, faces, crease_tags=tags)
+    he = cage.halfedges
+    sharp = cage.creases["sharpness"]
+    for e, h in enumerate(cage.e2h):
+        if he["twinID"][h] < 0:
+            a, b = he["vertexID"][h], he["vertexID"][he["nextID"][h]]
+            left = a // (ny + 1) == 0 and b // (ny + 1) == 0 and max(a % (ny + 1), b % (ny + 1)) <= 3
+            sharp[e] = 4.0 if left else 0.0
+    return cage
+
+
+def _boundary_crease_hits(cage, depth):
+    """Child-0 halfedges with a twin whose (older, boundary) vertex has two
+    creased edges, valence above 2 and whose own edge is creased: the case
+    where the one-pass adjoint reads the twin quad's next edge."""
+    from oracle import oracle
+    he, cr = oracle.refine_topology(cage, depth)
+    hits = 0
+    for d in range(2, depth):
+        hs = oracle.level_slice(cage, depth, d, "H")
+        rec = he[hs]
+        C = oracle.counts(cage, depth)["C"][d]
+        cs = oracle.level_slice(cage, depth, d, "C")
+        sharp = np.zeros(rec.shape[0] * 2 + 16, np.float32)
+        sharp[:C] = cr[cs]["sharpness"]
+        vold = oracle.counts(cage, depth)["V"][d - 1]
+        tw, ed, vx = rec[:, 0], rec[:, 1], rec[:, 2]
+        inc = {}
+        bnd = np.zeros(int(vx.max()) + 1, bool)
+        for h in range(rec.shape[0]):
+            inc.setdefault(int(vx[h]), set()).add(int(ed[h]))
+            if tw[h] < 0:
+                bnd[vx[h]] = True
+                nxt = (h & ~3) | ((h + 1) & 3)
+                inc.setdefault(int(vx[nxt]), set()).add(int(ed[h]))
+                bnd[vx[nxt]] = True
+        for h in range(0, rec.shape[0], 4):
+            v = int(vx[h])
+            if tw[h] < 0 or v >= vold or not bnd[v] or sharp[ed[h]] == 0:
+                continue
+            n_crease = sum(1 for e in inc[v] if e < C and sharp[e] > 0)
+            if n_crease == 2 and len(inc[v]) != 2:
+                hits += 1
+    return hits
+
+
+def test_one_pass_adjoint_boundary_crease_branch():
+    import torch
+    from halfedgecatmullclark_b200.torch_ext import RefinePoints, SubdivisionSurface
+    from oracle import oracle
+    cage = _boundary_crease_cage()
+    depth = 4
+    assert _boundary_crease_hits(cage, depth) > 0     # the branch is reached
+    s = SubdivisionSurface(cage, depth)
+    x = torch.tensor(cage.vertex_points, device="cuda", requires_grad=True)
+    pts = RefinePoints.apply(x, s.subd)
+    g = torch.randn_like(pts)
+    pts.backward(g)
+    he, cr = oracle.refine_topology(cage, depth)
+    ref = oracle.adjoint(cage, depth, he, cr, g.double().cpu().numpy())
+    assert rel_err(x.grad.cpu().numpy(), ref) <= 1e-5
