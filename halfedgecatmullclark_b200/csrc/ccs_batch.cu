@@ -412,7 +412,15 @@ __device__ __forceinline__ void adj_cage_section(const BatchArgs& a) {
     }
 }
 
-// adjoint, d >= 1: edge pass (section 1), point pass (section 2)
+// adjoint, d >= 2: one pass (adj_quad_step_tile)
+__device__ __forceinline__ void adj_level_step(const BatchArgs& a, int d) {
+    for_tiles(a, d, PH_ADJ_VERT, [&](const BatchCage& bc, int64_t lt) {
+        float* gOld = a.work + 3 * (bc.pt + bc.lv[d].ptOff);
+        adj_quad_step_tile<4>(batch_quad_view_stats(a, bc, d), adj_gnew(a, bc, d), gOld, lt * kBatchBlock);
+    });
+}
+
+// adjoint, d = 1: edge pass (section 1), point pass (section 2)
 template <int S>
 __device__ __forceinline__ void adj_level_section(const BatchArgs& a, int d) {
     if (S == 1) {
@@ -461,9 +469,19 @@ k_batch_adjoint(BatchArgs a, int d) {
         adj_cage_section<3>(a);
         return;
     }
+    if (d >= 2) {
+        adj_level_step(a, d);
+        return;
+    }
     adj_level_section<1>(a, d);
     if (!grid_sync(a.sync, a.spinCap, gridDim.x)) return;
     adj_level_section<2>(a, d);
+}
+
+// split schedule, adjoint, depth d >= 2: the one-pass step on its own register budget
+__global__ void __launch_bounds__(kBatchBlock, 5)
+k_batch_adj_step(BatchArgs a, int d) {
+    adj_level_step(a, d);
 }
 
 // split schedule: one ordinary launch per section (kernel boundaries order them)
@@ -816,6 +834,8 @@ static cudaError_t enqueue_batch(ccs_Batch* b, int op, bool creased) {
                     e = launch_persistent(b, k_batch_adjoint_section<SEC_CAGE_2>, max_tiles(b, 0, {PH_ADJ_FACE}), a, 0, false);
                 if (e == cudaSuccess)
                     e = launch_persistent(b, k_batch_adjoint_section<SEC_CAGE_3>, max_tiles(b, 0, {PH_ADJ_VERT}), a, 0, false);
+            } else if (d >= 2) {
+                e = launch_persistent(b, k_batch_adj_step, max_tiles(b, d, {PH_ADJ_VERT}), a, d, false);
             } else {
                 e = launch_persistent(b, k_batch_adjoint_section<SEC_LEVEL_1>, max_tiles(b, d, {PH_ADJ_EDGE}), a, d, false);
                 if (e == cudaSuccess)
