@@ -1,42 +1,42 @@
-// ccs_level.cu -- fused refinement step for quad levels (depth d >= 1).
+// ccs_level.cu -- refinement steps for quad levels (depth d >= 1).
 //
-// One step d -> d+1 runs as kernel A then a vertex pass:
+// Default pass, depth d >= 2: one launch per step, k_level_ab
+// (tile_level_ab in ccs_tiles.cuh; one thread per parent halfedge, the 4
+// lanes of a face adjacent, a parent quad's 16 children in a 16-lane group):
+//   - every load that needs only the record (one 16-byte load) is issued
+//     first: the vertex point, crease sharpness, the older vertex's ring
+//     statistics, across a parent edge the twin quad's two other vertices;
+//   - face point of its face (quad shuffles, halfedge order), stored by the
+//     face's first lane;
+//   - edge point of its edge by both halves (the twin face from a sibling
+//     quad's lanes inside the parent quad, else rebuilt), stored by the
+//     pair's larger halfedge -- the owner's value bit for bit;
+//   - its vertex share: ring statistics from the structure (face centre,
+//     edge midpoint) or the per-level table of older vertices; a face
+//     centre's four shares summed in the warp and stored, the others by float
+//     atomics into slots the previous step cleared; it clears the slots of
+//     the next step;
+//   - the 4 child records (+ UV codes) through a 16 KB shared tile and one
+//     TMA store per block (a tensor store from a 128-byte swizzled tile when
+//     the level's tensor map exists, else a bulk store; no multicast);
+//   - extra blocks refine the creases and add the next level's crease
+//     statistics.
+// Depth 1 (children of n-gons, no 16-lane structure), cages without kept
+// statistics, and the deterministic pass run the step as kernel A
+// (k_level_a: records, face and edge points, clearing) then a vertex pass:
+//   default (k_level_b): the vertex shares as above, read back from memory;
+//   deterministic (CCS_FLAG_DETERMINISTIC): every vertex summed by one thread
+//      in increasing halfedge order, the reference's one-thread order --
+//      bit-identical points.  Depth >= 2: k_level_v (one thread per older
+//      vertex, one ring walk, on a second stream) beside k_level_b_exact
+//      (face centres in the warp, edge midpoints by the parent pair's owner
+//      with the twin side's shares rebuilt).  Depth 1: k_vertex_det.
 //
-//   A  (one thread per parent halfedge; the 4 lanes of a face are adjacent)
-//      - reads the parent record with one 16-byte load (a warp reads 512
-//        contiguous bytes); the face's other records come from the 3 sibling
-//        lanes through shuffles;
-//      - builds the 4 child records (topology + UV code) in shared memory;
-//        one thread then writes the block's 16 KB tile with a single
-//        cp.async.bulk store (TMA engine, no multicast);
-//      - face point of its face (lanes' vertex points combined by shuffles,
-//        in halfedge order), stored by the face's first lane;
-//      - edge point of its edge, computed and stored by the pair's larger
-//        halfedge: both halves of the edge rule, the twin face's point
-//        rebuilt from the twin quad's four records (the same value, bit for
-//        bit, as the twin quad's lanes store);
-//      - clears the vertex slots the default vertex pass accumulates into;
-//      - extra blocks refine the creases of the level.
-//   Vertex pass, default (k_level_b, one thread per halfedge): the vertex
-//      share of its halfedge with ring statistics from the refined structure
-//      (face centres, edge midpoints) or from the per-level table of the
-//      older vertices' statistics (k_shape_stats + k_crease_stats, built
-//      with the topology);
-//      a face centre's shares are summed in the warp and stored, the other
-//      shares go out as float atomics (pairs combined in the warp first).
-//   Vertex pass, deterministic (CCS_FLAG_DETERMINISTIC): every vertex summed
-//      by one thread in increasing halfedge order, which is the reference's
-//      one-thread order -- bit-identical points.  Depth >= 2: k_level_v (one
-//      thread per older vertex, one ring walk, on a second stream) beside
-//      k_level_b_exact (face centres in the warp, edge midpoints by the
-//      parent pair's owner with the twin side's shares rebuilt).  Depth 1:
-//      k_vertex_det (one thread per vertex, sorted ring).
-//
-// Kernel A and the exact pass evaluate every float expression in the
-// reference's order; topology, creases, UVs, face and edge points are
+// Face and edge points are evaluated in the reference's operation order in
+// every kernel; topology, creases, UVs, face and edge points are
 // bit-identical to the reference in both modes.
 //
-// Twin relation used by A: for a twin pair (h, t), vertex(t) = vertex(next h)
+// Twin relation used here: for a twin pair (h, t), vertex(t) = vertex(next h)
 // and vertex(next t) = vertex(h).  The C ABI checks this on the cage (it is
 // then preserved by every refinement step) and uses the unfused kernels for
 // cages that break it.
