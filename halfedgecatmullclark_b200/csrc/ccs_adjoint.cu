@@ -129,14 +129,25 @@ static void adjoint_level(const Ctx& c, const View& L, float* gNew, float* gOld)
     c.prof->end(c.stream);
 }
 
+// The levels' gradients start as the caller's and accumulate in `work`.  The
+// finest level's are only read, and when its step runs the one-pass kernel
+// (which reads its input gradients only) they are read where the caller
+// holds them: only depths 1..D-1 are copied.
 cudaError_t run_adjoint(const Ctx& c, const float* gradPts, float* work, float* gradCage, int64_t cumV) {
-    cudaError_t st = cudaMemcpyAsync(work, gradPts, sizeof(float) * 3 * (size_t)cumV,
+#ifndef CCS_NO_ADJ_STEP
+    const bool finestInPlace = c.fusable && c.D - 1 >= 2 && stats_at(c, c.D - 1) != nullptr;
+#else
+    const bool finestInPlace = false;
+#endif
+    const int64_t copyV = finestInPlace ? c.lv[c.D].ptOff : cumV;
+    cudaError_t st = cudaMemcpyAsync(work, gradPts, sizeof(float) * 3 * (size_t)copyV,
                                      cudaMemcpyDeviceToDevice, c.stream);
     if (st != cudaSuccess) return st;
     st = cudaMemsetAsync(gradCage, 0, sizeof(float) * 3 * (size_t)c.cage->V, c.stream);
     if (st != cudaSuccess) return st;
     for (int d = c.D - 1; d >= 0; --d) {
-        float* gNew = work + 3 * c.lv[d + 1].ptOff;
+        float* gNew = (finestInPlace && d == c.D - 1) ? const_cast<float*>(gradPts) + 3 * c.lv[d + 1].ptOff
+                                                      : work + 3 * c.lv[d + 1].ptOff;
         if (d == 0) {
             CageView L;
             L.t = cage_tables_a(*c.cage);
