@@ -53,25 +53,33 @@ def parse():
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--depth", type=int, default=6)
+    p.add_argument("--depth", type=int, default=None,
+                   help="refinement depth (default: 6 for mixed_torus, 5 for height_grid)")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--e2e-steps", type=int, default=5)
     p.add_argument("--deterministic", action="store_true")
-    p.add_argument("--workload", default="mixed_torus", choices=["mixed_torus", "batch"],
-                   help="mixed_torus: the headline single-mesh refine; batch: 512 uneven cages, "
-                        "forward + adjoint, batched vs a loop of single-mesh calls")
+    p.add_argument("--workload", default="mixed_torus", choices=["mixed_torus", "height_grid", "batch"],
+                   help="mixed_torus: the headline single-mesh refine (64x64 mixed-valence torus, "
+                        "depth 6); height_grid: the large plain refine (256x256 height-field grid, "
+                        "depth 5, per-level GB/s); batch: 512 uneven cages, forward + adjoint, "
+                        "batched vs a loop of single-mesh calls")
     p.add_argument("--batch-count", type=int, default=512)
     return p.parse_args()
 
 
-def workload(depth):
+def workload(args):
     from halfedgecatmullclark_b200 import configs
-    return configs.mixed_torus(depth=depth)
+    if args.workload == "height_grid":
+        return configs.height_grid(depth=5 if args.depth is None else args.depth)
+    return configs.mixed_torus(depth=6 if args.depth is None else args.depth)
+
+
+WORKLOAD_NAMES = {"mixed_torus": "mixed_torus_64x64_depth%d", "height_grid": "height_grid_256x256_depth%d"}
 
 
 def config_dict(w, extra=None):
-    c = {"workload": "mixed_torus_64x64_depth%d" % w.depth, "cage_halfedges": w.cage.H,
+    c = {"workload": WORKLOAD_NAMES.get(w.name, w.name + "_depth%d") % w.depth, "cage_halfedges": w.cage.H,
          "cage_faces": w.cage.F, "depth": w.depth, "uv": w.cage.U > 0,
          "crease_edges": w.notes.get("crease_edges"), "l2": "flushed (256 MB write) between timed steps"}
     if extra:
@@ -213,7 +221,7 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    w = workload(args.depth)
+    w = workload(args)
     from oracle import refimpl
     from halfedgecatmullclark_b200 import metrics
     from halfedgecatmullclark_b200.subd import level_counts
@@ -481,7 +489,7 @@ def main():
     from halfedgecatmullclark_b200.subd import Subd
 
     rank, world = dist_init()
-    w = workload(args.depth)
+    w = workload(args)
     flags = N.FLAG_DETERMINISTIC if args.deterministic else 0
     subd = Subd(w.cage, w.depth, flags)
     stream = torch.cuda.Stream()

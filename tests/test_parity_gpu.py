@@ -240,3 +240,47 @@ def test_mixed_torus_depth6_properties():
         dpts = s.points()
     assert np.array_equal(dpts[:o32.shape[0]].view(np.uint32), o32.view(np.uint32))
     assert rel_err(dpts, pts) <= TOL_POINTS
+
+
+@pytest.mark.slow
+def test_height_grid_depth5_properties():
+    """Config 3 at full size (256x256 height-field grid with diagonal splits
+    and creases, depth 5: 393 M refined halfedges, 6.3 GB of records), checked
+    on the device arrays: twins an involution and vertex ids in range at
+    every level, finite points; the first three levels equal to the oracle
+    (topology and creases bit-exact, default points within 1e-5, the
+    deterministic pass bit for bit)."""
+    import torch
+    from halfedgecatmullclark_b200 import _native as N
+    from halfedgecatmullclark_b200 import configs
+    from halfedgecatmullclark_b200.subd import Subd
+    from oracle import oracle
+    w = configs.height_grid()
+    assert w.depth == 5
+    ohe, ocr = oracle.refine_topology(w.cage, 3)
+    o32 = oracle.refine_points(w.cage, 3, ohe, ocr, "scatter", np.float32)
+    cnt = oracle.counts(w.cage, w.depth)
+    for flags in (N.FLAG_PAGEABLE_HOST, N.FLAG_PAGEABLE_HOST | N.FLAG_DETERMINISTIC):
+        with Subd(w.cage, w.depth, flags) as s:
+            s.refine_scatter()
+            s.synchronize()
+            arr = s.device_arrays()
+            he, cr, pts = arr["halfedges"], arr["creases"], arr["points"]
+            assert he.shape[0] == cnt["cumH"][w.depth]
+            for d in range(1, w.depth + 1):
+                lv = he[s.level_slice(d, "H")]
+                tw = lv[:, 0].long()
+                ok = tw >= 0
+                assert torch.equal(lv[tw[ok], 0].long(), torch.nonzero(ok).squeeze(1))
+                assert int(lv[:, 2].min()) >= 0 and int(lv[:, 2].max()) < cnt["V"][d]
+                del tw, ok
+            assert bool(torch.isfinite(pts).all())
+            n = ohe.shape[0]
+            assert np.array_equal(he[:n, :3].cpu().numpy(), ohe[:, :3])
+            assert np.array_equal(cr[:ocr.shape[0]].cpu().numpy().view(np.uint8).reshape(-1),
+                                  ocr.view(np.uint8).reshape(-1))
+            p = pts[:o32.shape[0]].cpu().numpy()
+            if flags & N.FLAG_DETERMINISTIC:
+                assert np.array_equal(p.view(np.uint32), o32.view(np.uint32))
+            else:
+                assert rel_err(p, o32) <= TOL_POINTS
