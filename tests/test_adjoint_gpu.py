@@ -219,3 +219,22 @@ def test_one_pass_adjoint_boundary_crease_branch():
     he, cr = oracle.refine_topology(cage, depth)
     ref = oracle.adjoint(cage, depth, he, cr, g.double().cpu().numpy())
     assert rel_err(x.grad.cpu().numpy(), ref) <= 1e-5
+
+
+@pytest.mark.slow
+def test_fitting_cage_depth5_adjoint():
+    """Config 4 at its full depth (2000-face mixed cage, depth 5): the CUDA
+    adjoint of a random gradient against the FP64 oracle adjoint."""
+    import torch
+    from halfedgecatmullclark_b200 import configs
+    from halfedgecatmullclark_b200.torch_ext import RefinePoints
+    from oracle import oracle
+    w = configs.fitting_cage(depth=5)
+    s = surface(w)
+    x = torch.tensor(w.cage.vertex_points, device="cuda", requires_grad=True)
+    pts = RefinePoints.apply(x, s.subd)
+    g = torch.randn(pts.shape, device="cuda", generator=torch.Generator("cuda").manual_seed(5))
+    pts.backward(g)
+    he, cr = oracle.refine_topology(w.cage, w.depth)
+    ref = oracle.adjoint(w.cage, w.depth, he, cr, g.double().cpu().numpy())
+    assert rel_err(x.grad.cpu().numpy(), ref) <= 1e-5
