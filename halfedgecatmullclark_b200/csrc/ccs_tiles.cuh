@@ -489,12 +489,15 @@ __device__ __forceinline__ void tile_level_b(const QuadView<RW>& L, const float*
 // and the ring statistics; only the last come from memory (the older
 // vertices' table `ostats`; face centres and edge midpoints from the
 // structure).  So every halfedge evaluates its own edge point, not only the
-// pair's owner.  The twin face of an edge interior to a parent quad (child 1
-// or 2, whose twin is child 2 or 1 of a sibling quad in the same 16-lane
-// group) is read from that quad's lanes; across a parent edge (children 0
-// and 3) it is rebuilt from the twin quad's records as kernel A does.  Both
-// halves evaluate (0 + share(smaller halfedge)) + share(larger halfedge), so
-// both hold the owner's value bit for bit; the owner stores it.
+// pair's owner.  At depth d >= 2 the twin of child 1 or 2 is child 2 or 1 of
+// a sibling quad in the same 16-lane group, whose face point is read from
+// that quad's lanes; the twin of child 0 is child 3 of its quad and the twin
+// of child 3 is child 0 (CatmullClark.h:2778-2781), and that quad's face
+// point is rebuilt: its vertices are vertex(h) and vertex(next h) (the twin
+// relation) and the two others, read from its records, summed in its
+// halfedge order.  Both halves evaluate (0 + share(smaller halfedge)) +
+// share(larger halfedge), so both hold the owner's value bit for bit; the
+// owner stores it.
 // The vertex slots [0, V) of depth d+1 must be zero on entry; the tile also
 // clears its share of `zeroNext` (the slots the next level accumulates into).
 // Requires BLOCK a multiple of 32 and h0 a multiple of 16.
@@ -532,15 +535,14 @@ __device__ __forceinline__ void tile_level_ab(const LevelArgs& a, int64_t h0, in
         sOther = eo < a.C ? a.crIn[eo].sharpness : 0.0f;
     }
     const float4 st = (valid && k == 0) ? a.ostats[vx] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    // the twin quad's two vertices other than vertex(h) and vertex(next h)
-    const int32_t kt = tw & 3;
-    f3 qa = zero3(), qc = zero3();
+    // the twin quad's two vertices other than vertex(h) and vertex(next h):
+    // qF at position 2, qX at position 1 (child 0's twin) or 3 (child 3's)
+    f3 qF = zero3(), qX = zero3();
     if (gatherTwin) {
-        const int32_t tb = tw & ~3;
-        const int32_t va = __ldg(a.in + (int64_t)RW * (tb + ((kt + 2) & 3)) + 2);
-        const int32_t vc = __ldg(a.in + (int64_t)RW * (tb + ((kt + 3) & 3)) + 2);
-        qa = ld3(a.pin + 3 * (int64_t)va);
-        qc = ld3(a.pin + 3 * (int64_t)vc);
+        const int32_t vX = __ldg(a.in + (int64_t)RW * ((tw & ~3) + (k == 0 ? 1 : 3)) + 2);
+        const int32_t vF = __ldg(a.in + (int64_t)RW * ((tw & ~3) + 2) + 2);
+        qF = ld3(a.pin + 3 * (int64_t)vF);
+        qX = ld3(a.pin + 3 * (int64_t)vX);
     }
 
     // face point, and the next vertex's point from its shuffles
@@ -556,13 +558,11 @@ __device__ __forceinline__ void tile_level_ab(const LevelArgs& a, int64_t h0, in
         if (tw >= 0) {
             f3 Ft;
             if (gatherTwin) {
-                // twin quad positions kt, kt+1, kt+2, kt+3 hold vertex(next h),
-                // vertex(h), qa, qc (the twin relation); sum in position order
-                f3 r0 = pn, r1 = p, r2 = qa, r3 = qc;         // r_i at position (kt + i) & 3
-                // rotate so that r_i sits at position i
-                if (kt & 1) { const f3 x = r3; r3 = r2; r2 = r1; r1 = r0; r0 = x; }
-                if (kt & 2) { f3 x = r0; r0 = r2; r2 = x; x = r1; r1 = r3; r3 = x; }
-                Ft = add3(add3(add3(add3(zero3(), quarter3(r0)), quarter3(r1)), quarter3(r2)), quarter3(r3));
+                // the twin quad in position order: child 0's twin quad
+                // (v(h), qX, qF, v(next h)), child 3's (v(next h), v(h), qF, qX)
+                const f3 p4 = quarter3(p), pn4 = quarter3(pn), qX4 = quarter3(qX), qF4 = quarter3(qF);
+                const bool c0 = k == 0;
+                Ft = add3(add3(add3(add3(zero3(), c0 ? p4 : pn4), c0 ? qX4 : p4), qF4), c0 ? pn4 : qX4);
             } else {
                 Ft = Fsib;
             }
@@ -1581,7 +1581,9 @@ __device__ __forceinline__ void adj_quad_point_tile(const QuadView<RW>& L, const
 // then pass 2's vertex terms follow in the same thread.
 //   gEt[e(h)] = gE[e] + cE(h) gV[v(h)] + dE(next h) gV[v(next h)]      (own side)
 //                     + cE(t) gV[v(t)] + dE(next t) gV[v(next t)]      (twin t)
-// with v(t) = v(next h), v(next t) = v(h).  The twin side:
+// with v(t) = v(next h), v(next t) = v(h).  The twin side (at depth >= 2 the
+// twins of children 0, 1, 2, 3 of g are children 3, 2, 1, 0:
+// CatmullClark.h:2778-2781):
 //   * inside the parent quad (children 1, 2): the twin lane's own side;
 //   * across a parent edge, child 0 of g (twin t = child 3 of next(twin g)):
 //     cE(t) at the parent edge's midpoint, an interior vertex of valence 4
@@ -1591,8 +1593,11 @@ __device__ __forceinline__ void adj_quad_point_tile(const QuadView<RW>& L, const
 //   * child 3 of g (twin t = child 0 of twin(prev g)): cE(t) at the older
 //     vertex v(next h) (its statistics from the quad's child-0 lane, the
 //     boundary correction with t's edge, which is h's); dE(next t) = 0, at
-//     the interior midpoint of prev(g)'s edge;
-//   * anything else: the coefficients by ring walks (vertex_coef).
+//     the interior midpoint of prev(g)'s edge.
+// The vertex coefficients are lane_vertex_coef's with the statistics it
+// would read taken from the lanes: child 2 sits at a face centre (valence 4),
+// children 1 and 3 at edge midpoints whose creased edges are the halves of
+// one parent edge, child 0 at an older vertex (its statistics).
 // Both halves of an edge evaluate the same terms; gE is read, not written.
 template <int RW>
 __device__ __forceinline__ void adj_quad_step_tile(const QuadView<RW>& L, const float* __restrict__ gNew,
@@ -1618,14 +1623,31 @@ __device__ __forceinline__ void adj_quad_step_tile(const QuadView<RW>& L, const 
         if (k == 0) {
             gf = ld3(gF + 3 * (int64_t)(h >> 2));
             st = L.ostats[vx];
-            sOther = L.sharp(ed ^ 1);
         }
     }
     const int32_t ped = __shfl_sync(full, ed, lp), ptw = __shfl_sync(full, tw, lp);
+    // the other half of the parent edge at this lane's vertex (k = 0, 1, 3)
+    if (valid && k != 2) sOther = L.sharp((k == 1 ? ped : ed) ^ 1);
+    const float sPrev = __shfl_sync(full, sOwn, lp);
     VCoef kc{0.0f, 0.0f, 0.0f, 0.0f};
     ECoef ke{0.0f, 0.0f, 0.0f};
     if (valid) {
-        kc = lane_vertex_coef(L, h, tw, ed, ptw, ped, st);
+        float vp = 4.0f, cpre = 0.0f, avgS = 0.0f;
+        bool bnd = false;
+        if (k == 0) {
+            bnd = st.w != 0.0f;
+            vp = st.x;
+            avgS = bnd ? st.y - sOwn : st.y;
+            cpre = bnd ? st.z - fsign(sOwn) : st.z;
+        } else if (k != 2) {
+            const float sa = k == 1 ? sPrev : sOwn;   // this side's half of the parent edge
+            const bool own = k == 3;                  // the walk from h skips its own edge
+            bnd = (k == 1 ? ptw : tw) < 0;
+            vp = bnd ? 2.0f : 4.0f;
+            avgS = (bnd && own) ? sOther : sa + sOther;
+            cpre = (bnd && own) ? fsign(sOther) : fsign(sa) + fsign(sOther);
+        }
+        kc = coef_from_stats(vp, cpre, avgS, bnd, fsign(sOwn), fsign(sPrev));
         const float w = fsat(sOwn), b = tw < 0 ? 1.0f : 0.5f;    // edge_coef
         ke.al = (1.0f - w) * 0.25f + w * b * 0.5f;
         ke.be = w * b * 0.5f;
@@ -1641,10 +1663,9 @@ __device__ __forceinline__ void adj_quad_step_tile(const QuadView<RW>& L, const 
     const f3 ownSib = shfl3(own, (lane & ~15) | sibK);
     f3 twinSide = zero3();
     if (valid && tw >= 0) {
-        const int kt = tw & 3;
-        if ((k == 1 || k == 2) && tw == ((h & ~15) | sibK)) {
+        if (k == 1 || k == 2) {
             twinSide = ownSib;
-        } else if (k == 0 && kt == 3) {
+        } else if (k == 0) {
             // cE(t) at the midpoint (interior, valence 4)
             const VCoef ct = coef_from_stats(4.0f, fsign(sOwn) + fsign(sOther), sOwn + sOther, false, fsign(sOwn), 0.0f);
             // dE(next t) at the older vertex v(h) = this lane's
@@ -1658,16 +1679,13 @@ __device__ __forceinline__ void adj_quad_step_tile(const QuadView<RW>& L, const 
                 dEt = t * 0.25f * fsign(sOwn);
             }
             twinSide = add3(mul3(gn, ct.cE), mul3(gv, dEt));
-        } else if (k == 3 && kt == 0) {
+        } else {
             // cE(t) at the older vertex v(next h), seen from t (its edge is h's)
             const bool bnd = sq.w != 0.0f;
             const float avgS = bnd ? sq.y - sOwn : sq.y;
             const float cpre = bnd ? sq.z - fsign(sOwn) : sq.z;
             const VCoef ct = coef_from_stats(sq.x, cpre, avgS, bnd, fsign(sOwn), 0.0f);
             twinSide = mul3(gn, ct.cE);
-        } else {
-            const VCoef a = vertex_coef(L, tw), an = vertex_coef(L, qnext(tw));
-            twinSide = add3(mul3(gn, a.cE), mul3(gv, an.dE));
         }
     }
     const f3 gEt = add3(add3(ge, own), twinSide);
