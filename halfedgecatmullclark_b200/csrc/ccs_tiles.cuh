@@ -1656,9 +1656,16 @@ __device__ __forceinline__ void adj_quad_step_tile(const QuadView<RW>& L, const 
     const float dEn = __shfl_sync(full, kc.dE, ln);
     const f3 gn = shfl3(gv, ln);
     const f3 own = add3(mul3(gv, kc.cE), mul3(gn, dEn));
-    // the older vertex's statistics of the quad (its child-0 lane)
-    const float4 sq = make_float4(__shfl_sync(full, st.x, qb), __shfl_sync(full, st.y, qb),
-                                  __shfl_sync(full, st.z, qb), __shfl_sync(full, st.w, qb));
+    // child 3's twin coefficient cE(t) at the quad's older vertex, evaluated in
+    // the child-0 lane (its statistics; child 3's sharpness is its sPrev)
+    float cB = 0.0f;
+    if (valid && k == 0) {
+        const bool bnd = st.w != 0.0f;
+        const float avgS = bnd ? st.y - sPrev : st.y;
+        const float cpre = bnd ? st.z - fsign(sPrev) : st.z;
+        cB = coef_from_stats(st.x, cpre, avgS, bnd, fsign(sPrev), 0.0f).cE;
+    }
+    cB = __shfl_sync(full, cB, qb);
     const int sibK = k == 1 ? ((((j + 1) & 3) << 2) | 2) : ((((j + 3) & 3) << 2) | 1);
     const f3 ownSib = shfl3(own, (lane & ~15) | sibK);
     f3 twinSide = zero3();
@@ -1681,11 +1688,7 @@ __device__ __forceinline__ void adj_quad_step_tile(const QuadView<RW>& L, const 
             twinSide = add3(mul3(gn, ct.cE), mul3(gv, dEt));
         } else {
             // cE(t) at the older vertex v(next h), seen from t (its edge is h's)
-            const bool bnd = sq.w != 0.0f;
-            const float avgS = bnd ? sq.y - sOwn : sq.y;
-            const float cpre = bnd ? sq.z - fsign(sOwn) : sq.z;
-            const VCoef ct = coef_from_stats(sq.x, cpre, avgS, bnd, fsign(sOwn), 0.0f);
-            twinSide = mul3(gn, ct.cE);
+            twinSide = mul3(gn, cB);
         }
     }
     const f3 gEt = add3(add3(ge, own), twinSide);
