@@ -87,6 +87,14 @@ __device__ __forceinline__ f3 quad_face_point(f3 p, int qb) {
     return acc;
 }
 
+// The same face point from the lanes' quartered points p4 = p / 4 (x / 4 is
+// exact, so shuffling quarters gives the same terms): fewer instructions,
+// which the points-only step (issue-bound) gains from and the step with the
+// topology (bound by its dependent loads) measured slower with.
+__device__ __forceinline__ f3 quad_face_point4(f3 p4, int qb) {
+    const f3 q0 = shfl3(p4, qb), q1 = shfl3(p4, qb + 1), q2 = shfl3(p4, qb + 2), q3 = shfl3(p4, qb + 3);
+    return add3(add3(add3(add3(zero3(), q0), q1), q2), q3);
+}
 // The same face point, and in `pn` the point of the next lane of the quad
 // (taken from the face point's shuffles, none of its own).
 __device__ __forceinline__ f3 quad_face_point_next(f3 p, int qb, int k, f3& pn) {
@@ -546,8 +554,13 @@ __device__ __forceinline__ void tile_level_ab(const LevelArgs& a, int64_t h0, in
     }
 
     // face point, and the next vertex's point from its shuffles
-    f3 pn;
-    const f3 Fp = quad_face_point_next(p, qb, k, pn);
+    f3 pn, Fp;
+    if constexpr (TOPO) {
+        Fp = quad_face_point_next(p, qb, k, pn);
+    } else {
+        Fp = quad_face_point4(quarter3(p), qb);
+        pn = shfl3(p, ln);
+    }
     if (valid && k == 0) st3(a.pout + 3 * ((int64_t)a.V + f), Fp);
     const f3 Fsib = shfl3(Fp, (lane & ~15) | sibK);      // a sibling quad's face point
     // edge point of h's edge, by both halves
@@ -567,7 +580,11 @@ __device__ __forceinline__ void tile_level_ab(const LevelArgs& a, int64_t h0, in
                 Ft = Fsib;
             }
             const f3 sh_t = edge_share_fast<CREASED>(pn, p, Ft, false, w);
-            E = h > tw ? add3(add3(zero3(), sh_t), sh_h) : add3(add3(zero3(), sh_h), sh_t);
+            // (0 + a) + b and (0 + b) + a are the same float (x + y = y + x;
+            // 0 + x differs from x only for x = -0, which both orders turn
+            // into +0), so the points-only step skips the owner-order select
+            if constexpr (TOPO) E = h > tw ? add3(add3(zero3(), sh_t), sh_h) : add3(add3(zero3(), sh_h), sh_t);
+            else E = add3(add3(zero3(), sh_h), sh_t);
         } else {
             E = add3(zero3(), sh_h);
         }
