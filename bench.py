@@ -91,16 +91,57 @@ def config_dict(w, extra=None):
 # clocks sampled during the timed region
 # ---------------------------------------------------------------------------
 class ClockSampler:
+    """SM clock, power and clock-event reasons of this process's GPU, sampled
+    while the timed region runs: NVML read every 2 ms on a thread (nothing is
+    set), else `nvidia-smi -lms 200`."""
     QUERY = ("index,uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits
+    REASON_BITS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
+                   "sw_power_cap": 0x4}
 
     def __init__(self, uuid=None):
         self.uuid = uuid
         self.proc = None
         self.path = None
+        self.thread = None
+        self.rows = []
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        if self.uuid:
+            want = self.uuid.lower().replace("gpu-", "")
+            for i in range(pynvml.nvmlDeviceGetCount()):
+                h = pynvml.nvmlDeviceGetHandleByIndex(i)
+                u = pynvml.nvmlDeviceGetUUID(h)
+                u = (u.decode() if isinstance(u, bytes) else u).lower().replace("gpu-", "")
+                if u == want:
+                    return pynvml, h
+        return pynvml, pynvml.nvmlDeviceGetHandleByIndex(0)
 
     def start(self):
+        try:
+            import threading
+            nv, h = self._nvml_handle()
+            self.smax = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self.stop_flag = threading.Event()
+
+            def run():
+                while not self.stop_flag.is_set():
+                    try:
+                        self.rows.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
+                                          nv.nvmlDeviceGetPowerUsage(h) / 1000.0,
+                                          int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))))
+                    except Exception:
+                        break
+                    time.sleep(0.002)
+            self.thread = threading.Thread(target=run, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.thread = None
         try:
             fd, self.path = tempfile.mkstemp(suffix=".csv")
             os.close(fd)
@@ -111,7 +152,21 @@ class ClockSampler:
         except Exception:
             self.proc = None
 
+    def _stop_nvml(self):
+        self.stop_flag.set()
+        self.thread.join(timeout=5)
+        rows = self.rows
+        if not rows:
+            return None
+        pmax = max(r[1] for r in rows)
+        load = [r[0] for r in rows if r[1] > 0.35 * pmax] or [r[0] for r in rows]
+        reasons = sorted({n for r in rows for n, bit in self.REASON_BITS.items() if r[2] & bit})
+        return {"sm_mhz": statistics.median(load), "sm_max_mhz": self.smax, "reasons": reasons,
+                "samples": len(rows), "power_w_max": pmax, "source": "nvml, 2 ms"}
+
     def stop(self):
+        if self.thread is not None:
+            return self._stop_nvml()
         if self.proc is None:
             return None
         self.proc.terminate()
@@ -152,7 +207,7 @@ class ClockSampler:
         reasons = sorted({names[k] for r in rs for k in range(4) if "Active" in r[6 + k] and "Not" not in r[6 + k]})
         return {"sm_mhz": statistics.median(load) if load else None,
                 "sm_max_mhz": max(smax) if smax else None, "reasons": reasons,
-                "samples": len(rs), "power_w_max": pmax}
+                "samples": len(rs), "power_w_max": pmax, "source": "nvidia-smi, 200 ms"}
 
 
 def measured_peak():
@@ -429,12 +484,20 @@ def run_batch_workload(args):
             batch_step()
     bt.synchronize()
     barrier(world)
+    uuid = None
+    try:
+        uuid = str(torch.cuda.get_device_properties(torch.cuda.current_device()).uuid)
+    except Exception:
+        pass
+    sampler = ClockSampler(uuid)
+    sampler.start()
     with torch.cuda.stream(stream):
         a.record(stream)
         for _ in range(steps):
             batch_step()
         b.record(stream)
     bt.synchronize()
+    clocks = sampler.stop()
     batch_ms = shard.max_over_ranks(a.elapsed_time(b) / steps, world)
     # gradients of the last full step (the adjoint consumes its input, so
     # before the halves are timed alone)
@@ -472,7 +535,7 @@ def run_batch_workload(args):
                      "how": "Python loop of ccs_RefinePointsDevice_cuda + ccs_AdjointPointsDevice_cuda per cage"},
             "speedup_vs_loop": loop_ms / batch_ms, "topology_refine_ms": topo_ms,
             "forward_ms": parts["forward_ms"], "adjoint_ms": parts["adjoint_ms"],
-            "grad_agreement_rel": agree}
+            "grad_agreement_rel": agree, "clocks": clocks}
     print(json.dumps(line))
     return 0
 
@@ -527,6 +590,7 @@ def main():
     barrier(world)
     torch.cuda.synchronize()
     wall = time.perf_counter() - t_wall
+    clocks = sampler.stop()
     step_ms = [a.elapsed_time(b) for a, b in evs]
     total_ms = max_over_ranks(sum(step_ms), world)
 
@@ -538,7 +602,6 @@ def main():
             subd.refine_scatter()
     recs = subd.read_profile(1 << 16)
     subd.set_profiling(False)
-    clocks = sampler.stop()
 
     value = world * SH * args.steps / (total_ms / 1e3)
     rec_bytes = 16 if subd.record_words == 4 else 12
