@@ -244,18 +244,30 @@ def cpu_reference(w, seconds, max_runs=20, min_runs=2):
         s = refimpl.RefSubd(w.cage, w.depth)
         times = []
         t_end = time.perf_counter() + seconds
+        passes = {}
         try:
             while len(times) < max_runs and (len(times) < min_runs or time.perf_counter() < t_end):
                 t0 = time.perf_counter()
                 s.refine("scatter")
                 times.append(time.perf_counter() - t0)
+            # its four passes one by one, as the reference's bench_cpu times them
+            # (examples/subd_cpu.c:220-261); three runs each, median
+            for name, fn in (("halfedges", "ccs_RefineHalfedges"), ("creases", "ccs_RefineCreases"),
+                             ("vertex_uvs", "ccs_RefineVertexUvs"),
+                             ("vertex_points", "ccs_RefineVertexPoints_Scatter")):
+                pt = []
+                for _ in range(3):
+                    t0 = time.perf_counter()
+                    s.call(fn)
+                    pt.append(time.perf_counter() - t0)
+                passes[name] = statistics.median(pt) * 1e3
         finally:
             s.close()
         med = statistics.median(times)
         return {"value": sh / med, "unit": UNIT, "cores": cores, "kind": "reference",
                 "sample": "%d runs of the reference ccs_Refine_Scatter on the full workload "
                           "(OpenMP %d threads), median %.1f ms" % (len(times), cores, med * 1e3),
-                "ms_per_step": med * 1e3}
+                "ms_per_step": med * 1e3, "passes_ms": passes}
     # the oracle port, single-threaded, on a smaller depth of the same cage
     from oracle import oracle
     d = max(1, w.depth - 2)
