@@ -78,19 +78,12 @@ __device__ __forceinline__ void atomic_add3(float* o, f3 v) {
     }
 }
 
-// Face point of the quad held by lanes qb..qb+3, in halfedge order:
-// ((0 + p0/4) + p1/4) + p2/4) + p3/4   (CatmullClark.h:2032-2052)
-__device__ __forceinline__ f3 quad_face_point(f3 p, int qb) {
-    f3 acc = zero3();
-#pragma unroll
-    for (int i = 0; i < 4; ++i) acc = add3(acc, quarter3(shfl3(p, qb + i)));
-    return acc;
-}
-
-// The same face point from the lanes' quartered points p4 = p / 4 (x / 4 is
-// exact, so shuffling quarters gives the same terms): fewer instructions,
-// which the points-only step (issue-bound) gains from and the step with the
-// topology (bound by its dependent loads) measured slower with.
+// Face point of the quad held by lanes qb..qb+3, in halfedge order,
+// ((0 + p0/4) + p1/4) + p2/4) + p3/4 (CatmullClark.h:2032-2052), from the
+// lanes' quartered points p4 = p / 4 (x / 4 is exact, so shuffling quarters
+// gives the same terms).  Fewer instructions than quad_face_point_next: the
+// points-only step (issue-bound) gains from it, the step with the topology
+// (bound by its dependent loads) measured slower with it.
 __device__ __forceinline__ f3 quad_face_point4(f3 p4, int qb) {
     const f3 q0 = shfl3(p4, qb), q1 = shfl3(p4, qb + 1), q2 = shfl3(p4, qb + 2), q3 = shfl3(p4, qb + 3);
     return add3(add3(add3(add3(zero3(), q0), q1), q2), q3);
@@ -1150,44 +1143,9 @@ __device__ __forceinline__ void vertex_det_item(const View& L, const float* __re
 // ---------------------------------------------------------------------------
 // adjoint of the creased scatter rule (see ccs_adjoint.cu): three gathers
 // ---------------------------------------------------------------------------
-// item = older vertex v < V(d-1) of quad level d: one walk of its ring,
-// {valence, summed sharpness and crease count of every incident edge,
-// boundary} for ring_from_stats.  The walk reads prev(x)'s record only:
-// edge(prev x) is the next member's edge, or on a boundary the last edge.
-template <int RW>
-__device__ __forceinline__ void ring_stats_item(const QuadView<RW>& L, float4* __restrict__ out, int32_t v) {
-    const int32_t h0 = L.vert_he(v);
-    float s = L.hsharp(h0);
-    float n = 1.0f, tot = s, cnt = fsign(s);
-    int32_t x = h0;
-    int guard = 0;
-    for (;;) {
-        const int32_t pr = qprev(x);
-        const int32_t e = L.edge(pr);
-        x = L.twin(pr);
-        if (x == h0 || ++guard >= kWalkCap) break;
-        s = L.sharp(e);
-        tot = fadd(tot, s);
-        cnt = fadd(cnt, fsign(s));
-        if (x < 0) break;
-        n = fadd(n, 1.0f);
-    }
-    const bool bnd = x < 0;
-    if (bnd) {
-        guard = 0;
-        for (int32_t b = L.twin(h0); b >= 0 && guard < kWalkCap; ++guard) {
-            const int32_t c = qnext(b);
-            s = L.hsharp(c);
-            n = fadd(n, 1.0f);
-            tot = fadd(tot, s);
-            cnt = fadd(cnt, fsign(s));
-            b = L.twin(c);
-        }
-    }
-    out[v] = make_float4(n, tot, cnt, bnd ? 1.0f : 0.0f);
-}
-
-// The same statistics without walking the level: the valence and boundary of
+// Ring statistics of an older vertex v < V(d-1) of quad level d, {valence,
+// summed sharpness and crease count of every incident edge, boundary} for
+// ring_from_stats, without walking the level: the valence and boundary of
 // an older vertex are those it was created with (refinement keeps a
 // vertex's ring), and its creased edges are found from the crease side.
 //
@@ -1483,10 +1441,8 @@ __device__ __forceinline__ void lane_record(const QuadView<RW>& L, int64_t h64, 
 }
 // Pass 1, tile of halfedges [h0, h0 + blockDim): each halfedge adds its
 // side's terms cE(h) gV[v(h)] + dE(next h) gV[v(next h)] to gE[e] (next h is
-// the quad's next lane) with one float atomic triple; with PAIR instead the
-// pair's larger halfedge completes gE[e] itself, recomputing the twin side's
-// coefficients (its vertices are v(next h) and v(h)).
-template <int RW, bool PAIR = false>
+// the quad's next lane) with one float atomic triple.
+template <int RW>
 __device__ __forceinline__ void adj_quad_edge_tile(const QuadView<RW>& L, float* __restrict__ gNew, int64_t h0) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31, k = lane & 3, qb = lane & ~3, ln = qb | ((k + 1) & 3);
@@ -1509,20 +1465,7 @@ __device__ __forceinline__ void adj_quad_edge_tile(const QuadView<RW>& L, float*
     if (valid) kc = lane_vertex_coef(L, h, tw, ed, ptw, ped, st);
     const float dEn = __shfl_sync(full, kc.dE, ln);
     const f3 gn = shfl3(g, ln);
-    if (!PAIR) {
-        if (valid) atomic_add3(gE + 3 * (int64_t)ed, add3(mul3(g, kc.cE), mul3(gn, dEn)));
-        return;
-    }
-    if (!valid || !(h > tw)) return;
-    f3 acc = add3(mul3(g, kc.cE), mul3(gn, dEn));
-    if (tw >= 0) {
-        const VCoef kt = vertex_coef(L, tw), ktn = vertex_coef(L, qnext(tw));
-        acc = add3(acc, add3(mul3(gn, kt.cE), mul3(g, ktn.dE)));
-    }
-    float* o = gE + 3 * (int64_t)ed;
-    o[0] += acc.x;
-    o[1] += acc.y;
-    o[2] += acc.z;
+    if (valid) atomic_add3(gE + 3 * (int64_t)ed, add3(mul3(g, kc.cE), mul3(gn, dEn)));
 }
 
 // Pass 2, tile of halfedges: the face's gradient gF[f] + sum over its
