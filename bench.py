@@ -21,6 +21,11 @@ Metric: refined halfedges per second (sum of H_d over depths 1..6 per step).
               sources into oracle/_ref, OpenMP on all host cores) on the same
               cage and depth, a bounded sample of runs.
 
+``--op points`` times ccs_RefineVertexPoints_Scatter_cuda on the refined
+topology instead (the call of an animation or fitting loop); its e2e moves
+the cage points in and the points of every depth out through the
+differentiable entry point, and its cpu_baseline is the reference's
+ccs_RefineVertexPoints_Scatter.
 ``--impl reference`` times only the reference CPU path (rank 0).
 Multi-GPU (torchrun): every rank refines its own replica of the cage (the
 single-mesh path does not shard); value = all ranks' halfedges / max time.
@@ -59,6 +64,10 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--e2e-steps", type=int, default=5)
     p.add_argument("--deterministic", action="store_true")
+    p.add_argument("--op", default="refine", choices=["refine", "points"],
+                   help="refine: ccs_Refine_Scatter_cuda (topology, creases, UVs, points); points: "
+                        "ccs_RefineVertexPoints_Scatter_cuda on a refined topology (the call of an "
+                        "animation or fitting loop)")
     p.add_argument("--workload", default="mixed_torus", choices=["mixed_torus", "height_grid", "batch"],
                    help="mixed_torus: the headline single-mesh refine (64x64 mixed-valence torus, "
                         "depth 6); height_grid: the large plain refine (256x256 height-field grid, "
@@ -233,7 +242,7 @@ def traffic_table():
 # ---------------------------------------------------------------------------
 # CPU baseline: the reference compiled from its sources (oracle/_ref)
 # ---------------------------------------------------------------------------
-def cpu_reference(w, seconds, max_runs=20, min_runs=2):
+def cpu_reference(w, seconds, max_runs=20, min_runs=2, op="refine"):
     from oracle import refimpl
     from halfedgecatmullclark_b200 import metrics
     from halfedgecatmullclark_b200.subd import level_counts
@@ -243,12 +252,17 @@ def cpu_reference(w, seconds, max_runs=20, min_runs=2):
         refimpl.set_threads(cores)
         s = refimpl.RefSubd(w.cage, w.depth)
         times = []
-        t_end = time.perf_counter() + seconds
         passes = {}
         try:
+            if op == "points":
+                s.refine("scatter")                     # the topology, untimed
+            t_end = time.perf_counter() + seconds
             while len(times) < max_runs and (len(times) < min_runs or time.perf_counter() < t_end):
                 t0 = time.perf_counter()
-                s.refine("scatter")
+                if op == "points":
+                    s.call("ccs_RefineVertexPoints_Scatter")
+                else:
+                    s.refine("scatter")
                 times.append(time.perf_counter() - t0)
             # its four passes one by one, as the reference's bench_cpu times them
             # (examples/subd_cpu.c:220-261); three runs each, median
@@ -265,8 +279,10 @@ def cpu_reference(w, seconds, max_runs=20, min_runs=2):
             s.close()
         med = statistics.median(times)
         return {"value": sh / med, "unit": UNIT, "cores": cores, "kind": "reference",
-                "sample": "%d runs of the reference ccs_Refine_Scatter on the full workload "
-                          "(OpenMP %d threads), median %.1f ms" % (len(times), cores, med * 1e3),
+                "sample": "%d runs of the reference %s on the full workload "
+                          "(OpenMP %d threads), median %.1f ms"
+                          % (len(times), "ccs_RefineVertexPoints_Scatter" if op == "points" else "ccs_Refine_Scatter",
+                             cores, med * 1e3),
                 "ms_per_step": med * 1e3, "passes_ms": passes}
     # the oracle port, single-threaded, on a smaller depth of the same cage
     from oracle import oracle
@@ -569,6 +585,12 @@ def main():
     subd = Subd(w.cage, w.depth, flags)
     stream = torch.cuda.Stream()
     subd.set_stream(stream)
+    points_op = args.op == "points"
+    if points_op:
+        def step():
+            subd.refine_vertex_points("scatter")
+    else:
+        step = subd.refine_scatter
     levels = subd.levels
     SH = metrics.total_halfedges(levels)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
@@ -579,8 +601,10 @@ def main():
         pass
 
     with torch.cuda.stream(stream):
+        if points_op:
+            subd.refine_scatter()              # the topology the points step needs, untimed
         for _ in range(max(3, args.warmup)):
-            subd.refine_scatter()
+            step()
     torch.cuda.synchronize()
     barrier(world)
     torch.cuda.synchronize()
@@ -595,7 +619,7 @@ def main():
             a = torch.cuda.Event(enable_timing=True)
             b = torch.cuda.Event(enable_timing=True)
             a.record(stream)
-            subd.refine_scatter()
+            step()
             b.record(stream)
             evs.append((a, b))
     torch.cuda.synchronize()
@@ -611,7 +635,7 @@ def main():
     with torch.cuda.stream(stream):
         for _ in range(args.steps):
             flush.zero_()
-            subd.refine_scatter()
+            step()
     recs = subd.read_profile(1 << 16)
     subd.set_profiling(False)
 
@@ -645,7 +669,8 @@ def main():
             ms = statistics.mean(steps_by[("step", d)])
         else:
             ms = sum(statistics.mean(v) for k, v in by.items() if k[1] == d)
-        nb = metrics.level_bytes(levels[d], levels[d + 1], rec_bytes, subd.record_words == 4, d == 0, w.cage.U)
+        nb = metrics.level_bytes(levels[d], levels[d + 1], rec_bytes, subd.record_words == 4, d == 0, w.cage.U,
+                                 topology=not points_op)
         per_depth.append({"depth": d + 1, "ms": ms, "refined_halfedges": levels[d + 1]["H"],
                           "halfedges_per_s": levels[d + 1]["H"] / (ms / 1e3), "alg_bytes": nb,
                           "gbs": nb / (ms / 1e3) / 1e9, "frac_of_peak": nb / (ms / 1e3) / 1e9 / peak})
@@ -658,25 +683,38 @@ def main():
     host_pts = torch.from_numpy(w.cage.vertex_points.copy()).pin_memory()
     e2e_ms = []
     torch.cuda.synchronize()
+    if points_op:
+        # the points of every depth from pinned cage points to pinned host
+        # memory through the differentiable entry point (RefinePointsDevice)
+        from halfedgecatmullclark_b200.torch_ext import refine_points
+        host_out = torch.empty((subd.cumV, 3), dtype=torch.float32).pin_memory()
     for _ in range(args.e2e_steps):
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
         a.record(stream)
-        subd.upload_cage_points(host_pts.numpy())
-        subd.refine_scatter()
-        subd.download()
+        if points_op:
+            with torch.cuda.stream(stream):
+                x = host_pts.to("cuda", non_blocking=True)
+                host_out.copy_(refine_points(x, subd), non_blocking=True)
+        else:
+            subd.upload_cage_points(host_pts.numpy())
+            subd.refine_scatter()
+            subd.download()
         b.record(stream)
         torch.cuda.synchronize()
         e2e_ms.append(a.elapsed_time(b))
     e2e_total = max_over_ranks(sum(e2e_ms), world)
     h2d = 12 * w.cage.V
-    d2h = 4 * subd.record_words * subd.cumH + 12 * subd.cumC + 12 * subd.cumV
+    if points_op:
+        d2h = 12 * subd.cumV
+    else:
+        d2h = 4 * subd.record_words * subd.cumH + 12 * subd.cumC + 12 * subd.cumV
     launches = len([r for r in recs if r["kernel"] not in ("clear", "step")]) // max(1, args.steps)
 
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            base = cpu_reference(w, args.cpu_seconds)
+            base = cpu_reference(w, args.cpu_seconds, op=args.op)
         except Exception as exc:  # a missing baseline must not hide the GPU number
             base = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "unavailable",
                     "sample": "error: %s" % exc}
@@ -687,7 +725,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": config_dict(w, {"parallelism": "replicas x%d" % world,
-                                      "deterministic": bool(args.deterministic),
+                                      "deterministic": bool(args.deterministic), "op": args.op,
                                       "refined_halfedges_per_step": SH}),
             "e2e": {"value": world * SH * args.e2e_steps / (e2e_total / 1e3), "unit": UNIT,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,

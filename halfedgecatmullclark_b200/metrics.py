@@ -11,10 +11,13 @@ from __future__ import annotations
 
 
 def level_bytes(lv: dict, nxt: dict, rec: int = 16, uv: bool = True, cage: bool = False,
-                cage_uvs: int = 0) -> int:
-    """Minimum HBM bytes of one full refinement step (topology, creases, points)."""
+                cage_uvs: int = 0, topology: bool = True) -> int:
+    """Minimum HBM bytes of one full refinement step (topology, creases, points);
+    with topology=False, of its points alone on a refined topology."""
     H, V, C = lv["H"], lv["V"], lv["C"]
     Vn = nxt["V"]
+    if not topology:
+        return int(12 * V + 12 * Vn + 4 * C + (28 if cage else rec) * H)
     if cage:
         topo = 28 * H + 4 * rec * H + 8 * cage_uvs
     else:

@@ -10,7 +10,7 @@ the refined halfedges, deepest level first).  The forward saves no tensor:
 the adjoint needs only the subd's level offsets and its device topology.
 
 Both run on the caller's current CUDA stream, so the function composes with
-torch streams and CUDA-graph capture.
+torch streams.
 """
 from __future__ import annotations
 
