@@ -9,9 +9,11 @@ and the RMS error relative to the same scale for three FP32 results:
 * the oracle in FP32, i.e. the reference's own order of operations.
 
 It prints one line per result (run with ``-s`` to see them) and asserts the
-north star's bar: the default path is within 1e-5 and no less accurate than
-the reference's FP32 order by more than a small factor, and the
-deterministic path equals the FP32 oracle bit for bit.
+bar: the default path is within 1e-5 and no less accurate than the
+reference's FP32 order by more than a small factor, the deterministic path
+equals the FP32 oracle bit for bit, and, where the reference is built, the
+default path is within 1e-5 of the reference's own multi-threaded
+ccs_Refine_Scatter on the same cage and depth.
 """
 import numpy as np
 import pytest
@@ -64,3 +66,20 @@ def test_error_report_against_fp64(config):
     assert rows["default"][0] <= TOL_POINTS
     assert rows["default"][0] <= 4 * rows["fp32 reference order"][0] + 1e-7
     assert np.array_equal(p_det.view(np.uint32), o32.view(np.uint32))
+    # against the reference's own multi-threaded ccs_Refine_Scatter, when built
+    from oracle import refimpl
+    if refimpl.available():
+        refimpl.set_threads(refimpl.max_threads())
+        s = refimpl.RefSubd(w.cage, w.depth)
+        try:
+            s.refine("scatter")
+            ref = s.points().copy()
+            assert np.array_equal(s.halfedges()[:, :3], he[:, :3])
+        finally:
+            s.close()
+        d = p_def.astype(np.float64) - ref.astype(np.float64)
+        scale = float(np.abs(ref).max())
+        mx, rms = float(np.abs(d).max()) / scale, float(np.sqrt(np.mean(d * d))) / scale
+        print("fp32 reference %s default vs ccs_Refine_Scatter (%d threads): max %.3e rms %.3e"
+              % (config, refimpl.max_threads(), mx, rms))
+        assert mx <= TOL_POINTS
