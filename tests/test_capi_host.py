@@ -92,6 +92,12 @@ def test_invalid_arguments_are_refused_on_the_host(lib):
     bad.creases["nextID"][2] = -5
     mb = bad.as_cc_mesh()
     assert lib.ccs_CreateEx_cuda(ctypes.byref(mb), 3, 0, ctypes.byref(out)) == -1   # crease link
+    # an isolated vertex (no halfedge: the reference's gather rules would
+    # follow its vertex-to-halfedge entry of -1)
+    from halfedgecatmullclark_b200.cage import build_cage
+    pts = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0], [2, 2, 2]], np.float32)
+    iso = build_cage(pts, [[0, 1, 2, 3]]).as_cc_mesh()
+    assert lib.ccs_CreateEx_cuda(ctypes.byref(iso), 2, 0, ctypes.byref(out)) == -1
     big = configs.height_grid(n=256)
     mg = big.cage.as_cc_mesh()
     assert lib.ccs_CreateEx_cuda(ctypes.byref(mg), 6, 0, ctypes.byref(out)) == -3   # int32 overflow
