@@ -65,6 +65,25 @@ def test_header_shares_types_with_reference_header(tmp_path):
     assert r.returncode == 0, r.stderr
 
 
+def test_compat_header_keeps_the_reference_calls(tmp_path):
+    """include/ccs_cuda_compat.h after CatmullClark.h: the reference's own
+    calls, a call through a function pointer and an accessor compile."""
+    ref = "/root/reference/CatmullClark.h"
+    if not os.path.exists(ref):
+        pytest.skip("reference header not available")
+    src = tmp_path / "t.c"
+    src.write_text('#define CC_IMPLEMENTATION\n#include "CatmullClark.h"\n#include "ccs_cuda_compat.h"\n'
+                   'static void Bench(void (*f)(cc_Subd *), cc_Subd *s) { f(s); }\n'
+                   'int main(void) { cc_Mesh *m = ccm_Load("x.ccm"); cc_Subd *s = ccs_Create(m, 2);\n'
+                   '  ccs_Refine_Scatter(s); Bench(&ccs_Refine_Gather, s);\n'
+                   '  cc_VertexPoint p = ccs_VertexPoint(s, 0, 2); (void)p;\n'
+                   '  ccs_Release(s); ccm_Release(m); return 0; }\n')
+    for cc, std in (("gcc", "-std=gnu11"), ("g++", "-std=c++17")):
+        r = subprocess.run([cc, std, "-fsyntax-only", "-I/root/reference", "-I" + os.path.dirname(HEADER),
+                            "-x", "c" if cc == "gcc" else "c++", str(src)], capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+
+
 def test_error_strings(lib):
     for code in (0, -1, -2, -3, -4, -5, -6, -7):
         assert lib.ccs_ErrorString_cuda(code)
