@@ -87,6 +87,7 @@ k_adj_quad_edges(QuadView<RW> L, float* __restrict__ gNew) {
 template <int RW>
 __global__ void __launch_bounds__(kBlockA, CCS_ADJ_STEP_MIN_BLOCKS)
 k_adj_quad_step(QuadView<RW> L, const float* __restrict__ gNew, float* __restrict__ gOld) {
+    chain_wait_then_release();
     adj_quad_step_tile<RW>(L, gNew, gOld, (int64_t)blockIdx.x * kBlockA);
 }
 
@@ -103,7 +104,7 @@ static void adjoint_quad_level(const Ctx& c, const QuadView<RW>& L, float* gNew,
 #ifndef CCS_NO_ADJ_STEP
     if (L.d >= 2 && L.ostats) {
         c.prof->begin(c.stream, CCS_K_ADJ_STEP, L.d, L.H);
-        k_adj_quad_step<RW><<<nblocksA(L.H), kBlockA, 0, c.stream>>>(L, gNew, gOld);
+        launch_chained(k_adj_quad_step<RW>, nblocksA(L.H), kBlockA, c.stream, L, gNew, gOld);
         c.prof->end(c.stream);
         return;
     }

@@ -17,6 +17,17 @@ namespace ccs {
 // Upper bound on the steps of any ring or face walk in device code.
 static constexpr int kWalkCap = 1 << 16;
 
+// Programmatic dependent launch, for kernels launched by launch_chained: wait
+// until the previous grid in the stream has completed and its memory is
+// visible (a no-op for a kernel launched the ordinary way), then let the next
+// grid be launched (it fires once every block of this grid has run it, so
+// the next grid's blocks, which wait in turn, only fill slots this grid has
+// left).  Both must come before the kernel touches global memory.
+__device__ __forceinline__ void chain_wait_then_release() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // ---------------------------------------------------------------------------
 // Exact float helpers (CatmullClark.h:295-392)
 // ---------------------------------------------------------------------------

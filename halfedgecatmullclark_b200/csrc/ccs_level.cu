@@ -85,6 +85,7 @@ k_level_a(LevelArgs a) {
 template <int RW, bool TOPO, bool UV, bool CREASED, bool TMAP>
 __global__ void __launch_bounds__(kBlockL, CCS_AB_MIN_BLOCKS)
 k_level_ab(LevelArgs a, const __grid_constant__ CUtensorMap childMap) {
+    chain_wait_then_release();
     const int nbH = (a.H + kBlockL - 1) / kBlockL;
     if ((int)blockIdx.x >= nbH) {
         if (!TOPO) return;
@@ -247,13 +248,13 @@ static void level_ab(const Ctx& c, int d, bool topo, bool uv, float* pts) {
     memset(&none, 0, sizeof none);
     const CUtensorMap& map = tmap ? c.childMaps[d] : none;
     if (topo && tmap) {
-        if (uv) k_level_ab<RW, true, true, CREASED, RW == 4><<<nb, kBlockL, 0, c.stream>>>(a, map);
-        else k_level_ab<RW, true, false, CREASED, RW == 4><<<nb, kBlockL, 0, c.stream>>>(a, map);
+        if (uv) launch_chained(k_level_ab<RW, true, true, CREASED, RW == 4>, nb, kBlockL, c.stream, a, map);
+        else launch_chained(k_level_ab<RW, true, false, CREASED, RW == 4>, nb, kBlockL, c.stream, a, map);
     } else if (topo) {
-        if (RW == 4 && uv) k_level_ab<RW, true, true, CREASED, false><<<nb, kBlockL, 0, c.stream>>>(a, map);
-        else k_level_ab<RW, true, false, CREASED, false><<<nb, kBlockL, 0, c.stream>>>(a, map);
+        if (RW == 4 && uv) launch_chained(k_level_ab<RW, true, true, CREASED, false>, nb, kBlockL, c.stream, a, map);
+        else launch_chained(k_level_ab<RW, true, false, CREASED, false>, nb, kBlockL, c.stream, a, map);
     } else {
-        k_level_ab<RW, false, false, CREASED, false><<<nb, kBlockL, 0, c.stream>>>(a, map);
+        launch_chained(k_level_ab<RW, false, false, CREASED, false>, nb, kBlockL, c.stream, a, map);
     }
     c.prof->end(c.stream);
 }
