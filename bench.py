@@ -310,24 +310,31 @@ def run_reference(args):
     from halfedgecatmullclark_b200.subd import level_counts
     sh = metrics.total_halfedges(level_counts(w.cage, w.depth))
     cores = os.cpu_count() or 1
+    # the same config object as this arm's own line
+    cfg = config_dict(w, {"parallelism": "replicas x%d" % max(1, args.gpus),
+                          "deterministic": bool(args.deterministic), "op": args.op,
+                          "refined_halfedges_per_step": sh})
     if not refimpl.available():
-        base = cpu_reference(w, args.cpu_seconds)
+        base = cpu_reference(w, args.cpu_seconds, op=args.op)
         line = {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": UNIT,
                 "n_gpus": args.gpus, "steps": 0, "warmup": 0, "ms_per_step": base["ms_per_step"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                "data": "synthetic", "config": config_dict(w), "cpu_baseline": base,
+                "data": "synthetic", "config": cfg, "cpu_baseline": base,
                 "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return 0
     refimpl.set_threads(cores)
     s = refimpl.RefSubd(w.cage, w.depth)
+    call = "ccs_RefineVertexPoints_Scatter" if args.op == "points" else "ccs_Refine_Scatter"
     try:
+        if args.op == "points":
+            s.refine("scatter")                     # the topology, untimed
         for _ in range(args.warmup):
-            s.refine("scatter")
+            s.call(call)
         times = []
         for _ in range(args.steps):
             t0 = time.perf_counter()
-            s.refine("scatter")
+            s.call(call)
             times.append(time.perf_counter() - t0)
     finally:
         s.close()
@@ -336,10 +343,10 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic", "config": config_dict(w),
+            "data": "synthetic", "config": cfg,
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
-                             "sample": "%d timed runs of the reference ccs_Refine_Scatter on the full "
-                                       "workload, OpenMP %d threads" % (args.steps, cores)},
+                             "sample": "%d timed runs of the reference %s on the full "
+                                       "workload, OpenMP %d threads" % (args.steps, call, cores)},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
