@@ -72,3 +72,25 @@ def rel_err(a, b):
     b = np.asarray(b, np.float64)
     den = np.abs(b).max()
     return float(np.abs(a - b).max() / (den if den > 0 else 1.0))
+
+
+def small_cages():
+    """Edge-case cages: single faces (every edge a boundary), a quad and a
+    triangle sharing an edge, two quads, and a creased single quad with UVs."""
+    from halfedgecatmullclark_b200.cage import build_cage
+    rng = np.random.default_rng(11)
+    quad = np.array([[0, 0, 0], [1, 0, 0.1], [1, 1, 0], [0, 1, 0.2]], np.float32)
+    tri = np.array([[0, 0, 0], [1, 0, 0], [0.3, 0.9, 0.4]], np.float32)
+    pent = np.array([[np.cos(a), np.sin(a), 0.1 * i] for i, a in
+                     enumerate(np.linspace(0, 2 * np.pi, 5, endpoint=False))], np.float32)
+    two = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0.3], [0, 1, 0], [2, 0, 0.1], [2, 1, 0]], np.float32)
+    uvs = rng.uniform(0, 1, (4, 2)).astype(np.float32)
+    return [
+        ("quad", build_cage(quad, [[0, 1, 2, 3]])),
+        ("triangle", build_cage(tri, [[0, 1, 2]])),
+        ("pentagon", build_cage(pent, [[0, 1, 2, 3, 4]])),
+        ("quad_and_triangle", build_cage(two[:5], [[0, 1, 2, 3], [1, 4, 2]])),
+        ("two_quads", build_cage(two, [[0, 1, 2, 3], [1, 4, 5, 2]])),
+        ("creased_quad_uv", build_cage(quad, [[0, 1, 2, 3]], uvs=uvs, face_uvs=[[0, 1, 2, 3]],
+                                       crease_tags=[(0, 1, 1.5)])),
+    ]

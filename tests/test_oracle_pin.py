@@ -94,6 +94,24 @@ def test_oracle_bitexact_vs_reference(small_workloads, mode):
         assert np.array_equal(pts.view(np.uint32), rpts.view(np.uint32))
 
 
+@pytest.mark.parametrize("mode", MODES)
+def test_oracle_bitexact_vs_reference_small_cages(mode):
+    """The edge-case cages (single faces, two faces, a creased quad with UVs)
+    at depths 1-4: the oracle equals the single-threaded reference."""
+    refimpl = _need_ref()
+    from conftest import small_cages
+    from oracle import oracle
+    refimpl.set_threads(1)
+    for name, cage in small_cages():
+        for depth in (1, 2, 3, 4):
+            he, cr, pts = oracle.refine(cage, depth, mode)
+            rhe, rcr, rpts = refimpl.refine(cage, depth, mode)
+            cols = 4 if cage.U > 0 else 3
+            assert np.array_equal(he[:, :cols], rhe[:, :cols]), (name, depth)
+            assert np.array_equal(cr.view(np.uint8), rcr.view(np.uint8)), (name, depth)
+            assert np.array_equal(pts.view(np.uint32), rpts.view(np.uint32)), (name, depth)
+
+
 def test_fp64_oracle_close_to_reference_fp64(small_workloads):
     refimpl = _need_ref()
     if not refimpl.available64():
