@@ -2,8 +2,9 @@
 
 Runs the reference's own ccs_Refine_* (compiled from its sources into
 oracle/_ref by `make -C oracle ref`, single-threaded so the float sums are
-in halfedge order) on the seeded synthetic cages used by the tests and on
-the reference's sample .ccm cages, and records SHA-256 digests of the
+in halfedge order) on the seeded synthetic cages used by the tests, on the
+edge-case cages of tests/conftest.py (depths 1-4) and on the reference's
+sample .ccm cages, and records SHA-256 digests of the
 refined halfedges, creases and points, plus the per-depth counts.  The
 tests compare the oracle against these digests, which pins the oracle on
 machines where the reference is not available.
@@ -64,10 +65,16 @@ def main():
     if not refimpl.available():
         raise SystemExit("build the reference first: make -C oracle ref")
     refimpl.set_threads(1)
-    res = {"generator": "tests/golden/make_golden.py", "workloads": {}, "ccm": {}}
+    res = {"generator": "tests/golden/make_golden.py", "workloads": {}, "ccm": {}, "small": {}}
     for w in golden_workloads():
         key = "%s_H%d_d%d" % (w.name, w.cage.H, w.depth)
         res["workloads"][key] = entry(w.cage, w.depth)
+    # the edge-case cages (single faces, two faces, a creased quad with UVs)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from conftest import small_cages
+    for name, cage in small_cages():
+        for depth in (1, 2, 3, 4):
+            res["small"]["%s_d%d" % (name, depth)] = entry(cage, depth)
     if os.path.isdir(MESHES):
         os.makedirs(os.path.join(HERE, "_ccm"), exist_ok=True)
         for name in sorted(os.listdir(MESHES)):

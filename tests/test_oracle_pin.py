@@ -52,6 +52,26 @@ def test_oracle_matches_reference_digests():
     assert seen == 20
 
 
+def test_oracle_matches_reference_digests_small_cages():
+    """The edge-case cages at depths 1-4, all four point modes, against the
+    reference's digests (no reference build needed)."""
+    from conftest import small_cages
+    from oracle import oracle
+    g = golden()["small"]
+    seen = 0
+    for name, cage in small_cages():
+        for depth in (1, 2, 3, 4):
+            ref_modes = g["%s_d%d" % (name, depth)]["modes"]
+            for mode in MODES:
+                he, cr, pts = oracle.refine(cage, depth, mode)
+                ref = ref_modes[mode]
+                assert digest(he if cage.U > 0 else he[:, :3]) == ref["halfedges"], (name, depth, mode)
+                assert digest(cr) == ref["creases"], (name, depth, mode)
+                assert digest(pts) == ref["points"], (name, depth, mode)
+                seen += 1
+    assert seen == 96
+
+
 def test_oracle_matches_reference_digests_ccm():
     from halfedgecatmullclark_b200 import ccm
     from oracle import oracle
