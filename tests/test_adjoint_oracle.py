@@ -69,3 +69,27 @@ def test_dense_operator(case):
     # the rule acts on each coordinate alike (S (x) I3)
     x = rng.normal(size=(V, 3))
     assert np.allclose(forward64(w, he, cr, x), S @ x, rtol=1e-12, atol=1e-12)
+
+
+def test_dense_operator_small_cages():
+    """The edge-case cages (single faces, two faces, a creased quad with UVs)
+    at depths 1-4: the oracle's adjoint is the transpose of its forward,
+    exactly the dense operator built column by column."""
+    from conftest import small_cages
+    from oracle import oracle
+    rng = np.random.default_rng(2)
+    for name, cage in small_cages():
+        for depth in (1, 2, 3, 4):
+            he, cr = oracle.refine_topology(cage, depth)
+
+            def fwd(x):
+                return oracle.refine_points(cage, depth, he, cr, "scatter", np.float64, cage_points=x)
+            y = rng.normal(size=(fwd(cage.vertex_points.astype(np.float64)).shape[0], 3))
+            g = oracle.adjoint(cage, depth, he, cr, y)
+            dense = np.zeros_like(g)
+            for v in range(cage.V):
+                for c in range(3):
+                    e = np.zeros((cage.V, 3))
+                    e[v, c] = 1.0
+                    dense[v, c] = float(np.sum(fwd(e) * y))
+            assert np.abs(g - dense).max() <= 1e-12 * max(1.0, np.abs(dense).max()), (name, depth)
