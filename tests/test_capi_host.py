@@ -84,6 +84,26 @@ def test_compat_header_keeps_the_reference_calls(tmp_path):
         assert r.returncode == 0, r.stderr
 
 
+def test_compat_header_maps_every_subd_call():
+    """Every subd call the reference declares (ccs_Create, ccs_Release,
+    ccs_Refine*) has a same-named macro in include/ccs_cuda_compat.h, and each
+    maps to a `_cuda` entry point the library exports."""
+    ref = "/root/reference/CatmullClark.h"
+    if not os.path.exists(ref):
+        pytest.skip("reference header not available")
+    with open(ref) as fh:
+        decl = set(re.findall(r"^CCDEF [^(]*?\b(ccs_(?:Create|Release|Refine\w*))\(", fh.read(), re.M))
+    compat = os.path.join(os.path.dirname(HEADER), "ccs_cuda_compat.h")
+    with open(compat) as fh:
+        text = fh.read()
+    mapped = set(re.findall(r"^#define (ccs_\w+)\s+ccs_compat_\w+", text, re.M))
+    assert decl and decl <= mapped, decl - mapped
+    from halfedgecatmullclark_b200 import _native
+    out = subprocess.run(["nm", "-D", "--defined-only", _native.LIB_PATH], capture_output=True, text=True).stdout
+    for name in decl:
+        assert re.search(r"\b%s_cuda\b" % name, out), name
+
+
 def test_error_strings(lib):
     for code in (0, -1, -2, -3, -4, -5, -6, -7):
         assert lib.ccs_ErrorString_cuda(code)
