@@ -202,19 +202,6 @@ static SubdImpl* find(const cc_Subd* s) {
     return it == g_reg.end() ? nullptr : it->second;
 }
 
-// RAII: make the subd's device current, restore the caller's afterwards.
-struct DeviceGuard {
-    int prev = -1;
-    explicit DeviceGuard(int dev) {
-        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
-        if (prev != dev) cudaSetDevice(dev);
-    }
-    ~DeviceGuard() {
-        int cur = -1;
-        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
-    }
-};
-
 static void free_impl(SubdImpl* s) {
     if (!s) return;
     for (auto& kv : s->graphs) cudaGraphExecDestroy(kv.second);

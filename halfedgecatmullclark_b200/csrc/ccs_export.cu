@@ -173,9 +173,7 @@ int export_obj(const cc_Subd* subd, int32_t depth, const char* path) {
     SubdView sv;
     if (!path || !subd_view(subd, &sv) || depth < 0 || depth > sv.D) return CCS_ERR_ARG;
     if (depth > 0 && !sv.topo) return CCS_ERR_STATE;
-    int cur = -1;
-    cudaGetDevice(&cur);
-    if (cur != sv.device) cudaSetDevice(sv.device);
+    DeviceGuard g(sv.device);
     ObjArgs a;
     a.depth = depth;
     a.rw = sv.rw;
@@ -236,7 +234,6 @@ int export_obj(const cc_Subd* subd, int32_t depth, const char* path) {
     if (depth > 0) put("\n");
     cudaFreeHost(stage);
     ok = (fclose(f) == 0) && ok;
-    if (cur >= 0 && cur != sv.device) cudaSetDevice(cur);
     return ok ? CCS_OK : CCS_ERR_CUDA;
 }
 

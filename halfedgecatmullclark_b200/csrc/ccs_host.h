@@ -10,6 +10,19 @@
 
 namespace ccs {
 
+// RAII: make a subd's device current, restore the caller's afterwards.
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
 // A launch whose grid may be scheduled while the previous kernel in the
 // stream drains (programmatic stream serialization); the kernel must begin
 // with chain_wait_then_release().
