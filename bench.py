@@ -164,6 +164,11 @@ class ClockSampler:
     def _stop_nvml(self):
         self.stop_flag.set()
         self.thread.join(timeout=5)
+        try:
+            import pynvml
+            pynvml.nvmlShutdown()
+        except Exception:
+            pass
         rows = self.rows
         if not rows:
             return None
