@@ -306,6 +306,12 @@ def cpu_reference(w, seconds, max_runs=20, min_runs=2, op="refine"):
 
 
 def run_reference(args):
+    """The reference's own ccs_Refine_Scatter (or its points pass) on the same
+    workload, OpenMP on every host core.  Nothing of the CUDA package's
+    native code loads in this process: the cage comes from the reference's
+    LoadObj on the workload's OBJ text (the same cage, byte for byte, as the
+    CUDA arm's converter gives), and the halfedge total from the reference's
+    own ccs_CumulativeHalfedgeCountAtDepth."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
@@ -317,15 +323,14 @@ def run_reference(args):
         return 0
     w = workload(args)
     from oracle import refimpl
-    from halfedgecatmullclark_b200 import metrics
-    from halfedgecatmullclark_b200.subd import level_counts
-    sh = metrics.total_halfedges(level_counts(w.cage, w.depth))
     cores = os.cpu_count() or 1
-    # the same config object as this arm's own line
-    cfg = config_dict(w, {"parallelism": "replicas x%d" % max(1, args.gpus),
-                          "deterministic": bool(args.deterministic), "op": args.op,
-                          "refined_halfedges_per_step": sh})
     if not refimpl.available():
+        from halfedgecatmullclark_b200 import metrics
+        from halfedgecatmullclark_b200.subd import level_counts
+        sh = metrics.total_halfedges(level_counts(w.cage, w.depth))
+        cfg = config_dict(w, {"parallelism": "replicas x%d" % max(1, args.gpus),
+                              "deterministic": bool(args.deterministic), "op": args.op,
+                              "refined_halfedges_per_step": sh})
         base = cpu_reference(w, args.cpu_seconds, op=args.op)
         line = {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": UNIT,
                 "n_gpus": args.gpus, "steps": 0, "warmup": 0, "ms_per_step": base["ms_per_step"],
@@ -335,7 +340,13 @@ def run_reference(args):
         print(json.dumps(line))
         return 0
     refimpl.set_threads(cores)
-    s = refimpl.RefSubd(w.cage, w.depth)
+    cage = refimpl.cage_from_obj_text(w.obj())
+    s = refimpl.RefSubd(cage, w.depth)
+    sh = int(s.cumH)                               # halfedges of depths 1..D
+    # the same config object as the CUDA arm's own line
+    cfg = config_dict(w, {"parallelism": "replicas x%d" % max(1, args.gpus),
+                          "deterministic": bool(args.deterministic), "op": args.op,
+                          "refined_halfedges_per_step": sh})
     call = "ccs_RefineVertexPoints_Scatter" if args.op == "points" else "ccs_Refine_Scatter"
     try:
         if args.op == "points":
@@ -357,7 +368,8 @@ def run_reference(args):
             "data": "synthetic", "config": cfg,
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
                              "sample": "%d timed runs of the reference %s on the full "
-                                       "workload, OpenMP %d threads" % (args.steps, call, cores)},
+                                       "workload (cage by the reference's LoadObj), OpenMP %d threads"
+                                       % (args.steps, call, cores)},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -690,15 +702,17 @@ def main():
     total_prof = sum(sum(v) for v in by.values())
     # the dominant kernel of the subd's own stream (ring_stats runs on the
     # second stream beside kernel A: its events span the overlap)
-    dom_key = max((k for k in by if k[0] != "ring_stats"), key=lambda k: sum(by[k]))
+    dom_key = max((k for k in by if k[0] not in ("ring_stats", "crease_stats")), key=lambda k: sum(by[k]))
     dom_ms = statistics.mean(by[dom_key])
-    dom_bytes = metrics.kernel_bytes(dom_key[0], levels[dom_key[1]], rec_bytes)
+    def kbytes(kernel, d):
+        return metrics.kernel_bytes(kernel, levels[d], rec_bytes, levels[d - 1] if d >= 1 else None)
+    dom_bytes = kbytes(*dom_key)
     peak, peak_kind = measured_peak()
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9
     traffic = traffic_table().get("%s@%d" % dom_key)
     kernels = sorted(({"kernel": k[0], "level": k[1], "mean_ms": statistics.mean(v),
                        "share": sum(v) / total_prof,
-                       "gbs": metrics.kernel_bytes(k[0], levels[k[1]], rec_bytes) / (statistics.mean(v) / 1e3) / 1e9}
+                       "gbs": kbytes(*k) / (statistics.mean(v) / 1e3) / 1e9}
                       for k, v in by.items()), key=lambda x: -x["share"])
     per_depth = []
     for d in range(w.depth):
@@ -708,8 +722,12 @@ def main():
             ms = statistics.mean(steps_by[("step", d)])
         else:
             ms = sum(statistics.mean(v) for k, v in by.items() if k[1] == d)
+        # the default pass runs steps d >= 2 as one launch that reads each
+        # record once; the cage step, depth 1 and the exact pass read the
+        # records again in a separate vertex pass
+        fused = d >= 2 and not args.deterministic
         nb = metrics.level_bytes(levels[d], levels[d + 1], rec_bytes, subd.record_words == 4, d == 0, w.cage.U,
-                                 topology=not points_op)
+                                 topology=not points_op, fused=fused)
         per_depth.append({"depth": d + 1, "ms": ms, "refined_halfedges": levels[d + 1]["H"],
                           "halfedges_per_s": levels[d + 1]["H"] / (ms / 1e3), "alg_bytes": nb,
                           "gbs": nb / (ms / 1e3) / 1e9, "frac_of_peak": nb / (ms / 1e3) / 1e9 / peak})

@@ -722,7 +722,7 @@ const char* ccs_KernelName_cuda(int kernel) {
     static const char* names[] = {"topology", "creases", "face_points", "edge_points", "vertex_points",
                                   "clear", "level_fused", "adjoint", "uvs", "level_points", "old_vertices",
                                   "ring_stats", "adj_edges", "adj_faces", "adj_vertices", "exact_points", "step",
-                                  "level_step", "level_step_points", "adj_step"};
+                                  "level_step", "level_step_points", "adj_step", "crease_stats"};
     static_assert(sizeof(names) / sizeof(names[0]) == CCS_K_COUNT, "one name per kernel id");
     return (kernel >= 0 && kernel < CCS_K_COUNT) ? names[kernel] : "unknown";
 }

@@ -171,7 +171,7 @@ static void crease_stats_level(const Ctx& c, int d, cudaStream_t s) {
     float4* out = stats_at(c, d);
     if (!out || d < 1 || c.lv[d].C <= 0) return;
     const QuadView<RW> L = quad_view_l<RW>(c, d);
-    c.prof->begin(s, CCS_K_RING_STATS, d, L.C);
+    c.prof->begin(s, CCS_K_CREASE_STATS, d, L.C);
     k_crease_stats<RW><<<nblocksL(L.C), kBlockL, 0, s>>>(L, out, c.lv[d - 1].V);
     c.prof->end(s);
 }

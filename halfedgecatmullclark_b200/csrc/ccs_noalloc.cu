@@ -31,21 +31,64 @@ static __device__ __align__(256) float g_adjoint_scratch[kScratchFloats];
 
 // Host code must not use g_adjoint_scratch itself (on the host it names a
 // host-side stand-in, not GPU memory): it uses the device address looked up
-// once per device, with that device current.
+// with that device current, once per device and context.  The context's id
+// is kept beside the address: a caller that resets the device
+// (cudaDeviceReset) gets a new context, whose address is looked up again.
 static constexpr int kMaxDevices = 64;
+struct ScratchSlot {
+    float* addr = nullptr;
+    unsigned long long ctx = 0;
+};
 static std::mutex g_scratch_mu;
-static float* g_scratch_addr[kMaxDevices] = {};
+static ScratchSlot g_scratch[kMaxDevices];
+
+// The unique id of the calling thread's current context (cuCtxGetId, through
+// the runtime's driver entry points: no link against the driver library);
+// false when it cannot be read, in which case nothing is cached.
+static bool current_context_id(unsigned long long* id) {
+    using GetCurrent = int (*)(void**);
+    using GetId = int (*)(void*, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<GetCurrent>(p);
+        p = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<GetId>(p);
+    });
+    void* ctx = nullptr;
+    if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx) return false;
+    return get_id(ctx, id) == 0;
+}
 
 static int scratch_address(float** out) {
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return CCS_ERR_CUDA;
+    unsigned long long ctx = 0;
+    const bool known = current_context_id(&ctx);
     std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (!g_scratch_addr[dev]) {
+    ScratchSlot& slot = g_scratch[dev];
+    if (!known || !slot.addr || slot.ctx != ctx) {
         void* p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_adjoint_scratch) != cudaSuccess || !p) return CCS_ERR_CUDA;
-        g_scratch_addr[dev] = static_cast<float*>(p);
+        if (cudaGetSymbolAddress(&p, g_adjoint_scratch) != cudaSuccess || !p) {
+            slot = ScratchSlot{};
+            return CCS_ERR_CUDA;
+        }
+        slot.addr = static_cast<float*>(p);
+        slot.ctx = known ? ctx : 0;
+        if (!known) {                      // not cached: looked up again next time
+            *out = slot.addr;
+            slot = ScratchSlot{};
+            return CCS_OK;
+        }
     }
-    *out = g_scratch_addr[dev];
+    *out = slot.addr;
     return CCS_OK;
 }
 
@@ -61,13 +104,10 @@ extern "C" int ccs_AdjointPointsDeviceNoAlloc_cuda(cc_Subd* subd, const float* g
     if (3 * arrays.vertexCount > kScratchFloats) return set_last_error(CCS_ERR_SCRATCH_LIMIT);
     cudaPointerAttributes attr;
     if (cudaPointerGetAttributes(&attr, arrays.vertexPoints) != cudaSuccess) return set_last_error(CCS_ERR_CUDA);
-    int prev = -1;
-    cudaGetDevice(&prev);
-    if (prev != attr.device) cudaSetDevice(attr.device);
+    DeviceGuard guard(attr.device);        // the caller's device is back on every return
     float* work = nullptr;
     int st = scratch_address(&work);
     if (st == CCS_OK)
         st = adjoint_into(subd, gradPoints, gradCage, work, kScratchFloats, static_cast<cudaStream_t>(stream));
-    if (prev >= 0 && prev != attr.device) cudaSetDevice(prev);
     return set_last_error(st);
 }

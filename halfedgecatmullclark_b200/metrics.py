@@ -3,17 +3,22 @@
 Every figure counts each unique input read once and each output written
 once, in the packed layout (16-byte halfedge records, or 12 with
 CCS_FLAG_NO_UV; 12-byte creases; 12-byte points).  ``level_bytes`` is the
-minimum for a whole refinement step d -> d+1 when the point passes read the
-halfedges once more (the per-depth GB/s figure); ``kernel_bytes`` is the
+minimum for a whole refinement step d -> d+1 (the per-depth GB/s figure):
+when the step's point pass is fused with its topology (one launch that
+reads each record once: the default pass at depth >= 2) the records are
+counted once; when the point pass runs as a launch of its own it reads them
+again, and ``fused=False`` adds that second read.  ``kernel_bytes`` is the
 per-launch figure of one kernel, which defines its achieved bandwidth.
 """
 from __future__ import annotations
 
 
 def level_bytes(lv: dict, nxt: dict, rec: int = 16, uv: bool = True, cage: bool = False,
-                cage_uvs: int = 0, topology: bool = True) -> int:
+                cage_uvs: int = 0, topology: bool = True, fused: bool = False) -> int:
     """Minimum HBM bytes of one full refinement step (topology, creases, points);
-    with topology=False, of its points alone on a refined topology."""
+    with topology=False, of its points alone on a refined topology.  With
+    fused=True the point pass shares the topology's single read of the
+    records."""
     H, V, C = lv["H"], lv["V"], lv["C"]
     Vn = nxt["V"]
     if not topology:
@@ -23,12 +28,15 @@ def level_bytes(lv: dict, nxt: dict, rec: int = 16, uv: bool = True, cage: bool 
     else:
         topo = rec * H + 4 * rec * H
     creases = 12 * C + 24 * C
-    points = 12 * V + 12 * Vn + 4 * C + rec * H
+    points = 12 * V + 12 * Vn + 4 * C + (0 if fused else (28 if cage else rec) * H)
     return int(topo + creases + points)
 
 
-def kernel_bytes(kernel: str, lv: dict, rec: int = 16) -> int:
-    """Per-launch algorithmic bytes of one kernel at parent depth `lv`."""
+def kernel_bytes(kernel: str, lv: dict, rec: int = 16, prev: dict | None = None) -> int:
+    """Per-launch algorithmic bytes of one kernel at parent depth `lv`
+    (`prev` = the level before it, which gives the exact count of older
+    vertices at depth 1, where the quad-structure count below does not
+    hold)."""
     H, V, F, E, C = lv["H"], lv["V"], lv["F"], lv["E"], lv["C"]
     if kernel in ("topology", "uvs"):
         return int(rec * H + 4 * rec * H)
@@ -67,8 +75,14 @@ def kernel_bytes(kernel: str, lv: dict, rec: int = 16) -> int:
         # the crease records in; the gradients of depth d out
         return int(rec * H + 12 * (V + F + E) + 16 * max(V - nb, 0) + 12 * C + 12 * V)
     if kernel == "ring_stats":
-        # records of children 0 and 3 walked, statistics out
-        return int(rec * H // 2 + 16 * max(V - nb, 0))
+        # shape half (k_shape_stats): valence and boundary from the vertex
+        # numbering and the cage alone -- no level data read; one float4 per
+        # older vertex out.
+        return int(16 * (prev["V"] if prev is not None else max(V - nb, 0)))
+    if kernel == "crease_stats":
+        # crease half (k_crease_stats): the level's crease records in; the
+        # atomics of its creased edges go to the statistics already written
+        return int(12 * C)
     if kernel == "exact_points":
         # records + crease records + face and edge points in; the points of
         # its vertices in and out

@@ -244,10 +244,14 @@ int ccs_AdjointPointsDevice_cuda(cc_Subd *subd, const float *gradPoints, float *
  * subds whose refined points fit: 3 * (total refined points) <= 4,194,304,
  * i.e. at most 1,398,101 points over all levels; larger subds are refused
  * with CCS_ERR_SCRATCH_LIMIT.  The caller passes the inputs and outputs as
- * for ccs_AdjointPointsDevice_cuda; the results are identical.
+ * for ccs_AdjointPointsDevice_cuda.  It runs the same kernels, which sum
+ * with float atomics, so the two agree up to the order of those additions
+ * (within 1e-5 relative), not bit for bit.
  *
  * The first call on a device looks up that device's address of the array
  * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * The address is looked up again after the device's context changes (a
+ * caller's cudaDeviceReset).
  * All calls share the one array, so calls whose work can overlap on the GPU
  * (different streams, or different host threads) race and must be
  * serialised by the caller. */
@@ -366,7 +370,9 @@ enum {
     CCS_K_STEP = 16 /* a whole refinement step d -> d+1, on the subd's stream */,
     CCS_K_LEVEL_STEP = 17 /* depth >= 2: topology, creases and all points in one launch */,
     CCS_K_LEVEL_STEP_POINTS = 18 /* depth >= 2: all points of a step in one launch */,
-    CCS_K_ADJ_STEP = 19 /* adjoint of a depth >= 2 step in one launch */, CCS_K_COUNT = 20
+    CCS_K_ADJ_STEP = 19 /* adjoint of a depth >= 2 step in one launch */,
+    CCS_K_CREASE_STATS = 20 /* crease half of a level's ring statistics (ring_stats = the shape half) */,
+    CCS_K_COUNT = 21
 };
 /* When enabled, every launch of the subd is bracketed by CUDA events on its
  * stream (and CUDA graphs are not used). */

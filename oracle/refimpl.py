@@ -157,6 +157,28 @@ def load_obj_text(text: str) -> dict | None:
         os.unlink(name)
 
 
+class RefCage:
+    """A cage as the reference's own ``LoadObj`` builds it (the attributes
+    ``RefSubd`` reads), with no code of the CUDA package involved."""
+
+    def __init__(self, arrays: dict):
+        self.vertex_points = arrays["points"]
+        self.uvs = arrays["uvs"]
+        self.halfedges = arrays["halfedges"]
+        self.creases = arrays["creases"]
+        self.v2h, self.e2h, self.f2h = arrays["v2h"], arrays["e2h"], arrays["f2h"]
+        self.V, self.U = len(self.vertex_points), len(self.uvs)
+        self.H, self.E, self.F = len(self.halfedges), len(self.creases), len(self.f2h)
+
+
+def cage_from_obj_text(text: str) -> RefCage:
+    """The reference's LoadObj (examples/obj_to_ccm.c:666) on OBJ text."""
+    arrays = load_obj_text(text)
+    if arrays is None:
+        raise ValueError("the reference's LoadObj refused the OBJ text")
+    return RefCage(arrays)
+
+
 class _MeshRef:
     def __init__(self, cage, fp64=False):
         self.keep = []

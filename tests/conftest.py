@@ -15,7 +15,12 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-REFERENCE_MESHES = "/root/reference/examples/meshes"
+# The reference checkout the checker reads, when it is present (never on a
+# machine that only runs the GPU tests).  One variable, CCS_REFERENCE_DIR,
+# names it for every test and recipe; the default is where the container
+# that builds this repository mounts it.
+REF = os.environ.get("CCS_REFERENCE_DIR", "/root/reference")
+REFERENCE_MESHES = os.path.join(REF, "examples", "meshes")
 LOCAL_MESHES = os.path.join(ROOT, "tests", "golden", "_ccm")
 
 

@@ -29,7 +29,8 @@ sys.path.insert(0, ROOT)
 from halfedgecatmullclark_b200 import ccm, configs  # noqa: E402
 from oracle import refimpl  # noqa: E402
 
-MESHES = "/root/reference/examples/meshes"
+REF = os.environ.get("CCS_REFERENCE_DIR", "/root/reference")
+MESHES = os.path.join(REF, "examples", "meshes")
 MODES = ["scatter", "gather", "nocreases_scatter", "nocreases_gather"]
 
 

@@ -38,3 +38,31 @@ def test_reference_arm_has_no_batch_run():
     assert r.returncode == 0, r.stderr[-2000:]
     line = json.loads(r.stdout.strip().splitlines()[-1])
     assert line["impl"] == "reference" and "unavailable" in line
+
+
+def test_reference_arm_loads_no_cuda_library():
+    """The reference arm times the reference alone: after a full run of it in
+    one process, no shared object of the CUDA package is mapped there, and its
+    halfedge total is the reference's own count."""
+    from oracle import refimpl
+    if not refimpl.available():
+        pytest.skip("oracle/_ref not built")
+    code = (
+        "import sys, json, io, contextlib\n"
+        "sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', '--warmup', '0']\n"
+        "import bench\n"
+        "buf = io.StringIO()\n"
+        "with contextlib.redirect_stdout(buf):\n"
+        "    rc = bench.run_reference(bench.parse())\n"
+        "maps = open('/proc/self/maps').read()\n"
+        "print(json.dumps({'rc': rc, 'line': buf.getvalue().strip().splitlines()[-1],\n"
+        "                  'cuda_lib': 'libccs_cuda' in maps, 'ref_lib': 'libccref.so' in maps}))\n")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=900, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    out = json.loads(r.stdout.strip().splitlines()[-1])
+    assert out["rc"] == 0 and out["ref_lib"] and not out["cuda_lib"]
+    line = json.loads(out["line"])
+    from halfedgecatmullclark_b200 import configs, metrics
+    from halfedgecatmullclark_b200.subd import level_counts
+    w = configs.mixed_torus(depth=6)
+    assert line["config"]["refined_halfedges_per_step"] == metrics.total_halfedges(level_counts(w.cage, 6))

@@ -8,7 +8,7 @@ import subprocess
 import numpy as np
 import pytest
 
-from conftest import ROOT, gpu_available
+from conftest import REF, ROOT, gpu_available
 
 HEADER = os.path.join(ROOT, "include", "ccs_cuda.h")
 
@@ -52,7 +52,7 @@ def test_header_compiles_as_c_and_cpp(tmp_path):
 
 
 def test_header_shares_types_with_reference_header(tmp_path):
-    ref = "/root/reference/CatmullClark.h"
+    ref = os.path.join(REF, "CatmullClark.h")
     if not os.path.exists(ref):
         pytest.skip("reference header not available")
     src = tmp_path / "t.c"
@@ -60,7 +60,7 @@ def test_header_shares_types_with_reference_header(tmp_path):
                    '_Static_assert(sizeof(cc_Halfedge_SemiRegular) == 16, "record");\n'
                    '_Static_assert(sizeof(cc_Crease) == 12, "crease");\n'
                    'int f(cc_Subd *s){ return ccs_Refine_Scatter_cuda(s) + ccs_HalfedgeTwinID(s, 0, 1); }\n')
-    r = subprocess.run(["gcc", "-std=gnu11", "-fsyntax-only", "-I/root/reference",
+    r = subprocess.run(["gcc", "-std=gnu11", "-fsyntax-only", "-I" + REF,
                         "-I" + os.path.dirname(HEADER), str(src)], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
 
@@ -68,7 +68,7 @@ def test_header_shares_types_with_reference_header(tmp_path):
 def test_compat_header_keeps_the_reference_calls(tmp_path):
     """include/ccs_cuda_compat.h after CatmullClark.h: the reference's own
     calls, a call through a function pointer and an accessor compile."""
-    ref = "/root/reference/CatmullClark.h"
+    ref = os.path.join(REF, "CatmullClark.h")
     if not os.path.exists(ref):
         pytest.skip("reference header not available")
     src = tmp_path / "t.c"
@@ -79,7 +79,7 @@ def test_compat_header_keeps_the_reference_calls(tmp_path):
                    '  cc_VertexPoint p = ccs_VertexPoint(s, 0, 2); (void)p;\n'
                    '  ccs_Release(s); ccm_Release(m); return 0; }\n')
     for cc, std in (("gcc", "-std=gnu11"), ("g++", "-std=c++17")):
-        r = subprocess.run([cc, std, "-fsyntax-only", "-I/root/reference", "-I" + os.path.dirname(HEADER),
+        r = subprocess.run([cc, std, "-fsyntax-only", "-I" + REF, "-I" + os.path.dirname(HEADER),
                             "-x", "c" if cc == "gcc" else "c++", str(src)], capture_output=True, text=True)
         assert r.returncode == 0, r.stderr
 
@@ -88,7 +88,7 @@ def test_compat_header_maps_every_subd_call():
     """Every subd call the reference declares (ccs_Create, ccs_Release,
     ccs_Refine*) has a same-named macro in include/ccs_cuda_compat.h, and each
     maps to a `_cuda` entry point the library exports."""
-    ref = "/root/reference/CatmullClark.h"
+    ref = os.path.join(REF, "CatmullClark.h")
     if not os.path.exists(ref):
         pytest.skip("reference header not available")
     with open(ref) as fh:
