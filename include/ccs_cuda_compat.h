@@ -31,8 +31,19 @@ static inline void ccs_compat_finish_(cc_Subd *subd, int status)
         ccs_Download_cuda(subd);
 }
 
+/* ccs_Create's flags (CCS_FLAG_*), chosen when the program is compiled, as
+ * the reference's own variants are (CC_DISABLE_UV): 0 by default; e.g.
+ * -DCCS_COMPAT_FLAGS=CCS_FLAG_DETERMINISTIC sums every point in the
+ * reference's one-thread order, bit for bit. */
+#ifndef CCS_COMPAT_FLAGS
+#define CCS_COMPAT_FLAGS 0u
+#endif
+
 static inline cc_Subd *ccs_compat_Create(const cc_Mesh *cage, int32_t maxDepth)
-{ return ccs_Create_cuda(cage, maxDepth); }
+{
+    cc_Subd *subd = NULL;
+    return ccs_CreateEx_cuda(cage, maxDepth, (uint32_t)(CCS_COMPAT_FLAGS), &subd) == CCS_OK ? subd : NULL;
+}
 static inline void ccs_compat_Release(cc_Subd *subd)
 { ccs_Release_cuda(subd); }
 

@@ -245,6 +245,20 @@ class RefSubd:
         return _arr(self.s.vertexPoints, 3 * self.cumV,
                     np.float64 if self.fp64 else np.float32).reshape(-1, 3)
 
+    def views(self) -> dict:
+        """Zero-copy numpy views of the subd's packed arrays (valid until
+        close()): halfedges cumH x 4 int32, creases cumC x 3 int32 (the
+        sharpness as its bits; FP32 build only), points cumV x 3."""
+        def view(ptr, n, dtype):
+            dt = np.dtype(dtype)
+            return np.frombuffer((ctypes.c_char * (n * dt.itemsize)).from_address(ptr), dtype=dt, count=n)
+        out = {"halfedges": view(self.s.halfedges, 4 * self.cumH, np.int32).reshape(-1, 4),
+               "points": view(self.s.vertexPoints, 3 * self.cumV,
+                              np.float64 if self.fp64 else np.float32).reshape(-1, 3)}
+        if not self.fp64:
+            out["creases"] = view(self.s.creases, 3 * self.cumC, np.int32).reshape(-1, 3)
+        return out
+
     def close(self) -> None:
         if self.ptr:
             self.L.ccs_Release(self.ptr)

@@ -81,3 +81,60 @@ def test_reference_calls_through_the_compat_header(tmp_path):
     ohe, ocr, opts = oracle.refine(w.cage, w.depth, "scatter", np.float32, 4)
     assert np.array_equal(he, ohe)
     assert rel_err(pts, opts) <= 1e-5
+
+
+PROGRAMS = {k: os.path.join(ROOT, "oracle", "_ref", k) for k in ("subd_cpu_ref", "subd_cpu_cuda", "subd_cpu_cuda_det")}
+
+
+def _run_program(exe, cage_path, depth, workdir, threads=None):
+    """examples/subd_cpu.c's command line: <mesh.ccm> <maxDepth> <exportObj>;
+    it writes subd_<d>.obj for d = 0..maxDepth into its working directory."""
+    os.makedirs(workdir, exist_ok=True)
+    env = dict(os.environ)
+    if threads:
+        env["OMP_NUM_THREADS"] = str(threads)
+    r = subprocess.run([exe, cage_path, str(depth), "1"], cwd=workdir, env=env, capture_output=True,
+                       text=True, timeout=600)
+    assert r.returncode == 0, (exe, r.returncode, r.stdout[-2000:], r.stderr[-2000:])
+    assert "All done!" in r.stdout
+    return [os.path.join(workdir, "subd_%d.obj" % d) for d in range(depth + 1)]
+
+
+@pytest.mark.parametrize("cage_name,depth", [("ArmorGuy.ccm", 3), ("Bigguy.ccm", 4)])
+def test_reference_program_through_the_compat_header(tmp_path, cage_name, depth):
+    """The drop-in with the reference's own program: examples/subd_cpu.c
+    (:1-281), compiled unchanged but for include/ccs_cuda_compat.h after
+    CatmullClark.h and linked to libccs_cuda.so (oracle/Makefile, target
+    subd_cpu), runs its four Bench() passes and its OBJ export (:263-273) on a
+    sample cage.  Its subd_<d>.obj files equal those of the same program built
+    against the reference alone: byte for byte when both sum the points in
+    one order (CCS_FLAG_DETERMINISTIC here, one OpenMP thread there); with the
+    default flags (float atomics on both sides) every "vt" and "f" line byte
+    for byte and the "v" coordinates within 1e-5 of the largest one (plus the
+    1e-6 step of "%f")."""
+    from conftest import ccm_paths
+    for exe in PROGRAMS.values():
+        if not os.path.exists(exe):
+            pytest.skip("oracle/_ref programs not built (make -C oracle subd_cpu)")
+    paths = [p for p in ccm_paths() if os.path.basename(p) == cage_name]
+    if not paths:
+        pytest.skip("the reference's sample cages are not present")
+    cage = paths[0]
+    ref1 = _run_program(PROGRAMS["subd_cpu_ref"], cage, depth, str(tmp_path / "ref1"), threads=1)
+    det = _run_program(PROGRAMS["subd_cpu_cuda_det"], cage, depth, str(tmp_path / "det"))
+    for a, b in zip(det, ref1):
+        with open(a, "rb") as fa, open(b, "rb") as fb:
+            assert fa.read() == fb.read(), "%s differs from the reference program's" % os.path.basename(a)
+    refn = _run_program(PROGRAMS["subd_cpu_ref"], cage, depth, str(tmp_path / "refn"))
+    dflt = _run_program(PROGRAMS["subd_cpu_cuda"], cage, depth, str(tmp_path / "dflt"))
+    for a, b in zip(dflt, refn):
+        with open(a, "rb") as fa, open(b, "rb") as fb:
+            la, lb = fa.read().split(b"\n"), fb.read().split(b"\n")
+        assert len(la) == len(lb)
+        va = [x for x in la if x.startswith(b"v ")]
+        vb = [x for x in lb if x.startswith(b"v ")]
+        assert [x for x in la if not x.startswith(b"v ")] == [x for x in lb if not x.startswith(b"v ")]
+        pa = np.array([x.split()[1:] for x in va], np.float64)
+        pb = np.array([x.split()[1:] for x in vb], np.float64)
+        assert pa.shape == pb.shape and pa.shape[0] > 0
+        assert np.abs(pa - pb).max() <= 1e-5 * np.abs(pb).max() + 1.5e-6, os.path.basename(a)
