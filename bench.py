@@ -26,6 +26,10 @@ topology instead (the call of an animation or fitting loop); its e2e moves
 the cage points in and the points of every depth out through the
 differentiable entry point, and its cpu_baseline is the reference's
 ccs_RefineVertexPoints_Scatter.
+``batch`` (default line): the batched workload -- 512 uneven cages, forward
+points + loss gradient + adjoint, batched (one persistent launch per depth)
+against a Python loop of the single-mesh calls on the same GPU -- measured
+after the headline refine in the same run (``--no-batch`` leaves it off).
 ``--impl reference`` times only the reference CPU path (rank 0).
 Multi-GPU (torchrun): every rank refines its own replica of the cage (the
 single-mesh path does not shard); value = all ranks' halfedges / max time.
@@ -74,6 +78,8 @@ def parse():
                         "depth 5, per-level GB/s); batch: 512 uneven cages, forward + adjoint, "
                         "batched vs a loop of single-mesh calls")
     p.add_argument("--batch-count", type=int, default=512)
+    p.add_argument("--no-batch", action="store_true",
+                   help="leave the batched workload's measurement off the default line")
     return p.parse_args()
 
 
@@ -451,21 +457,24 @@ def subd_halfedges(subd):
     return metrics.total_halfedges(subd.levels)
 
 
-def run_batch_workload(args):
-    """Many uneven cages; one step = forward (points), the gradient of the
-    fitting loss (mean squared distance to a fixed target), adjoint.  Batched
-    (one persistent launch per depth, CUDA graph, autotuned grid) against a
-    Python loop of the single-mesh C-ABI calls on the same GPU and stream;
-    both arms compute the loss gradient as one elementwise operation."""
+def batch_measure(args, rank, world):
+    """Many uneven cages (512 by default: faces log-uniform in [50, 5000],
+    depths uniform in {2..6}); one step = forward (points), the gradient of
+    the fitting loss (mean squared distance to a fixed target), adjoint.
+    Batched (one persistent launch per depth, CUDA graph, autotuned grid)
+    against a Python loop of the single-mesh C-ABI calls on the same GPU and
+    stream; both arms compute the loss gradient as one elementwise operation.
+    Under torchrun every rank refines its own shard of the cages (no
+    exchange); times are the max over ranks.  Returns the measurement on
+    rank 0 (None elsewhere)."""
     import ctypes
     import torch
     from halfedgecatmullclark_b200 import _native as N
     from halfedgecatmullclark_b200 import batch as B
     from halfedgecatmullclark_b200 import configs
+    from halfedgecatmullclark_b200 import shard
     from halfedgecatmullclark_b200.subd import Subd
 
-    from halfedgecatmullclark_b200 import shard
-    rank, world = dist_init()
     ws_all = configs.batch_cages(count=args.batch_count)
     # independent cages: each rank refines its own share, no exchange
     parts = shard.shard([shard.cage_work(w.cage, w.depth) for w in ws_all], world)
@@ -518,7 +527,7 @@ def run_batch_workload(args):
             L.ccs_AdjointPointsDevice_cuda(s.ptr, g.data_ptr(), gc.data_ptr(), sp)
 
     torch.cuda.synchronize()
-    for _ in range(max(1, args.warmup)):
+    for _ in range(max(3, args.warmup)):
         loop_step()
     torch.cuda.synchronize()
     barrier(world)
@@ -531,6 +540,21 @@ def run_batch_workload(args):
     torch.cuda.synchronize()
     loop_ms = shard.max_over_ranks(a.elapsed_time(b) / steps, world)
     loop_sample = [bufs[i][3].clone() for i in (0, len(bufs) // 2, len(bufs) - 1)]
+    # the loop's own kernels: device time of every launch of one step, from
+    # the library's per-launch events; the rest of loop_ms is per-call
+    # launch overhead, the only part that batching removes by itself
+    for s in subds:
+        s.set_profiling(True)
+    loop_step()
+    torch.cuda.synchronize()
+    kern_ms = 0.0
+    launches = 0
+    for s in subds:
+        recs = [r for r in s.read_profile(1 << 14) if r["kernel"] != "step"]
+        kern_ms += sum(r["ms"] for r in recs)
+        launches += len(recs)
+        s.set_profiling(False)
+    kern_ms = shard.max_over_ranks(kern_ms, world)
     for s in subds:
         s.close()
     del bufs, P_all, G_all
@@ -557,7 +581,7 @@ def run_batch_workload(args):
         bt.adjoint()
 
     with torch.cuda.stream(stream):
-        for _ in range(max(1, args.warmup)):
+        for _ in range(max(3, args.warmup)):
             batch_step()
     bt.synchronize()
     barrier(world)
@@ -581,9 +605,10 @@ def run_batch_workload(args):
     agree = max(float((arr["grad_cage_points"][bt.cage_slice(i)] - ref).abs().max() /
                       max(ref.abs().max(), 1e-30))
                 for i, ref in zip((0, len(ws) // 2, len(ws) - 1), loop_sample))
-    # the two halves alone (same stream, CUDA events)
+    # the parts alone (same stream, CUDA events)
     parts = {}
-    for name, fn in (("forward_ms", bt.refine_points), ("adjoint_ms", bt.adjoint)):
+    for name, fn in (("forward_ms", bt.refine_points), ("adjoint_ms", bt.adjoint),
+                     ("loss_grad_ms", lambda: loss_grad(arr["points"], arr["grad_points"]))):
         with torch.cuda.stream(stream):
             a.record(stream)
             for _ in range(steps):
@@ -595,26 +620,45 @@ def run_batch_workload(args):
     sh = int(shard.sum_over_ranks(sum(inf["halfedgeCount"] for inf in bt.info), world))
     topo_ms = shard.max_over_ranks(topo_ms, world)
     bt.close()
+    del arr
+    torch.cuda.empty_cache()
+    if rank != 0:
+        return None
+    return {"metric": "batched forward+adjoint cages/s", "value": len(ws_all) / (batch_ms / 1e3),
+            "unit": "cages/s", "ms_per_step": batch_ms, "steps": steps,
+            "config": {"workload": "batch_cages_%d" % len(ws_all), "faces": "log-uniform [50, 5000]",
+                       "depths": "uniform {2..6}", "refined_halfedges": sh,
+                       "parallelism": "cage shards x%d (no exchange)" % world,
+                       "schedule": {"blocks_per_sm": tune["blocks_per_sm"], "split": tune.get("split"),
+                                    "tried": tune["tried"]}},
+            "loop": {"value": len(ws_all) / (loop_ms / 1e3), "unit": "cages/s", "ms_per_step": loop_ms,
+                     "kernel_ms": kern_ms, "launches": launches, "overhead_ms": loop_ms - kern_ms,
+                     "max_speedup_from_overhead": loop_ms / kern_ms if kern_ms > 0 else None,
+                     "how": "Python loop of ccs_RefinePointsDevice_cuda per cage, the loss gradient over "
+                            "all cages' points in one op, then ccs_AdjointPointsDevice_cuda per cage; "
+                            "kernel_ms = device time of its launches (per-launch events), the rest is "
+                            "per-call overhead"},
+            "speedup_vs_loop": loop_ms / batch_ms, "topology_refine_ms": topo_ms,
+            "forward_ms": parts["forward_ms"], "adjoint_ms": parts["adjoint_ms"],
+            "loss_grad_ms": parts["loss_grad_ms"],
+            "grad_agreement_rel": agree, "clocks": clocks,
+            "step": "forward points, gradient of the mean squared distance to a fixed target, adjoint"}
+
+
+def run_batch_workload(args):
+    """The batched workload as the line's own metric (--workload batch)."""
+    rank, world = dist_init()
+    m = batch_measure(args, rank, world)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
     if rank != 0:
         return 0
-    line = {"metric": "batched forward+adjoint cages/s", "value": len(ws_all) / (batch_ms / 1e3),
-            "unit": "cages/s", "n_gpus": world, "steps": steps, "warmup": args.warmup,
-            "ms_per_step": batch_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "batch_cages_%d" % len(ws_all), "faces": "log-uniform [50, 5000]",
-                       "depths": "uniform {2..6}", "refined_halfedges": sh,
-                       "parallelism": "cage shards x%d (no exchange)" % world,
-                       "schedule": {"blocks_per_sm": tune["blocks_per_sm"], "tried": tune["tried"]}},
-            "loop": {"value": len(ws_all) / (loop_ms / 1e3), "unit": "cages/s", "ms_per_step": loop_ms,
-                     "how": "Python loop of ccs_RefinePointsDevice_cuda per cage, the loss gradient over "
-                            "all cages' points in one op, then ccs_AdjointPointsDevice_cuda per cage"},
-            "speedup_vs_loop": loop_ms / batch_ms, "topology_refine_ms": topo_ms,
-            "forward_ms": parts["forward_ms"], "adjoint_ms": parts["adjoint_ms"],
-            "grad_agreement_rel": agree, "clocks": clocks,
-            "step": "forward points, gradient of the mean squared distance to a fixed target, adjoint"}
+    line = {"metric": m["metric"], "value": m["value"], "unit": m["unit"], "n_gpus": world,
+            "steps": m["steps"], "warmup": args.warmup, "ms_per_step": m["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": m["config"]}
+    line.update({k: v for k, v in m.items() if k not in line and k != "metric"})
     print(json.dumps(line))
     return 0
 
@@ -681,7 +725,8 @@ def main():
     step_ms = [a.elapsed_time(b) for a, b in evs]
     total_ms = max_over_ranks(sum(step_ms), world)
 
-    # per-kernel CUDA events (same workload, profiling launches one by one)
+    # per-kernel device times: the same refine replayed as a profiled CUDA
+    # graph whose event record nodes time every launch as the graph runs it
     subd.set_profiling(True)
     with torch.cuda.stream(stream):
         for _ in range(args.steps):
@@ -695,17 +740,21 @@ def main():
 
     # roofline of the dominant kernel
     by = {}
+    units = {}
     for r in recs:
         by.setdefault((r["kernel"], r["level"]), []).append(r["ms"])
+        units[(r["kernel"], r["level"])] = r["units"]
     steps_by = {k: v for k, v in by.items() if k[0] == "step"}
     by = {k: v for k, v in by.items() if k[0] != "step"}
     total_prof = sum(sum(v) for v in by.values())
     # the dominant kernel of the subd's own stream (ring_stats runs on the
     # second stream beside kernel A: its events span the overlap)
-    dom_key = max((k for k in by if k[0] not in ("ring_stats", "crease_stats")), key=lambda k: sum(by[k]))
+    dom_key = max((k for k in by if k[0] not in ("ring_stats", "crease_stats", "cage_side")),
+                  key=lambda k: sum(by[k]))
     dom_ms = statistics.mean(by[dom_key])
     def kbytes(kernel, d):
-        return metrics.kernel_bytes(kernel, levels[d], rec_bytes, levels[d - 1] if d >= 1 else None)
+        u = units.get((kernel, d)) if kernel in ("cage_side", "ring_stats") and d == 0 else None
+        return metrics.kernel_bytes(kernel, levels[d], rec_bytes, levels[d - 1] if d >= 1 else None, u)
     dom_bytes = kbytes(*dom_key)
     peak, peak_kind = measured_peak()
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9
@@ -776,6 +825,13 @@ def main():
             base = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "unavailable",
                     "sample": "error: %s" % exc}
     subd.close()
+    del flush
+    torch.cuda.empty_cache()
+    # the batched workload (many uneven cages, forward + adjoint against a
+    # loop of single-mesh calls), on the same line so that every run records it
+    batch = None
+    if not args.no_batch and not args.deterministic and args.op == "refine" and args.workload == "mixed_torus":
+        batch = batch_measure(args, rank, world)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -801,6 +857,8 @@ def main():
         }
         if base is not None:
             line["cpu_baseline"] = base
+        if batch is not None:
+            line["batch"] = batch
         print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist

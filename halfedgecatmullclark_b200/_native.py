@@ -28,7 +28,7 @@ POINT_MODES = {"scatter": 0, "gather": 1, "nocreases_scatter": 2, "nocreases_gat
 KERNEL_NAMES = ["topology", "creases", "face_points", "edge_points", "vertex_points", "clear",
                 "level_fused", "adjoint", "uvs", "level_points", "old_vertices", "ring_stats", "adj_edges",
                 "adj_faces", "adj_vertices", "exact_points", "step", "level_step", "level_step_points",
-                "adj_step", "crease_stats"]
+                "adj_step", "crease_stats", "cage_side"]
 
 
 class CcsError(RuntimeError):

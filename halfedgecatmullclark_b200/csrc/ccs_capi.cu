@@ -135,19 +135,30 @@ static bool twins_consistent(const cc_Mesh* m) {
 // ---------------------------------------------------------------------------
 // profiling
 // ---------------------------------------------------------------------------
+static void record_event(cudaEvent_t e, cudaStream_t s, bool capture) {
+    if (capture) cudaEventRecordWithFlags(e, s, cudaEventRecordExternal);
+    else cudaEventRecord(e, s);
+}
 int Profiler::begin(cudaStream_t s, int kernel, int level, int64_t units) {
     if (!on) return -1;
     TimedLaunch t{kernel, level, units, nullptr, nullptr};
     cudaEventCreate(&t.a);
     cudaEventCreate(&t.b);
-    cudaEventRecord(t.a, s);
+    record_event(t.a, s, capture);
     pending.push_back(t);
     return (int)pending.size() - 1;
 }
 void Profiler::end(cudaStream_t s, int index) {
     if (!on || pending.empty()) return;
-    if (index >= 0 && index < (int)pending.size()) cudaEventRecord(pending[(size_t)index].b, s);
-    else cudaEventRecord(pending.back().b, s);
+    if (index >= 0 && index < (int)pending.size()) record_event(pending[(size_t)index].b, s, capture);
+    else record_event(pending.back().b, s, capture);
+}
+static void destroy_events(std::vector<TimedLaunch>& v) {
+    for (auto& t : v) {
+        if (t.a) cudaEventDestroy(t.a);
+        if (t.b) cudaEventDestroy(t.b);
+    }
+    v.clear();
 }
 
 // ---------------------------------------------------------------------------
@@ -180,6 +191,9 @@ struct SubdImpl {
     std::vector<uint8_t> childMapOk;
     Profiler prof;
     std::map<int, cudaGraphExec_t> graphs;
+    // profiled graphs (key op | kProfiledGraph): their timed launches, whose
+    // events the graph's event record nodes set on every replay
+    std::map<int, std::vector<TimedLaunch>> profTemplates;
 
     Ctx ctx(cudaStream_t s) {
         Ctx c;
@@ -206,9 +220,10 @@ static void free_impl(SubdImpl* s) {
     if (!s) return;
     for (auto& kv : s->graphs) cudaGraphExecDestroy(kv.second);
     s->graphs.clear();
-    for (auto& t : s->prof.pending) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
+    destroy_events(s->prof.pending);
+    for (auto& kv : s->profTemplates) destroy_events(kv.second);
     cudaFree(s->dc.he); cudaFree(s->dc.cr); cudaFree(s->dc.pts); cudaFree(s->dc.uvs);
-    cudaFree(s->dc.v2h); cudaFree(s->dc.e2h); cudaFree(s->dc.f2h); cudaFree(s->dc.fsz);
+    cudaFree(s->dc.v2h); cudaFree(s->dc.e2h); cudaFree(s->dc.f2h); cudaFree(s->dc.fsz); cudaFree(s->dc.vshape);
     cudaFree(s->he); cudaFree(s->cr); cudaFree(s->pts); cudaFree(s->work); cudaFree(s->err); cudaFree(s->stats);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     if (s->side) cudaStreamDestroy(s->side);
@@ -229,6 +244,9 @@ template <class T>
 static cudaError_t dmalloc(T** p, size_t bytes) {
     return cudaMalloc((void**)p, bytes ? bytes : 16);
 }
+
+// the device walks' iteration cap (kWalkCap), for the host's copy of one
+static constexpr int32_t kHostWalkCap = 1 << 16;
 
 static int upload_cage(SubdImpl* s, const cc_Mesh* m) {
     DevCage& d = s->dc;
@@ -252,6 +270,27 @@ static int upload_cage(SubdImpl* s, const cc_Mesh* m) {
     for (int32_t h = 0; h < d.H; ++h) ++fsz[(size_t)m->halfedges[h].faceID];
     if (dmalloc(&d.fsz, sizeof(int32_t) * (size_t)d.F)) return CCS_ERR_ALLOC;
     if (cudaMemcpyAsync(d.fsz, fsz.data(), sizeof(int32_t) * (size_t)d.F, cudaMemcpyHostToDevice, st))
+        return CCS_ERR_CUDA;
+    // the ring shape of every cage vertex (valence, boundary), the walk of
+    // the device's old_vertex_shape done once: refinement never changes it
+    std::vector<int32_t> vshape((size_t)d.V, 0);
+    const cc_Halfedge* he = m->halfedges;
+    for (int32_t v = 0; v < d.V; ++v) {
+        const int32_t h0 = m->vertexToHalfedgeIDs[v];
+        int32_t cnt = 1, x = he[he[h0].prevID].twinID, guard = 0;
+        for (; x >= 0 && x != h0 && guard < kHostWalkCap; x = he[he[x].prevID].twinID, ++guard) ++cnt;
+        if (x < 0) {
+            guard = 0;
+            for (int32_t y = he[h0].twinID; y >= 0 && guard < kHostWalkCap; ++guard) {
+                y = he[y].nextID;
+                ++cnt;
+                y = he[y].twinID;
+            }
+        }
+        vshape[(size_t)v] = (cnt & 0x3FFFFFFF) | (x < 0 ? (1 << 30) : 0);
+    }
+    if (dmalloc(&d.vshape, sizeof(int32_t) * (size_t)d.V)) return CCS_ERR_ALLOC;
+    if (cudaMemcpyAsync(d.vshape, vshape.data(), sizeof(int32_t) * (size_t)d.V, cudaMemcpyHostToDevice, st))
         return CCS_ERR_CUDA;
     if (cudaStreamSynchronize(st) != cudaSuccess) return CCS_ERR_CUDA;
     return CCS_OK;
@@ -374,35 +413,70 @@ static cudaError_t enqueue(SubdImpl* s, int op, cudaStream_t st) {
 }
 
 // Run an operation: replay its CUDA graph when allowed, else launch directly.
+// With profiling on, the operation replays a graph of its own that carries
+// an event record node before and after every timed launch: the records
+// then time the launches as the production graph runs them (the stream is
+// synchronised after each replay to read them).
+static constexpr int kProfiledGraph = 1 << 20;
+
 static int execute(SubdImpl* s, int op) {
     DeviceGuard g(s->device);
     cudaStream_t st = s->stream;
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     if (st) cudaStreamIsCapturing(st, &cap);
-    const bool use_graph = st && !s->prof.on && !(s->flags & CCS_FLAG_NO_GRAPH) &&
-                           cap == cudaStreamCaptureStatusNone;
+    const bool use_graph = st && !(s->flags & CCS_FLAG_NO_GRAPH) && cap == cudaStreamCaptureStatusNone;
     if (!use_graph) {
         cudaError_t e = enqueue(s, op, st);
         return e == cudaSuccess ? CCS_OK : CCS_ERR_CUDA;
     }
-    auto it = s->graphs.find(op);
+    const bool prof = s->prof.on;
+    const int key = prof ? (op | kProfiledGraph) : op;
+    auto it = s->graphs.find(key);
     if (it == s->graphs.end()) {
+        std::vector<TimedLaunch> saved;
+        if (prof) {
+            std::swap(saved, s->prof.pending);
+            s->prof.capture = true;
+        }
         cudaGraph_t graph = nullptr;
-        if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return CCS_ERR_CUDA;
-        cudaError_t e = enqueue(s, op, st);
-        cudaError_t e2 = cudaStreamEndCapture(st, &graph);
-        if (e != cudaSuccess || e2 != cudaSuccess || !graph) {
+        cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            e = enqueue(s, op, st);
+            const cudaError_t e2 = cudaStreamEndCapture(st, &graph);
+            if (e == cudaSuccess) e = e2;
+        }
+        std::vector<TimedLaunch> timed;
+        if (prof) {
+            s->prof.capture = false;
+            timed = std::move(s->prof.pending);
+            s->prof.pending = std::move(saved);
+        }
+        if (e != cudaSuccess || !graph) {
             if (graph) cudaGraphDestroy(graph);
+            destroy_events(timed);
             cudaGetLastError();
             return CCS_ERR_CUDA;
         }
         cudaGraphExec_t exec = nullptr;
         e = cudaGraphInstantiate(&exec, graph, 0);
         cudaGraphDestroy(graph);
-        if (e != cudaSuccess) return CCS_ERR_CUDA;
-        it = s->graphs.emplace(op, exec).first;
+        if (e != cudaSuccess) {
+            destroy_events(timed);
+            return CCS_ERR_CUDA;
+        }
+        it = s->graphs.emplace(key, exec).first;
+        if (prof) s->profTemplates[key] = std::move(timed);
     }
-    return cudaGraphLaunch(it->second, st) == cudaSuccess ? CCS_OK : CCS_ERR_CUDA;
+    if (cudaGraphLaunch(it->second, st) != cudaSuccess) return CCS_ERR_CUDA;
+    if (prof) {
+        if (cudaStreamSynchronize(st) != cudaSuccess) return CCS_ERR_CUDA;
+        for (const TimedLaunch& t : s->profTemplates[key]) {
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, t.a, t.b);
+            s->prof.pending.push_back(TimedLaunch{t.kernel, t.level, t.units, nullptr, nullptr, ms});
+        }
+    }
+    return CCS_OK;
 }
 
 static int refine_points_op(cc_Subd* subd, int mode) {
@@ -701,8 +775,8 @@ int ccs_ReadProfile_cuda(cc_Subd* subd, ccs_KernelTime* out, int cap) {
     if (cudaStreamSynchronize(s->stream) != cudaSuccess) return ret(CCS_ERR_CUDA);
     int n = 0;
     for (auto& t : s->prof.pending) {
-        float ms = 0.0f;
-        cudaEventElapsedTime(&ms, t.a, t.b);
+        float ms = t.ms;
+        if (t.a) cudaEventElapsedTime(&ms, t.a, t.b);
         if (n < cap) {
             out[n].kernel = t.kernel;
             out[n].level = t.level;
@@ -710,10 +784,8 @@ int ccs_ReadProfile_cuda(cc_Subd* subd, ccs_KernelTime* out, int cap) {
             out[n].units = t.units;
         }
         ++n;
-        cudaEventDestroy(t.a);
-        cudaEventDestroy(t.b);
     }
-    s->prof.pending.clear();
+    destroy_events(s->prof.pending);
     g_last = CCS_OK;
     return n < cap ? n : cap;
 }
@@ -722,7 +794,8 @@ const char* ccs_KernelName_cuda(int kernel) {
     static const char* names[] = {"topology", "creases", "face_points", "edge_points", "vertex_points",
                                   "clear", "level_fused", "adjoint", "uvs", "level_points", "old_vertices",
                                   "ring_stats", "adj_edges", "adj_faces", "adj_vertices", "exact_points", "step",
-                                  "level_step", "level_step_points", "adj_step", "crease_stats"};
+                                  "level_step", "level_step_points", "adj_step", "crease_stats",
+                                  "cage_side"};
     static_assert(sizeof(names) / sizeof(names[0]) == CCS_K_COUNT, "one name per kernel id");
     return (kernel >= 0 && kernel < CCS_K_COUNT) ? names[kernel] : "unknown";
 }

@@ -55,6 +55,9 @@ struct DevCage {
     int32_t* e2h = nullptr;
     int32_t* f2h = nullptr;
     int32_t* fsz = nullptr;     // F x face size (halfedges per cage face)
+    // V x the ring shape of each cage vertex, which no refinement changes:
+    // valence in bits 0-29, boundary in bit 30 (null: walked when needed)
+    int32_t* vshape = nullptr;
     int32_t V = 0, U = 0, H = 0, E = 0, F = 0;
 };
 
@@ -70,10 +73,15 @@ struct TimedLaunch {
     int kernel, level;
     int64_t units;
     cudaEvent_t a, b;
+    float ms = -1.0f;            // a profiled graph's replay: time already read, no events
 };
 
 struct Profiler {
     bool on = false;
+    // while a profiled CUDA graph is being recorded, begin/end put event
+    // record nodes into it (cudaEventRecordExternal) instead of recording
+    // on the stream; the graph's replays then time its launches as they run
+    bool capture = false;
     std::vector<TimedLaunch> pending;
     // begin returns the record's index; end closes that record (or the last)
     int begin(cudaStream_t s, int kernel, int level, int64_t units);

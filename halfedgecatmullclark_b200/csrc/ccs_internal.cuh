@@ -112,12 +112,14 @@ struct CageTables {
     const int32_t* __restrict__ f2h;
     const int32_t* __restrict__ fsz;   // cage face sizes
     const float* __restrict__ uvs;     // U x 2
+    const int32_t* __restrict__ vshape;  // cage vertex ring shapes (DevCage::vshape), or null
     CageCounts n;
 };
 
 __host__ __device__ inline CageTables make_cage_tables(const DevCage& c) {
     CageTables t;
     t.he = c.he; t.v2h = c.v2h; t.e2h = c.e2h; t.f2h = c.f2h; t.fsz = c.fsz; t.uvs = c.uvs;
+    t.vshape = c.vshape;
     t.n.V = c.V; t.n.F = c.F; t.n.E = c.E; t.n.H = c.H;
     return t;
 }

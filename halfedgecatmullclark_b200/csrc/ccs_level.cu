@@ -140,9 +140,80 @@ k_crease_stats(QuadView<RW> L, float4* __restrict__ out, int32_t Vold) {
     if (i < L.C) crease_stats_item(L, Vold, out, (int32_t)i);
 }
 
+// Shape statistics of every level 1..D-1 in one launch: item i of the packed
+// table (level j + 1 in [off[j], off[j + 1]), V(j) entries) is vertex
+// i - off[j] of level j + 1.
+static constexpr int kMaxShapeLevels = 32;
+struct ShapeLevels {
+    int64_t off[kMaxShapeLevels + 1];
+    int32_t n = 0;
+};
+
+__device__ __forceinline__ void shape_levels_item(const CageTables& t, float4* __restrict__ stats,
+                                                  const ShapeLevels& sl, int64_t i) {
+    int j = 0;
+    while (j + 1 < sl.n && i >= sl.off[j + 1]) ++j;
+    shape_stats_item(t, j + 1, stats + sl.off[j], (int32_t)(i - sl.off[j]));
+}
+
+// The second stream's share of the cage step in one launch: blocks
+// [0, nbT) refine the cage's halfedges (4 children each, + UV codes),
+// [nbT, nbT + nbC) its creases, the rest build the shape half of every
+// level's ring statistics (nbT = nbC = 0: the statistics alone).
+template <int RW, bool UV>
+__global__ void __launch_bounds__(kBlockL)
+k_cage_side(CageTables t, int32_t* __restrict__ recOut, const cc_Crease* __restrict__ crIn,
+            cc_Crease* __restrict__ crOut, int32_t C, float4* __restrict__ stats, ShapeLevels sl, int nbT,
+            int nbC) {
+    const int b = blockIdx.x;
+    if (b < nbT) {
+        const int64_t c = (int64_t)b * kBlockL + threadIdx.x;
+        if (c < 4 * (int64_t)t.n.H) cage_topology_item<RW, true, UV>(t, recOut, c);
+        return;
+    }
+    if (b < nbT + nbC) {
+        const int64_t e = (int64_t)(b - nbT) * kBlockL + threadIdx.x;
+        if (e < C) crease_item(crIn, crOut, (int32_t)e);
+        return;
+    }
+    const int64_t i = (int64_t)(b - nbT - nbC) * kBlockL + threadIdx.x;
+    if (i < sl.off[sl.n]) shape_levels_item(t, stats, sl, i);
+}
+
 // ---------------------------------------------------------------------------
 // host
 // ---------------------------------------------------------------------------
+// The packed layout of the statistics of levels 1..D-1 (false: none kept).
+static bool shape_levels(const Ctx& c, ShapeLevels* sl) {
+    const int n = c.D - 1;
+    if (!c.stats || !c.statsOff || n < 1 || n > kMaxShapeLevels) return false;
+    sl->n = n;
+    for (int j = 0; j < n; ++j) sl->off[j] = c.statsOff[j + 1];
+    sl->off[n] = c.statsOff[n] + c.lv[n - 1].V;
+    return true;
+}
+
+// One k_cage_side launch on `s`: with `topo` the cage's topology and creases
+// beside the statistics (profiled as "cage_side"), else the statistics alone
+// ("ring_stats" at level 0, every level).
+template <int RW, bool UV>
+static void cage_side_launch(const Ctx& c, const ShapeLevels& sl, bool topo, cudaStream_t s) {
+    const int32_t C = c.lv[0].C;
+    const int nbT = topo ? (int)nblocksL(4 * (int64_t)c.lv[0].H) : 0;
+    const int nbC = topo ? (int)nblocksL(C) : 0;
+    const unsigned nb = (unsigned)(nbT + nbC) + nblocksL(sl.off[sl.n]);
+    c.prof->begin(s, topo ? CCS_K_CAGE_SIDE : CCS_K_RING_STATS, 0, sl.off[sl.n]);
+    k_cage_side<RW, UV><<<nb, kBlockL, 0, s>>>(make_cage_tables(*c.cage), c.he + (int64_t)RW * c.lv[1].heOff,
+                                              c.cage->cr, c.cr + c.lv[1].crOff, C, c.stats, sl, nbT, nbC);
+    c.prof->end(s);
+}
+
+static void cage_side(const Ctx& c, const ShapeLevels& sl, bool topo, bool uv, cudaStream_t s) {
+    if (c.rw == 4 && uv) cage_side_launch<4, true>(c, sl, topo, s);
+    else if (c.rw == 4) cage_side_launch<4, false>(c, sl, topo, s);
+    else cage_side_launch<3, false>(c, sl, topo, s);
+}
+
 template <int RW>
 static QuadView<RW> quad_view_l(const Ctx& c, int d) {
     QuadView<RW> L;
@@ -183,6 +254,15 @@ static void ring_stats_level(const Ctx& c, int d, cudaStream_t s) {
 }
 
 cudaError_t run_ring_stats(const Ctx& c) {
+    ShapeLevels sl;
+    if (shape_levels(c, &sl)) {
+        cage_side(c, sl, false, false, c.stream);       // the shape half of every level
+        for (int d = 1; d < c.D; ++d) {
+            if (c.rw == 4) crease_stats_level<4>(c, d, c.stream);
+            else crease_stats_level<3>(c, d, c.stream);
+        }
+        return cudaGetLastError();
+    }
     for (int d = 1; d < c.D; ++d) {
         if (c.rw == 4) ring_stats_level<4>(c, d, c.stream);
         else ring_stats_level<3>(c, d, c.stream);
@@ -370,13 +450,18 @@ static cudaError_t fused_levels(const Ctx& c, bool topo, bool uv, float* pts, bo
 cudaError_t run_fused(const Ctx& c, bool topo, const float* cagePts, float* pts, int mode, bool det) {
     const bool creased = mode == CCS_POINTS_SCATTER;
     const bool uv = c.cage->U > 0 && c.rw == 4;
-    // beside the cage step's points: its topology and creases, then the shape
-    // half of every level's ring statistics
+    // beside the cage step's points, on the second stream: its topology and
+    // creases and the shape half of every level's ring statistics, in one
+    // launch when the statistics are kept
     Fork shapes(c, topo && c.stats);
-    if (topo)
+    ShapeLevels sl;
+    const bool side = topo && shape_levels(c, &sl);
+    if (side) cage_side(c, sl, true, uv, shapes.stream());
+    else if (topo)
         for (int d = 1; d < c.D; ++d) shape_stats_level(c, d, shapes.stream());
     const int step = c.prof->begin(c.stream, CCS_K_STEP, 0, c.lv[0].H);
-    cudaError_t e = run_cage_step(c, topo, uv, cagePts, pts + 3 * c.lv[1].ptOff, mode, det, shapes.stream());
+    cudaError_t e = run_cage_step(c, topo && !side, uv, cagePts, pts + 3 * c.lv[1].ptOff, mode, det,
+                                  shapes.stream());
     c.prof->end(c.stream, step);
     if (e == cudaSuccess) {
         if (c.rw == 4)

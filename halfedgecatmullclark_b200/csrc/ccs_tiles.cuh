@@ -1174,6 +1174,12 @@ __device__ __forceinline__ void old_vertex_shape(const CageTables& t, int32_t v,
         return;
     }
     if (v >= n.V) { valence = t.fsz[v - n.V]; bnd = false; return; }
+    if (t.vshape) {                                  // a cage vertex, its shape kept
+        const int32_t x = t.vshape[v];
+        valence = x & 0x3FFFFFFF;
+        bnd = (x >> 30) & 1;
+        return;
+    }
     // a cage vertex: its ring in the cage (twin(prev h) forward, next(twin h) back)
     const int32_t h0 = t.v2h[v];
     int32_t cntv = 1, x = h0, guard = 0;

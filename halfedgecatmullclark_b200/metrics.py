@@ -32,12 +32,18 @@ def level_bytes(lv: dict, nxt: dict, rec: int = 16, uv: bool = True, cage: bool 
     return int(topo + creases + points)
 
 
-def kernel_bytes(kernel: str, lv: dict, rec: int = 16, prev: dict | None = None) -> int:
+def kernel_bytes(kernel: str, lv: dict, rec: int = 16, prev: dict | None = None, units: int | None = None) -> int:
     """Per-launch algorithmic bytes of one kernel at parent depth `lv`
     (`prev` = the level before it, which gives the exact count of older
     vertices at depth 1, where the quad-structure count below does not
-    hold)."""
+    hold; `units` = the launch's own item count where it is not a level's:
+    the statistics entries of every level for "cage_side" and the
+    every-level "ring_stats" launch)."""
     H, V, F, E, C = lv["H"], lv["V"], lv["F"], lv["E"], lv["C"]
+    if kernel == "cage_side":
+        # cage records in, 4 child records out, cage creases in and their
+        # children out, one float4 of shape statistics per entry out
+        return int(28 * H + 4 * rec * H + 36 * C + 16 * (units or 0))
     if kernel in ("topology", "uvs"):
         return int(rec * H + 4 * rec * H)
     if kernel == "creases":
@@ -77,7 +83,9 @@ def kernel_bytes(kernel: str, lv: dict, rec: int = 16, prev: dict | None = None)
     if kernel == "ring_stats":
         # shape half (k_shape_stats): valence and boundary from the vertex
         # numbering and the cage alone -- no level data read; one float4 per
-        # older vertex out.
+        # older vertex out (every level's entries when `units` is given).
+        if units is not None:
+            return int(16 * units)
         return int(16 * (prev["V"] if prev is not None else max(V - nb, 0)))
     if kernel == "crease_stats":
         # crease half (k_crease_stats): the level's crease records in; the

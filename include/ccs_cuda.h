@@ -372,10 +372,15 @@ enum {
     CCS_K_LEVEL_STEP_POINTS = 18 /* depth >= 2: all points of a step in one launch */,
     CCS_K_ADJ_STEP = 19 /* adjoint of a depth >= 2 step in one launch */,
     CCS_K_CREASE_STATS = 20 /* crease half of a level's ring statistics (ring_stats = the shape half) */,
-    CCS_K_COUNT = 21
+    CCS_K_CAGE_SIDE = 21 /* cage topology, cage creases and every level's shape statistics in one launch */,
+    CCS_K_COUNT = 22
 };
-/* When enabled, every launch of the subd is bracketed by CUDA events on its
- * stream (and CUDA graphs are not used). */
+/* When enabled, every launch of the subd is bracketed by CUDA events.  A
+ * refinement operation then replays a CUDA graph of its own whose event
+ * record nodes time each launch as the graph runs it (the call waits for the
+ * stream after each replay); with CCS_FLAG_NO_GRAPH, or while the caller
+ * captures the stream, and for the adjoint entry points, the launches are
+ * direct and the events are recorded on the stream. */
 int ccs_SetProfiling_cuda(cc_Subd *subd, int enable);
 /* Copies up to `cap` records of the launches since the last call (waits for
  * the stream); returns the number of records, or a negative status. */

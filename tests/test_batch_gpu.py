@@ -144,3 +144,47 @@ def test_split_schedule_matches_fused(workloads):
     assert np.array_equal(outs[0][0], outs[1][0])
     assert np.array_equal(outs[0][1].view(np.uint32), outs[1][1].view(np.uint32))
     assert rel_err(outs[1][2], outs[0][2]) <= 1e-5
+
+
+@pytest.mark.slow
+def test_batch_config5_distribution_matches_reference():
+    """64 cages drawn from the batched workload's own distribution (faces
+    log-uniform in [50, 5000], mixed triangles / quads / pentagons, 0-10 %
+    crease edges with sharpness U[0, 4], depths uniform in {2..6}; about 0.5 G
+    refined halfedges), each against the reference's own ccs_Refine_Scatter
+    (CatmullClark.h:3060-3064, compiled from its sources): topology and
+    creases bit-exact, default points within 1e-5; the deterministic batch bit
+    for bit against the reference's points pass on one thread."""
+    import os
+    from halfedgecatmullclark_b200 import _native as N
+    from halfedgecatmullclark_b200 import configs
+    from halfedgecatmullclark_b200.batch import Batch
+    from oracle import refimpl
+    if not refimpl.available():
+        pytest.skip("oracle/_ref not built")
+    ws = configs.batch_cages(count=64, seed=21)
+    assert {w.depth for w in ws} == {2, 3, 4, 5, 6}
+    cores = os.cpu_count() or 1
+    with Batch([w.cage for w in ws], [w.depth for w in ws]) as b, \
+            Batch([w.cage for w in ws], [w.depth for w in ws], N.FLAG_DETERMINISTIC) as bd:
+        b.refine()
+        bd.refine()
+        b.synchronize()
+        bd.synchronize()
+        for i, w in enumerate(ws):
+            refimpl.set_threads(cores)
+            r = refimpl.RefSubd(w.cage, w.depth)
+            try:
+                r.refine("scatter")
+                rhe, rcr, rpts = r.halfedges(), r.creases(), r.points()
+                he, cr, pts = b.download(i)
+                assert np.array_equal(he[:, :3], rhe[:, :3]), w.name
+                assert np.array_equal(cr.view(np.uint8), rcr.view(np.uint8)), w.name
+                assert rel_err(pts, rpts) <= 1e-5, (w.name, rel_err(pts, rpts))
+                refimpl.set_threads(1)
+                r.call("ccs_RefineVertexPoints_Scatter")
+                dpts = bd.download(i)[2]
+                assert np.array_equal(dpts.view(np.uint32), r.points().view(np.uint32)), w.name
+            finally:
+                refimpl.set_threads(cores)
+                r.close()

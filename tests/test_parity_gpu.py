@@ -284,3 +284,36 @@ def test_height_grid_depth5_properties():
                 assert np.array_equal(p.view(np.uint32), o32.view(np.uint32))
             else:
                 assert rel_err(p, o32) <= TOL_POINTS
+
+
+def test_profiled_refine_times_the_graph_and_matches():
+    """With profiling on, a refine replays a graph of its own with event
+    record nodes: every launch and every step d -> d+1 comes back with a
+    positive device time, the steps' records cover depths 0..D-1, and the
+    results equal those of the unprofiled graph (deterministic pass: bit for
+    bit); a second profiled refine gives the same records again."""
+    import torch
+    from halfedgecatmullclark_b200 import _native as N
+    from halfedgecatmullclark_b200 import configs
+    from halfedgecatmullclark_b200.subd import Subd
+    w = configs.mixed_torus(nu=12, nv=10, strip=4, depth=4, seed=7)
+    with Subd(w.cage, w.depth, N.FLAG_DETERMINISTIC) as s:
+        st = torch.cuda.Stream()
+        s.set_stream(st)
+        s.refine_scatter()
+        s.download()
+        he0, pts0 = s.halfedges(), s.points()
+        s.set_profiling(True)
+        counts = []
+        for _ in range(2):
+            s.refine_scatter()
+            recs = s.read_profile(1 << 12)
+            counts.append(len(recs))
+            assert recs and all(r["ms"] > 0 for r in recs)
+            steps = sorted(r["level"] for r in recs if r["kernel"] == "step")
+            assert steps == list(range(w.depth))
+        s.set_profiling(False)
+        assert counts[0] == counts[1]
+        s.download()
+        assert np.array_equal(s.halfedges(), he0)
+        assert np.array_equal(s.points().view(np.uint32), pts0.view(np.uint32))
