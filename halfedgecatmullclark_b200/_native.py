@@ -28,7 +28,8 @@ POINT_MODES = {"scatter": 0, "gather": 1, "nocreases_scatter": 2, "nocreases_gat
 KERNEL_NAMES = ["topology", "creases", "face_points", "edge_points", "vertex_points", "clear",
                 "level_fused", "adjoint", "uvs", "level_points", "old_vertices", "ring_stats", "adj_edges",
                 "adj_faces", "adj_vertices", "exact_points", "step", "level_step", "level_step_points",
-                "adj_step", "crease_stats", "cage_side"]
+                "adj_step", "crease_stats", "cage_side", "cage_map",
+                "adj_cage_map"]
 
 
 class CcsError(RuntimeError):
@@ -106,6 +107,8 @@ SIGNATURES = {
     "ccs_RefinePointsDevice_cuda": ([_P, _P, _P, _I, _P], _I),
     "ccs_AdjointPointsDevice_cuda": ([_P, _P, _P, _P], _I),
     "ccs_HalfedgeNormals_cuda": ([_P, _P, _P, ctypes.c_int, _P], _I),
+    "ccs_CageStepMatrix_cuda": ([_P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int32),
+                                 ctypes.POINTER(ctypes.c_int64), _P, _P, _P, ctypes.c_int64], _I),
     "ccs_ExportObj_cuda": ([_P, ctypes.c_int32, ctypes.c_char_p], _I),
     "ccs_AdjointPointsDeviceNoAlloc_cuda": ([_P, _P, _P, _P], _I),
     "ccs_BatchCreate_cuda": ([_P, _P, ctypes.c_int32, _U, ctypes.POINTER(_P)], _I),

@@ -150,7 +150,13 @@ cudaError_t run_adjoint(const Ctx& c, const float* gradPts, float* work, float* 
     for (int d = c.D - 1; d >= 0; --d) {
         float* gNew = (finestInPlace && d == c.D - 1) ? const_cast<float*>(gradPts) + 3 * c.lv[d + 1].ptOff
                                                       : work + 3 * c.lv[d + 1].ptOff;
-        if (d == 0) {
+        if (d == 0 && c.maps && c.maps->creasedT.rows == c.cage->V) {
+            // dL/dcage = S^T dL/dP1 with the transposed map of the cage step
+            c.prof->begin(c.stream, CCS_K_ADJ_CAGE_MAP, 0, c.cage->V);
+            st = launch_cage_map(c.maps->creasedT, gNew, gradCage, c.stream);
+            c.prof->end(c.stream);
+            if (st != cudaSuccess) return st;
+        } else if (d == 0) {
             CageView L;
             L.t = cage_tables_a(*c.cage);
             L.cr = c.cage->cr;

@@ -187,6 +187,8 @@ struct SubdImpl {
     bool pinned = true;
     bool topo_ready = false, creases_ready = false;
     bool fusable = true;           // twin relation holds: fused kernels allowed
+    CageMaps maps;                 // the cage step as sparse linear maps
+    bool haveMaps = false;
     std::vector<CUtensorMap> childMaps;  // per level d: TMA map of the child records it writes
     std::vector<uint8_t> childMapOk;
     Profiler prof;
@@ -202,6 +204,7 @@ struct SubdImpl {
         c.side = side; c.forkEv = forkEv; c.joinEv = joinEv;
         c.stats = stats; c.statsOff = statsOff.data();
         c.fusable = fusable;
+        c.maps = haveMaps ? &maps : nullptr;
         if (!childMaps.empty()) { c.childMaps = childMaps.data(); c.childMapOk = childMapOk.data(); }
         return c;
     }
@@ -224,6 +227,7 @@ static void free_impl(SubdImpl* s) {
     for (auto& kv : s->profTemplates) destroy_events(kv.second);
     cudaFree(s->dc.he); cudaFree(s->dc.cr); cudaFree(s->dc.pts); cudaFree(s->dc.uvs);
     cudaFree(s->dc.v2h); cudaFree(s->dc.e2h); cudaFree(s->dc.f2h); cudaFree(s->dc.fsz); cudaFree(s->dc.vshape);
+    free_cage_map(&s->maps.creased); free_cage_map(&s->maps.creasedT); free_cage_map(&s->maps.smooth);
     cudaFree(s->he); cudaFree(s->cr); cudaFree(s->pts); cudaFree(s->work); cudaFree(s->err); cudaFree(s->stats);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     if (s->side) cudaStreamDestroy(s->side);
@@ -362,6 +366,11 @@ static int create(const cc_Mesh* cage, int32_t D, uint32_t flags, cc_Subd** out)
     }
     st = upload_cage(s, cage);
     if (st != CCS_OK) { free_impl(s); return st; }
+    // the cage step of the default pass as linear maps (fixed topology and
+    // sharpness), built once
+    st = build_cage_maps(cage, &s->maps);
+    if (st != CCS_OK) { free_impl(s); return st; }
+    s->haveMaps = true;
     if (s->rw == 4) {
         s->childMaps.resize((size_t)D + 1);
         s->childMapOk.assign((size_t)D + 1, 0);
@@ -510,6 +519,7 @@ int adjoint_into(const cc_Subd* subd, const float* gradPoints, float* gradCage, 
 }
 
 int set_last_error(int status) { return ret(status); }
+int validate_cage_host(const cc_Mesh* m) { return validate_cage(m); }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link
 // against the driver library)
@@ -795,7 +805,7 @@ const char* ccs_KernelName_cuda(int kernel) {
                                   "clear", "level_fused", "adjoint", "uvs", "level_points", "old_vertices",
                                   "ring_stats", "adj_edges", "adj_faces", "adj_vertices", "exact_points", "step",
                                   "level_step", "level_step_points", "adj_step", "crease_stats",
-                                  "cage_side"};
+                                  "cage_side", "cage_map", "adj_cage_map"};
     static_assert(sizeof(names) / sizeof(names[0]) == CCS_K_COUNT, "one name per kernel id");
     return (kernel >= 0 && kernel < CCS_K_COUNT) ? names[kernel] : "unknown";
 }

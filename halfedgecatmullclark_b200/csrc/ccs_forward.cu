@@ -415,8 +415,16 @@ cudaError_t run_cage_step(const Ctx& c, bool topo, bool uv, const float* cagePts
         points_level(c, cage_view(c), cagePts, pout, mode, det);
         return cudaGetLastError();
     }
-    const CageView L = cage_view(c);
     const bool creased = mode == CCS_POINTS_SCATTER;
+    if (c.maps) {
+        // every point of depth 1 as one sparse product of the cage points
+        const CageMap& m = creased ? c.maps->creased : c.maps->smooth;
+        c.prof->begin(c.stream, CCS_K_CAGE_MAP, 0, m.rows);
+        const cudaError_t e = launch_cage_map(m, cagePts, pout, c.stream);
+        c.prof->end(c.stream);
+        return e;
+    }
+    const CageView L = cage_view(c);
     c.prof->begin(c.stream, CCS_K_FACE_POINTS, 0, L.H);
     k_face_points_clear<CageView><<<nblocks(L.F > L.V ? L.F : L.V), kBlock, 0, c.stream>>>(L, cagePts, pout);
     c.prof->end(c.stream);

@@ -61,6 +61,25 @@ struct DevCage {
     int32_t V = 0, U = 0, H = 0, E = 0, F = 0;
 };
 
+// The cage step of a point rule as a sparse linear map (ccs_cagemap.cu):
+// CSR rows over the cage points, rows in depth 1's layout (or, for the
+// transpose, one row per cage vertex over depth 1's points).
+struct CageMap {
+    int32_t* rowptr = nullptr;
+    int32_t* col = nullptr;
+    float* w = nullptr;
+    int32_t rows = 0;
+    int64_t nnz = 0;
+};
+struct CageMaps {
+    CageMap creased;    // the scatter rule (:1437-1463, :1602-1648, :1872-1991)
+    CageMap creasedT;   // its transpose: the adjoint's cage level
+    CageMap smooth;     // the NoCreases scatter rule (:1517-1548, :1713-1756)
+};
+int build_cage_maps(const cc_Mesh* cage, CageMaps* out);
+void free_cage_map(CageMap* m);
+cudaError_t launch_cage_map(const CageMap& m, const float* in, float* out, cudaStream_t s);
+
 // Counts of one depth and the offsets of its arrays in the packed hierarchy.
 struct Level {
     int32_t d;
@@ -108,6 +127,8 @@ struct Ctx {
     float4* stats = nullptr;
     const int64_t* statsOff = nullptr;
     bool fusable = true;         // the twin relation vertex(twin h) = vertex(next h) holds
+    // the cage step's linear maps (default atomic pass; null = not built)
+    const CageMaps* maps = nullptr;
     // TMA tensor maps of the child records each level d writes (level d+1's
     // records as rows of 128 bytes), indexed by d; null / 0 = not available
     const CUtensorMap* childMaps = nullptr;

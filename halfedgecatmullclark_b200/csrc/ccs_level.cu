@@ -75,6 +75,9 @@ k_level_a(LevelArgs a) {
     }
     __shared__ __align__(128) int32_t tile[kBlockL * 4 * RW];
     tile_level_a<kBlockL, RW, TOPO, UV, true, CREASED>(a, (int64_t)blockIdx.x * kBlockL, tile);
+    // the slots the step after next accumulates into (zeroNextN = 0: none)
+    for (int64_t i = (int64_t)blockIdx.x * kBlockL + threadIdx.x; i < a.zeroNextN; i += (int64_t)nbH * kBlockL)
+        a.zeroNext[i] = 0.0f;
 }
 
 // depth d >= 2, default pass: kernel A and the vertex pass in one launch
@@ -340,7 +343,8 @@ static void level_ab(const Ctx& c, int d, bool topo, bool uv, float* pts) {
 }
 
 template <int RW, bool CREASED>
-static void level_a(const Ctx& c, int d, bool topo, bool uv, const float* pin, float* pout, bool zeroV) {
+static void level_a(const Ctx& c, int d, bool topo, bool uv, const float* pin, float* pout, bool zeroV,
+                    float* clearNext = nullptr) {
     const Level& lv = c.lv[d];
     LevelArgs a;
     a.in = c.he + (int64_t)RW * lv.heOff;
@@ -352,6 +356,7 @@ static void level_a(const Ctx& c, int d, bool topo, bool uv, const float* pin, f
     a.H = lv.H; a.V = lv.V; a.F = lv.F; a.E = lv.E; a.C = lv.C;
     a.zeroV = zeroV ? 1 : 0;
     if (topo) fold_crease_stats(c, d, a);
+    if (clearNext) next_slots(c, d, clearNext, a);   // clearNext = the points of every depth
     const unsigned nb = nblocksL(lv.H) + (topo ? nblocksL(lv.C) : 0u);
     c.prof->begin(c.stream, topo ? CCS_K_LEVEL_FUSED : CCS_K_FACE_POINTS, d, lv.H);
     if (topo) {
@@ -416,23 +421,24 @@ static cudaError_t fused_levels(const Ctx& c, bool topo, bool uv, float* pts, bo
         const float* pin = pts + 3 * c.lv[d].ptOff;
         float* pout = pts + 3 * c.lv[d + 1].ptOff;
         const int step = c.prof->begin(c.stream, CCS_K_STEP, d, c.lv[d].H);
+        // at depth 1 kernel A also clears the slots depth 3 accumulates into
+        // (the first k_level_ab step's; each k_level_ab clears the next's)
+        float* clear3 = (ab && d == 1 && c.D >= 3) ? pts : nullptr;
         if (topo && d == 1) {
             // level 1's creases come from the cage step: the crease half of
             // its statistics beside kernel A (whose crease items add level 2's)
             shapes.join();
             Fork f(c);
             crease_stats_level<RW>(c, 1, f.stream());
-            level_a<RW, CREASED>(c, d, topo, uv, pin, pout, !det);
+            level_a<RW, CREASED>(c, d, topo, uv, pin, pout, !det, clear3);
             f.join();
         } else if (ab && d >= 2) {
             level_ab<RW, CREASED>(c, d, topo, uv, pts);
             c.prof->end(c.stream, step);
             continue;
         } else {
-            level_a<RW, CREASED>(c, d, topo, uv, pin, pout, !det);
+            level_a<RW, CREASED>(c, d, topo, uv, pin, pout, !det, clear3);
         }
-        if (ab && d == 1 && c.D >= 3)
-            cudaMemsetAsync(pts + 3 * c.lv[3].ptOff, 0, sizeof(float) * 3 * (size_t)c.lv[2].V, c.stream);
         if (!det) {
             level_b<RW, CREASED>(c, d, pin, pout);
         } else if (d >= 2) {

@@ -39,6 +39,26 @@ def max_supported_depth(cage: Cage) -> int:
     return int(N.lib().ccs_MaxSupportedDepth_cuda(ctypes.byref(m)))
 
 
+def cage_step_matrix(cage: Cage, mode: str = "scatter", transpose: bool = False):
+    """The cage step of a point rule as CSR arrays (rowptr, col, w): depth-1
+    points = S @ cage points (ccs_CageStepMatrix_cuda; host only).  With
+    `transpose`, S^T (the adjoint's cage level)."""
+    L = N.lib()
+    m = cage.as_cc_mesh()
+    rows = ctypes.c_int32()
+    nnz = ctypes.c_int64()
+    md = N.POINT_MODES[mode]
+    N.check(L.ccs_CageStepMatrix_cuda(ctypes.byref(m), md, 1 if transpose else 0, ctypes.byref(rows),
+                                      ctypes.byref(nnz), None, None, None, 0), "ccs_CageStepMatrix_cuda")
+    rp = np.zeros(rows.value + 1, np.int32)
+    col = np.zeros(max(nnz.value, 1), np.int32)
+    w = np.zeros(max(nnz.value, 1), np.float32)
+    N.check(L.ccs_CageStepMatrix_cuda(ctypes.byref(m), md, 1 if transpose else 0, ctypes.byref(rows),
+                                      ctypes.byref(nnz), rp.ctypes.data, col.ctypes.data, w.ctypes.data,
+                                      nnz.value), "ccs_CageStepMatrix_cuda")
+    return rp, col[:nnz.value], w[:nnz.value]
+
+
 class Subd:
     """A refined hierarchy living on the GPU (and mirrored on the host)."""
 

@@ -258,6 +258,20 @@ int ccs_AdjointPointsDevice_cuda(cc_Subd *subd, const float *gradPoints, float *
 int ccs_AdjointPointsDeviceNoAlloc_cuda(cc_Subd *subd, const float *gradPoints, float *gradCage,
                                         void *stream);
 
+/* The cage step of a point rule as a sparse matrix (host only; no GPU work;
+ * no counterpart in the reference, whose rules it applies symbolically:
+ * CatmullClark.h:1437-1463, :1602-1648 and :1872-1991 for
+ * mode = CCS_POINTS_SCATTER; :1517-1548 and :1713-1756 for
+ * CCS_POINTS_NOCREASES_SCATTER).  For a fixed topology and sharpness the
+ * points of depth 1 are S x (cage points); rows are depth 1's points
+ * ([old vertices | faces | edges]), columns cage vertices; `transpose`
+ * (scatter rule only) gives S^T, the adjoint's cage level.  This is the map
+ * the default pass evaluates as its cage step.  CSR arrays: rowptr (rows + 1
+ * entries), col and w (nnz entries).  Call with cap = 0 for *rows and *nnz,
+ * then with arrays of those sizes. */
+int ccs_CageStepMatrix_cuda(const cc_Mesh *cage, int mode, int transpose, int32_t *rows, int64_t *nnz,
+                            int32_t *rowptr, int32_t *col, float *w, int64_t cap);
+
 /* Per-halfedge normals of the finest level, the refined-surface consumer of
  * the reference's GLSL library (glsl/CatmullClark_Scatter.glsl:931-960,
  * ccs_HalfedgeNormal_Fast / ccs_HalfedgeNormal): `normals` (device, H(D) x 3
@@ -373,7 +387,9 @@ enum {
     CCS_K_ADJ_STEP = 19 /* adjoint of a depth >= 2 step in one launch */,
     CCS_K_CREASE_STATS = 20 /* crease half of a level's ring statistics (ring_stats = the shape half) */,
     CCS_K_CAGE_SIDE = 21 /* cage topology, cage creases and every level's shape statistics in one launch */,
-    CCS_K_COUNT = 22
+    CCS_K_CAGE_MAP = 22 /* the cage step's points as one sparse linear map (default pass) */,
+    CCS_K_ADJ_CAGE_MAP = 23 /* the adjoint's cage level: the transposed map */,
+    CCS_K_COUNT = 24
 };
 /* When enabled, every launch of the subd is bracketed by CUDA events.  A
  * refinement operation then replays a CUDA graph of its own whose event
