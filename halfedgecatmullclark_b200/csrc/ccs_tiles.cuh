@@ -57,6 +57,22 @@ __device__ __forceinline__ void tensor_store_tile(const void* tmap, const void* 
     asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
 }
 
+// The same two copies issued without the wait: the issuing thread must call
+// bulk_wait_read() before the block ends (or reuses the tile).
+__device__ __forceinline__ void bulk_store_tile_async(void* gdst, const void* ssrc, uint32_t bytes) {
+    const uint32_t s = (uint32_t)__cvta_generic_to_shared(ssrc);
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;"
+                 :: "l"(gdst), "r"(s), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void tensor_store_tile_async(const void* tmap, const void* ssrc, int32_t row) {
+    const uint32_t s = (uint32_t)__cvta_generic_to_shared(ssrc);
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];"
+                 :: "l"(tmap), "r"(0), "r"(row), "r"(s) : "memory");
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+
 __device__ __forceinline__ f3 shfl3(f3 v, int src) {
     return f3{__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src),
               __shfl_sync(0xffffffffu, v.z, src)};
@@ -507,7 +523,7 @@ __device__ __forceinline__ void tile_level_b(const QuadView<RW>& L, const float*
 // halfedges) from a 128-byte swizzled tile (1024-byte aligned): 16-byte chunk
 // c of row r sits at chunk c ^ (r & 7), which also spreads every
 // quarter-warp's stores over the 32 banks.
-template <int BLOCK, int RW, bool TOPO, bool UV, bool CREASED, bool TMAP = false>
+template <int BLOCK, int RW, bool TOPO, bool UV, bool CREASED, bool TMAP = false, int EARLY = 0>
 __device__ __forceinline__ void tile_level_ab(const LevelArgs& a, int64_t h0, int32_t* tile, int64_t zeroStride,
                                               const void* tmap = nullptr) {
     static_assert(!TMAP || (RW == 4 && BLOCK == 256), "tensor-store tiles are 256 sixteen-byte records wide");
@@ -523,6 +539,51 @@ __device__ __forceinline__ void tile_level_ab(const LevelArgs& a, int64_t h0, in
     const int32_t f = h >> 2;
     const int32_t ptw = __shfl_sync(full, tw, lp);
     const int32_t ped = __shfl_sync(full, ed, lp);
+
+    // child records through the shared tile and one bulk store (EARLY = 1:
+    // issued after the record's gathers, 2: before them -- both before the
+    // points, with the wait left to the end; 0: after the points)
+    auto child_records = [&]() {
+        const int lo = qb | ((k + 2) & 3);
+        const int32_t prev = (h & ~3) | ((k + 3) & 3), next = (h & ~3) | ((k + 1) & 3);
+        int32_t c_tw[4], c_ed[4], c_vx[4], uvc[4] = {rec.uv, 0, 0, 0};
+        if (UV) {
+            const float u = uv_dec_fast((uint32_t)rec.uv), v = uv_dec_fast((uint32_t)rec.uv >> 16);
+            const float un = __shfl_sync(full, u, ln), vn = __shfl_sync(full, v, ln);
+            const float uo = __shfl_sync(full, u, lo), vo = __shfl_sync(full, v, lo);
+            const float up = __shfl_sync(full, u, lp), vp = __shfl_sync(full, v, lp);
+            uvc[1] = uv_enc_fast(flerp(u, un, 0.5f), flerp(v, vn, 0.5f));
+            uvc[2] = uv_enc_fast(fquarter(fadd(fadd(fadd(u, un), uo), up)),
+                                 fquarter(fadd(fadd(fadd(v, vn), vo), vp)));
+            uvc[3] = uv_enc_fast(flerp(u, up, 0.5f), flerp(v, vp, 0.5f));
+        }
+        c_tw[0] = child(qnext(tw), 3); c_tw[1] = child(next, 2); c_tw[2] = child(prev, 1); c_tw[3] = child(ptw, 0);
+        c_ed[0] = 2 * ed + (h > tw ? 0 : 1); c_ed[1] = 2 * a.E + h; c_ed[2] = 2 * a.E + prev;
+        c_ed[3] = 2 * ped + (prev > ptw ? 1 : 0);
+        c_vx[0] = vx; c_vx[1] = a.V + a.F + ed; c_vx[2] = a.V + f; c_vx[3] = a.V + a.F + ped;
+        if constexpr (TMAP) {
+            const int r = tid >> 1, sw = r & 7, cb = (tid & 1) << 2;
+            int4* row = reinterpret_cast<int4*>(tile) + 8 * r;
+#pragma unroll
+            for (int m = 0; m < 4; ++m) row[(cb + m) ^ sw] = make_int4(c_tw[m], c_ed[m], c_vx[m], UV ? uvc[m] : 0);
+        } else {
+            put_children<RW, UV>(tile, tid, lane, c_tw, c_ed, c_vx, uvc);
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            if constexpr (TMAP) {
+                if (EARLY != 0) tensor_store_tile_async(tmap, tile, (int32_t)(h0 >> 1));
+                else tensor_store_tile(tmap, tile, (int32_t)(h0 >> 1));
+            } else {
+                const int64_t n = (a.H - h0) < BLOCK ? (a.H - h0) : BLOCK;
+                if (EARLY != 0) bulk_store_tile_async(a.out + 4 * RW * h0, tile, (uint32_t)(n * 16 * RW));
+                else bulk_store_tile(a.out + 4 * RW * h0, tile, (uint32_t)(n * 16 * RW));
+            }
+        }
+    };
+
+    if constexpr (TOPO && EARLY == 2) child_records();
 
     // every load that needs only the record, issued before any is used
     const int sibK = k == 1 ? ((((j + 1) & 3) << 2) | 2) : ((((j + 3) & 3) << 2) | 1);
@@ -545,6 +606,9 @@ __device__ __forceinline__ void tile_level_ab(const LevelArgs& a, int64_t h0, in
         qF = ld3(a.pin + 3 * (int64_t)vF);
         qX = ld3(a.pin + 3 * (int64_t)vX);
     }
+
+    // EARLY = 1: the child records go out while those loads are in flight
+    if constexpr (TOPO && EARLY == 1) child_records();
 
     // face point, and the next vertex's point from its shuffles
     f3 pn, Fp;
@@ -632,43 +696,9 @@ __device__ __forceinline__ void tile_level_ab(const LevelArgs& a, int64_t h0, in
     // clear this thread's share of the next level's accumulation slots
     for (int64_t i = h64; i < a.zeroNextN; i += zeroStride) a.zeroNext[i] = 0.0f;
 
-    // child records through the shared tile and one bulk store
-    if (TOPO) {
-        const int lo = qb | ((k + 2) & 3);
-        const int32_t prev = (h & ~3) | ((k + 3) & 3), next = (h & ~3) | ((k + 1) & 3);
-        int32_t c_tw[4], c_ed[4], c_vx[4], uvc[4] = {rec.uv, 0, 0, 0};
-        if (UV) {
-            const float u = uv_dec_fast((uint32_t)rec.uv), v = uv_dec_fast((uint32_t)rec.uv >> 16);
-            const float un = __shfl_sync(full, u, ln), vn = __shfl_sync(full, v, ln);
-            const float uo = __shfl_sync(full, u, lo), vo = __shfl_sync(full, v, lo);
-            const float up = __shfl_sync(full, u, lp), vp = __shfl_sync(full, v, lp);
-            uvc[1] = uv_enc_fast(flerp(u, un, 0.5f), flerp(v, vn, 0.5f));
-            uvc[2] = uv_enc_fast(fquarter(fadd(fadd(fadd(u, un), uo), up)),
-                                 fquarter(fadd(fadd(fadd(v, vn), vo), vp)));
-            uvc[3] = uv_enc_fast(flerp(u, up, 0.5f), flerp(v, vp, 0.5f));
-        }
-        c_tw[0] = child(qnext(tw), 3); c_tw[1] = child(next, 2); c_tw[2] = child(prev, 1); c_tw[3] = child(ptw, 0);
-        c_ed[0] = 2 * ed + (h > tw ? 0 : 1); c_ed[1] = 2 * a.E + h; c_ed[2] = 2 * a.E + prev;
-        c_ed[3] = 2 * ped + (prev > ptw ? 1 : 0);
-        c_vx[0] = vx; c_vx[1] = a.V + a.F + ed; c_vx[2] = a.V + f; c_vx[3] = a.V + a.F + ped;
-        if constexpr (TMAP) {
-            const int r = tid >> 1, sw = r & 7, cb = (tid & 1) << 2;
-            int4* row = reinterpret_cast<int4*>(tile) + 8 * r;
-#pragma unroll
-            for (int m = 0; m < 4; ++m) row[(cb + m) ^ sw] = make_int4(c_tw[m], c_ed[m], c_vx[m], UV ? uvc[m] : 0);
-        } else {
-            put_children<RW, UV>(tile, tid, lane, c_tw, c_ed, c_vx, uvc);
-        }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        if (tid == 0) {
-            if constexpr (TMAP) {
-                tensor_store_tile(tmap, tile, (int32_t)(h0 >> 1));
-            } else {
-                const int64_t n = (a.H - h0) < BLOCK ? (a.H - h0) : BLOCK;
-                bulk_store_tile(a.out + 4 * RW * h0, tile, (uint32_t)(n * 16 * RW));
-            }
-        }
+    if constexpr (TOPO && EARLY == 0) child_records();
+    if constexpr (TOPO && EARLY != 0) {
+        if (tid == 0) bulk_wait_read();
     }
 }
 
