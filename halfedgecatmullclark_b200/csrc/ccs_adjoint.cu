@@ -84,10 +84,26 @@ k_adj_quad_edges(QuadView<RW> L, float* __restrict__ gNew) {
 #ifndef CCS_ADJ_STEP_MIN_BLOCKS
 #define CCS_ADJ_STEP_MIN_BLOCKS 6
 #endif
+// blocks ahead whose records k_adj_quad_step asks L2 to fetch (0: none):
+// one wave, as k_level_ab (depth 5 of the headline workload: 0.362 ->
+// 0.352 ms)
+#ifndef CCS_ADJ_PREFETCH_AHEAD
+#define CCS_ADJ_PREFETCH_AHEAD 888
+#endif
 template <int RW>
 __global__ void __launch_bounds__(kBlockA, CCS_ADJ_STEP_MIN_BLOCKS)
 k_adj_quad_step(QuadView<RW> L, const float* __restrict__ gNew, float* __restrict__ gOld) {
     chain_wait_then_release();
+#if CCS_ADJ_PREFETCH_AHEAD > 0
+    if (threadIdx.x == 0) {
+        const int64_t p0 = ((int64_t)blockIdx.x + CCS_ADJ_PREFETCH_AHEAD) * kBlockA;
+        if (p0 < L.H) {
+            const int64_t n = (L.H - p0) < kBlockA ? (L.H - p0) : kBlockA;
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
+                         :: "l"(L.he + (int64_t)RW * p0), "r"((uint32_t)(n * 4 * RW)) : "memory");
+        }
+    }
+#endif
     adj_quad_step_tile<RW>(L, gNew, gOld, (int64_t)blockIdx.x * kBlockA);
 }
 

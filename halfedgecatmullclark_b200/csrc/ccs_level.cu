@@ -89,9 +89,17 @@ k_level_a(LevelArgs a) {
 // first, the tensor store left to drain while the points are computed
 // (measured at depth 5 of the headline workload: 0.480 ms, against 0.485
 // ms after the record's gathers are issued (1) and 0.489 ms after the
-// points (0))
+// points (0); letting only warp 0 wait for the tile at a split named
+// barrier added spills and measured 0.486 ms)
 #ifndef CCS_AB_EARLY_STORE
 #define CCS_AB_EARLY_STORE 2
+#endif
+// blocks ahead whose records k_level_ab asks L2 to fetch (0: none): one
+// wave of the grid, 148 SMs x 6 resident blocks.  Measured at depth 5 of the
+// headline workload: 0.478 -> 0.455 ms for the full step and 0.346 ->
+// 0.317 ms for the points-only step, the same for 444 to 1776 blocks ahead
+#ifndef CCS_AB_PREFETCH_AHEAD
+#define CCS_AB_PREFETCH_AHEAD 888
 #endif
 template <int RW, bool TOPO, bool UV, bool CREASED, bool TMAP>
 __global__ void __launch_bounds__(kBlockL, CCS_AB_MIN_BLOCKS)
@@ -107,6 +115,18 @@ k_level_ab(LevelArgs a, const __grid_constant__ CUtensorMap childMap) {
         }
         return;
     }
+#if CCS_AB_PREFETCH_AHEAD > 0
+    // the records of the tile about one wave ahead, fetched into L2 while
+    // this one runs (a bulk prefetch: no shared memory, no wait)
+    if (threadIdx.x == 0) {
+        const int64_t p0 = ((int64_t)blockIdx.x + CCS_AB_PREFETCH_AHEAD) * kBlockL;
+        if (p0 < a.H) {
+            const int64_t n = (a.H - p0) < kBlockL ? (a.H - p0) : kBlockL;
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
+                         :: "l"(a.in + (int64_t)RW * p0), "r"((uint32_t)(n * 4 * RW)) : "memory");
+        }
+    }
+#endif
     __shared__ __align__(1024) int32_t tile[TOPO ? kBlockL * 4 * RW : 4];
     // one tile per block: the child records' store is issued first and left
     // to drain while the points are computed
