@@ -174,43 +174,6 @@ __device__ __forceinline__ void for_tiles(const BatchArgs& a, int d, int phase, 
     }
 }
 
-// tiles ahead whose parent records a block of the one-pass steps asks L2 to
-// fetch (0: none).  With one block per tile the tile about one wave ahead;
-// in a persistent grid this block's next tile.
-#ifndef CCS_BATCH_PREFETCH_AHEAD
-#define CCS_BATCH_PREFETCH_AHEAD 0
-#endif
-__device__ __forceinline__ void prefetch_tile_records(const BatchArgs& a, int d, int phase, int64_t t) {
-#if CCS_BATCH_PREFETCH_AHEAD > 0
-    if (threadIdx.x != 0) return;
-    const int64_t* ts = a.tiles + ((int64_t)d * PH_COUNT + phase) * (a.count + 1);
-    const int64_t ahead = gridDim.x < (unsigned)CCS_BATCH_PREFETCH_AHEAD ? (int64_t)gridDim.x
-                                                                       : (int64_t)CCS_BATCH_PREFETCH_AHEAD;
-    const int64_t tp = t + ahead;
-    if (tp >= ts[a.count]) return;
-    const int c = find_cage(ts, a.count, tp);
-    const BatchCage& bc = a.cages[c];
-    const int64_t h0 = (tp - ts[c]) * kBatchBlock, H = bc.lv[d].H;
-    if (h0 >= H) return;
-    const int64_t n = (H - h0) < kBatchBlock ? (H - h0) : kBatchBlock;
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
-                 :: "l"(a.he + 4 * (bc.he + bc.lv[d].heOff + h0)), "r"((uint32_t)(n * 16)) : "memory");
-#endif
-}
-
-// for_tiles, each tile's body preceded by the prefetch of the records of the
-// tile CCS_BATCH_PREFETCH_AHEAD ahead
-template <class Body>
-__device__ __forceinline__ void for_tiles_prefetch(const BatchArgs& a, int d, int phase, Body body) {
-    const int64_t* ts = a.tiles + ((int64_t)d * PH_COUNT + phase) * (a.count + 1);
-    const int64_t total = ts[a.count];
-    for (int64_t t = blockIdx.x; t < total; t += gridDim.x) {
-        prefetch_tile_records(a, d, phase, t);
-        const int c = find_cage(ts, a.count, t);
-        body(a.cages[c], t - ts[c]);
-    }
-}
-
 __device__ __forceinline__ QuadView<4> batch_quad_view_stats(const BatchArgs& a, const BatchCage& bc, int d) {
     QuadView<4> L = batch_quad_view(a, bc, d);
     L.ostats = a.stats + bc.stats[d];
@@ -343,7 +306,7 @@ __device__ __forceinline__ void fwd_crease_stats(const BatchArgs& a, int d, int 
 // default pass, depth d >= 2, section 1
 template <bool TOPO, bool CREASED>
 __device__ __forceinline__ void fwd_level_ab(const BatchArgs& a, int d, int32_t* tile) {
-        for_tiles_prefetch(a, d, PH_A, [&](const BatchCage& bc, int64_t lt) {
+        for_tiles(a, d, PH_A, [&](const BatchCage& bc, int64_t lt) {
             LevelArgs la = batch_level_args(a, bc, d);
             la.ostats = a.stats + bc.stats[d];
             if (d + 2 <= bc.depth) {
@@ -451,7 +414,7 @@ __device__ __forceinline__ void adj_cage_section(const BatchArgs& a) {
 
 // adjoint, d >= 2: one pass (adj_quad_step_tile)
 __device__ __forceinline__ void adj_level_step(const BatchArgs& a, int d) {
-    for_tiles_prefetch(a, d, PH_ADJ_VERT, [&](const BatchCage& bc, int64_t lt) {
+    for_tiles(a, d, PH_ADJ_VERT, [&](const BatchCage& bc, int64_t lt) {
         float* gOld = a.work + 3 * (bc.pt + bc.lv[d].ptOff);
         adj_quad_step_tile<4>(batch_quad_view_stats(a, bc, d), adj_gnew(a, bc, d), gOld, lt * kBatchBlock);
     });
