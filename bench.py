@@ -589,8 +589,10 @@ def batch_measure(args, rank, world):
 
     def batch_step():
         bt.refine_points()
-        loss_grad(arr["points"], arr["grad_points"])   # the adjoint then consumes it
-        bt.adjoint()
+        # the adjoint of P - T with the finest levels' P - T formed inside its
+        # first step (ccs_BatchAdjointDistance_cuda); the loop forms P - T in
+        # one elementwise pass and feeds it to the plain adjoint
+        bt.adjoint_distance(T_all)
         arr["grad_cage_points"].mul_(scale)
 
     with torch.cuda.stream(stream):
@@ -620,7 +622,7 @@ def batch_measure(args, rank, world):
                 for i, ref in zip((0, len(ws) // 2, len(ws) - 1), loop_sample))
     # the parts alone (same stream, CUDA events)
     parts = {}
-    for name, fn in (("forward_ms", bt.refine_points), ("adjoint_ms", bt.adjoint),
+    for name, fn in (("forward_ms", bt.refine_points), ("adjoint_ms", lambda: bt.adjoint_distance(T_all)),
                      ("loss_grad_ms", lambda: loss_grad(arr["points"], arr["grad_points"]))):
         with torch.cuda.stream(stream):
             a.record(stream)
@@ -656,8 +658,11 @@ def batch_measure(args, rank, world):
             "forward_ms": parts["forward_ms"], "adjoint_ms": parts["adjoint_ms"],
             "loss_grad_ms": parts["loss_grad_ms"],
             "grad_agreement_rel": agree, "clocks": clocks,
-            "step": "forward points, gradient of the mean squared distance to a fixed target (P - T in "
-                    "one pass; the adjoint is linear, so the 2/N factor scales the cage gradient), adjoint"}
+            "step": "forward points, gradient of the mean squared distance to a fixed target, adjoint; "
+                    "the adjoint is linear, so both arms feed it P - T and scale the cage gradient by 2/N. "
+                    "Loop: P - T in one elementwise pass, then the per-cage adjoints. Batch: "
+                    "ccs_BatchAdjointDistance_cuda, the finest levels' P - T formed inside the first "
+                    "adjoint step (adjoint_ms includes its elementwise part; loss_grad_ms is the loop's pass)"}
 
 
 def run_batch_workload(args):

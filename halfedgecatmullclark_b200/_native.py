@@ -116,6 +116,7 @@ SIGNATURES = {
     "ccs_BatchRefine_cuda": ([_P, _I], _I),
     "ccs_BatchRefinePoints_cuda": ([_P, _I], _I),
     "ccs_BatchAdjointPoints_cuda": ([_P], _I),
+    "ccs_BatchAdjointDistance_cuda": ([_P, _P], _I),
     "ccs_BatchGetArrays_cuda": ([_P, ctypes.POINTER(BatchArrays)], _I),
     "ccs_BatchCageInfo_cuda": ([_P, ctypes.c_int32, ctypes.POINTER(BatchCageInfo)], _I),
     "ccs_BatchSetStream_cuda": ([_P, _P], _I),

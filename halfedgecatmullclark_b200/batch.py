@@ -68,6 +68,15 @@ class Batch:
     def adjoint(self):
         N.check(self.L.ccs_BatchAdjointPoints_cuda(self.ptr), "ccs_BatchAdjointPoints_cuda")
 
+    def adjoint_distance(self, target):
+        """grad_cage_points = S^T (P - target) (ccs_BatchAdjointDistance_cuda):
+        the adjoint of a fitting loss's gradient direction, with the finest
+        levels' P - target formed inside the first adjoint step.  `target`: a
+        float32 CUDA tensor in the points' layout, kept alive by the caller."""
+        assert target.is_cuda and target.dtype.is_floating_point and target.is_contiguous()
+        N.check(self.L.ccs_BatchAdjointDistance_cuda(self.ptr, target.data_ptr()),
+                "ccs_BatchAdjointDistance_cuda")
+
     def synchronize(self):
         N.check(self.L.ccs_BatchSynchronize_cuda(self.ptr), "ccs_BatchSynchronize_cuda")
 

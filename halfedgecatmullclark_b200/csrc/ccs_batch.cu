@@ -62,6 +62,8 @@ enum Phase {
     PH_ADJ_VERT,        // V_0 (cage) or H_d
     PH_ZERO3,           // d = 1: V_2 vertex slots of depth 3 (the one-pass step of depth 2)
     PH_CREASE_STATS_NEXT,  // C_(d+1) creases of depth d + 1 (their statistics, before depth d + 1)
+    PH_DIST,            // d = 0: the points whose fitting gradient P - T the distance adjoint
+                        // writes before its steps (every level but a depth >= 3 cage's finest)
     PH_COUNT
 };
 
@@ -74,6 +76,14 @@ struct BatchCage {
     int64_t stats[kMaxBatchDepth + 1];  // level d's ring statistics (V(d-1) entries), 1 <= d < depth
     Level lv[kMaxBatchDepth + 1];
 };
+
+// Points of a cage whose fitting gradient the distance adjoint writes to the
+// working buffer first: all of them, but for a cage of depth >= 3 not its
+// finest level, which the first adjoint step reads as P - T directly.
+__host__ __device__ inline int64_t dist_points(const BatchCage& bc) {
+    const Level& f = bc.lv[bc.depth];
+    return bc.depth >= 3 ? f.ptOff : f.ptOff + f.V;
+}
 
 struct GridSync {
     unsigned int count;
@@ -90,6 +100,7 @@ struct BatchArgs {
     const float* cagePts;
     float* pts;
     float* work;                         // adjoint: running gradient per refined point
+    const float* target = nullptr;       // distance adjoint: the points' target (null: plain adjoint)
     float* gradCage;                     // adjoint output
     float4* stats;                       // ring statistics of the older vertices, every level
     GridSync* sync;
@@ -416,7 +427,28 @@ __device__ __forceinline__ void adj_cage_section(const BatchArgs& a) {
 __device__ __forceinline__ void adj_level_step(const BatchArgs& a, int d) {
     for_tiles(a, d, PH_ADJ_VERT, [&](const BatchCage& bc, int64_t lt) {
         float* gOld = a.work + 3 * (bc.pt + bc.lv[d].ptOff);
-        adj_quad_step_tile<4>(batch_quad_view_stats(a, bc, d), adj_gnew(a, bc, d), gOld, lt * kBatchBlock);
+        if (a.target && d + 1 == bc.depth) {
+            // distance adjoint, the cage's finest level: its gradient P - T as it is read
+            const int64_t o = 3 * (bc.pt + bc.lv[d + 1].ptOff);
+            adj_quad_step_tile_g<4, GradDistance>(batch_quad_view_stats(a, bc, d),
+                                                  GradDistance{a.pts + o, a.target + o}, gOld, lt * kBatchBlock);
+        } else {
+            adj_quad_step_tile<4>(batch_quad_view_stats(a, bc, d), adj_gnew(a, bc, d), gOld, lt * kBatchBlock);
+        }
+    });
+}
+
+// distance adjoint, before its steps: work = P - T over the PH_DIST points
+__global__ void __launch_bounds__(kBatchBlock)
+k_batch_dist_init(BatchArgs a, int) {
+    const int tid = threadIdx.x;
+    for_tiles(a, 0, PH_DIST, [&](const BatchCage& bc, int64_t lt) {
+        const int64_t i = lt * kBatchBlock + tid;
+        if (i >= dist_points(bc)) return;
+        const int64_t o = 3 * (bc.pt + i);
+        a.work[o + 0] = fsub(a.pts[o + 0], a.target[o + 0]);
+        a.work[o + 1] = fsub(a.pts[o + 1], a.target[o + 1]);
+        a.work[o + 2] = fsub(a.pts[o + 2], a.target[o + 2]);
     });
 }
 
@@ -568,6 +600,7 @@ struct ccs_Batch {
     int numSMs = 148;
     bool graphOk = true;
     bool topoReady = false;                  // ccs_BatchRefine_cuda has run
+    const float* target = nullptr;           // the distance adjoint's target (its graph holds it)
     std::map<int, cudaGraphExec_t> graphs;
     std::mutex mu;
 };
@@ -597,6 +630,7 @@ static int64_t phase_units(const BatchCage& bc, int d, int ph) {
         case PH_ADJ_VERT: return d == 0 ? lv.V : lv.H;
         case PH_ZERO3: return d == 1 && bc.depth >= 3 ? bc.lv[2].V : 0;
         case PH_CREASE_STATS_NEXT: return d >= 1 && d + 1 < bc.depth ? bc.lv[d + 1].C : 0;
+        case PH_DIST: return d == 0 ? dist_points(bc) : 0;
         default: return 0;
     }
 }
@@ -786,7 +820,7 @@ static int64_t max_tiles(const ccs_Batch* b, int d, std::initializer_list<int> p
     return m;
 }
 
-enum BatchOp { BOP_REFINE = 0, BOP_POINTS = 1, BOP_ADJOINT = 2 };
+enum BatchOp { BOP_REFINE = 0, BOP_POINTS = 1, BOP_ADJOINT = 2, BOP_ADJOINT_DIST = 3 };
 
 // split schedule, forward: the sections of depth d as ordinary launches
 template <bool TOPO, bool CREASED, bool DET>
@@ -826,8 +860,15 @@ static cudaError_t enqueue_batch(ccs_Batch* b, int op, bool creased) {
     BatchArgs a = batch_args(b);
     cudaError_t e = cudaMemsetAsync(b->sync, 0, sizeof(GridSync), b->stream);
     if (e != cudaSuccess) return e;
-    if (op == BOP_ADJOINT) {
+    if (op == BOP_ADJOINT || op == BOP_ADJOINT_DIST) {
         e = cudaMemsetAsync(b->gradCage, 0, sizeof(float) * 3 * (size_t)b->totCagePts, b->stream);
+        if (op == BOP_ADJOINT_DIST) {
+            // P - T into the working buffer, but for the finest levels the
+            // first adjoint step reads as P - T itself
+            a.target = b->target;
+            if (e == cudaSuccess)
+                e = launch_persistent(b, k_batch_dist_init, max_tiles(b, 0, {PH_DIST}), a, 0, false);
+        }
         for (int d = b->maxDepth - 1; d >= 0 && e == cudaSuccess; --d) {
             if (!b->split) {
                 const int64_t mt = max_tiles(b, d, {PH_ADJ_EDGE, PH_ADJ_FACE, PH_ADJ_VERT});
@@ -967,6 +1008,24 @@ int ccs_BatchAdjointPoints_cuda(ccs_Batch* batch) {
     BatchDevice g(batch->device);
     if (!adjoint_buffers(batch)) return set_last_error(CCS_ERR_ALLOC);
     return set_last_error(run_batch(batch, BOP_ADJOINT, true));
+}
+
+int ccs_BatchAdjointDistance_cuda(ccs_Batch* batch, const float* target) {
+    if (!batch || !target) return set_last_error(CCS_ERR_ARG);
+    std::lock_guard<std::mutex> lock(batch->mu);
+    if (!batch->topoReady) return set_last_error(CCS_ERR_STATE);
+    BatchDevice g(batch->device);
+    if (!adjoint_buffers(batch)) return set_last_error(CCS_ERR_ALLOC);
+    if (batch->target != target) {
+        // this operation's graph holds the target's address: capture anew
+        auto it = batch->graphs.find(BOP_ADJOINT_DIST * 2 + 1);
+        if (it != batch->graphs.end()) {
+            cudaGraphExecDestroy(it->second);
+            batch->graphs.erase(it);
+        }
+        batch->target = target;
+    }
+    return set_last_error(run_batch(batch, BOP_ADJOINT_DIST, true));
 }
 
 int ccs_BatchGetArrays_cuda(ccs_Batch* batch, ccs_BatchArrays* out) {

@@ -1595,29 +1595,44 @@ __device__ __forceinline__ void adj_quad_point_tile(const QuadView<RW>& L, const
 // children 1 and 3 at edge midpoints whose creased edges are the halves of
 // one parent edge, child 0 at an older vertex (its statistics).
 // Both halves of an edge evaluate the same terms; gE is read, not written.
-template <int RW>
-__device__ __forceinline__ void adj_quad_step_tile(const QuadView<RW>& L, const float* __restrict__ gNew,
-                                                   float* __restrict__ gOld, int64_t h0) {
+// Where the adjoint step reads the gradients of depth d+1's points (index =
+// the point's slot in the level: [vertices | faces | edges]): an array, or,
+// for the finest level of a fitting loss, the difference P - T of the
+// level's points and its target, formed as it is read.
+struct GradArray {
+    const float* __restrict__ g;
+    __device__ __forceinline__ f3 at(int64_t i) const { return ld3(g + 3 * i); }
+};
+struct GradDistance {
+    const float* __restrict__ p;
+    const float* __restrict__ t;
+    __device__ __forceinline__ f3 at(int64_t i) const {
+        const f3 a = ld3(p + 3 * i), b = ld3(t + 3 * i);
+        return f3{fsub(a.x, b.x), fsub(a.y, b.y), fsub(a.z, b.z)};
+    }
+};
+
+template <int RW, class GradIn>
+__device__ __forceinline__ void adj_quad_step_tile_g(const QuadView<RW>& L, const GradIn gin,
+                                                     float* __restrict__ gOld, int64_t h0) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31, k = lane & 3, qb = lane & ~3, j = (lane >> 2) & 3;
     const int ln = qb | ((k + 1) & 3), lp = qb | ((k + 3) & 3);
     const int64_t h64 = h0 + threadIdx.x;
     const bool valid = h64 < L.H;
     const int32_t h = (int32_t)h64;
-    const float* gV = gNew;
-    const float* gF = gNew + 3 * (int64_t)L.V;
-    const float* gE = gNew + 3 * ((int64_t)L.V + L.F);
+    const int64_t fBase = L.V, eBase = (int64_t)L.V + L.F;
     int32_t tw = -1, ed = 0, vx = 0;
     float4 st = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     f3 gv = zero3(), ge = zero3(), gf = zero3();
     float sOwn = 0.0f, sOther = 0.0f;
     if (valid) {
         lane_record(L, h64, tw, ed, vx);
-        gv = ld3(gV + 3 * (int64_t)vx);
-        ge = ld3(gE + 3 * (int64_t)ed);
+        gv = gin.at(vx);
+        ge = gin.at(eBase + ed);
         sOwn = L.sharp(ed);
         if (k == 0) {
-            gf = ld3(gF + 3 * (int64_t)(h >> 2));
+            gf = gin.at(fBase + (h >> 2));
             st = L.ostats[vx];
         }
     }
@@ -1711,6 +1726,13 @@ __device__ __forceinline__ void adj_quad_step_tile(const QuadView<RW>& L, const 
     } else if (k == 0) {
         atomic_add3(o, s);
     }
+}
+
+// the gradients of depth d+1 from an array gNew (the same slots)
+template <int RW>
+__device__ __forceinline__ void adj_quad_step_tile(const QuadView<RW>& L, const float* __restrict__ gNew,
+                                                   float* __restrict__ gOld, int64_t h0) {
+    adj_quad_step_tile_g<RW, GradArray>(L, GradArray{gNew}, gOld, h0);
 }
 
 }  // namespace ccs

@@ -333,6 +333,14 @@ int ccs_BatchRefine_cuda(ccs_Batch *batch, int mode);
 int ccs_BatchRefinePoints_cuda(ccs_Batch *batch, int mode);
 /* Adjoint of the scatter rule: gradPoints (consumed) -> gradCagePoints. */
 int ccs_BatchAdjointPoints_cuda(ccs_Batch *batch);
+/* The adjoint of a fitting loss's gradient direction, fused: gradCagePoints =
+ * S^T (P - T), P = the refined points the last ccs_BatchRefinePoints_cuda
+ * left, T = `target` (device, the points' layout).  The gradient of
+ * mean ||P - T||^2 over the N points is 2/N times this.  The finest level of
+ * every cage of depth >= 3 is read as P - T inside the first adjoint step;
+ * the other levels are set to P - T in the gradPoints buffer first.  No
+ * counterpart in the reference (which has no adjoint). */
+int ccs_BatchAdjointDistance_cuda(ccs_Batch *batch, const float *target);
 int ccs_BatchGetArrays_cuda(ccs_Batch *batch, ccs_BatchArrays *out);
 int ccs_BatchCageInfo_cuda(const ccs_Batch *batch, int32_t cage, ccs_BatchCageInfo *out);
 int ccs_BatchSetStream_cuda(ccs_Batch *batch, void *stream);

@@ -188,3 +188,32 @@ def test_batch_config5_distribution_matches_reference():
             finally:
                 refimpl.set_threads(cores)
                 r.close()
+
+
+@pytest.mark.parametrize("split", [True, False])
+def test_batch_distance_adjoint_matches_plain(workloads, split):
+    """ccs_BatchAdjointDistance_cuda (the finest level of every cage of depth
+    >= 3 read as P - T inside its first adjoint step, the other levels set to
+    P - T first) equals the plain batched adjoint fed P - T, within the float
+    atomics' reordering: cages of depths 1-4, both launch schedules, two calls
+    with different targets (the second re-captures the operation's graph)."""
+    import torch
+    from halfedgecatmullclark_b200.batch import Batch
+    with Batch([w.cage for w in workloads], [w.depth for w in workloads]) as b:
+        b.set_stream(torch.cuda.current_stream())
+        b.refine()
+        b.set_schedule(0 if split else 4, split)
+        arr = b.arrays()
+        gen = torch.Generator(device="cuda").manual_seed(7)
+        for _ in range(2):
+            T = torch.randn(arr["points"].shape, device="cuda", generator=gen)
+            b.refine_points()
+            b.adjoint_distance(T)
+            b.synchronize()
+            got = arr["grad_cage_points"].clone()
+            arr["grad_points"].copy_(arr["points"] - T)
+            b.adjoint()
+            b.synchronize()
+            ref = arr["grad_cage_points"].clone()
+            assert torch.isfinite(got).all()
+            assert rel_err(got.cpu().numpy(), ref.cpu().numpy()) <= 1e-5
