@@ -57,6 +57,30 @@ static inline unsigned nblocksL(int64_t n) { return (unsigned)((n + kBlockL - 1)
 // prefetched the next tile's records and left each bulk store in flight ran
 // 1.5x slower at depth 5: 5 resident blocks per SM instead of 8 hid less of
 // the gather latency than the extra overlap won.)
+// Thread 0 of a block asks L2 for the records of tile `tile + ahead` (a bulk
+// prefetch: no shared memory, no wait; nothing when that tile is past the
+// level's end).
+template <int RW>
+__device__ __forceinline__ void prefetch_records_ahead(const int32_t* in, int64_t H, int64_t tile, int ahead) {
+    if (ahead <= 0 || threadIdx.x != 0) return;
+    const int64_t p0 = (tile + ahead) * kBlockL;
+    if (p0 >= H) return;
+    const int64_t n = (H - p0) < kBlockL ? (H - p0) : kBlockL;
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
+                 :: "l"(in + (int64_t)RW * p0), "r"((uint32_t)(n * 4 * RW)) : "memory");
+}
+
+// blocks ahead whose records kernel A and the vertex passes prefetch (0:
+// none): one wave at 8 resident blocks.  The exact pass at depth 5 of the
+// headline workload: kernel A 0.377 -> 0.348 ms, its face-centre and
+// edge-midpoint pass 0.508 -> 0.500 ms, the refine 1.225 -> 1.177 ms
+#ifndef CCS_A_PREFETCH_AHEAD
+#define CCS_A_PREFETCH_AHEAD 1184
+#endif
+#ifndef CCS_B_PREFETCH_AHEAD
+#define CCS_B_PREFETCH_AHEAD 1184
+#endif
+
 #ifndef CCS_A_MIN_BLOCKS
 #define CCS_A_MIN_BLOCKS 8
 #endif
@@ -73,6 +97,7 @@ k_level_a(LevelArgs a) {
         }
         return;
     }
+    prefetch_records_ahead<RW>(a.in, a.H, blockIdx.x, CCS_A_PREFETCH_AHEAD);
     __shared__ __align__(128) int32_t tile[kBlockL * 4 * RW];
     tile_level_a<kBlockL, RW, TOPO, UV, true, CREASED>(a, (int64_t)blockIdx.x * kBlockL, tile);
     // the slots the step after next accumulates into (zeroNextN = 0: none)
@@ -115,18 +140,9 @@ k_level_ab(LevelArgs a, const __grid_constant__ CUtensorMap childMap) {
         }
         return;
     }
-#if CCS_AB_PREFETCH_AHEAD > 0
     // the records of the tile about one wave ahead, fetched into L2 while
-    // this one runs (a bulk prefetch: no shared memory, no wait)
-    if (threadIdx.x == 0) {
-        const int64_t p0 = ((int64_t)blockIdx.x + CCS_AB_PREFETCH_AHEAD) * kBlockL;
-        if (p0 < a.H) {
-            const int64_t n = (a.H - p0) < kBlockL ? (a.H - p0) : kBlockL;
-            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
-                         :: "l"(a.in + (int64_t)RW * p0), "r"((uint32_t)(n * 4 * RW)) : "memory");
-        }
-    }
-#endif
+    // this one runs
+    prefetch_records_ahead<RW>(a.in, a.H, blockIdx.x, CCS_AB_PREFETCH_AHEAD);
     __shared__ __align__(1024) int32_t tile[TOPO ? kBlockL * 4 * RW : 4];
     // one tile per block: the child records' store is issued first and left
     // to drain while the points are computed
@@ -138,6 +154,7 @@ k_level_ab(LevelArgs a, const __grid_constant__ CUtensorMap childMap) {
 template <int RW, bool CREASED, bool STRUCT>
 __global__ void __launch_bounds__(kBlockL, 8)
 k_level_b(QuadView<RW> L, const float* __restrict__ pin, float* __restrict__ pout) {
+    prefetch_records_ahead<RW>(L.he, L.H, blockIdx.x, CCS_B_PREFETCH_AHEAD);
     tile_level_b<RW, CREASED, STRUCT>(L, pin, pout, (int64_t)blockIdx.x * kBlockL);
 }
 
@@ -145,6 +162,7 @@ k_level_b(QuadView<RW> L, const float* __restrict__ pin, float* __restrict__ pou
 template <int RW, bool CREASED>
 __global__ void __launch_bounds__(kBlockL, 5)
 k_level_b_exact(QuadView<RW> L, const float* __restrict__ pin, float* __restrict__ pout) {
+    prefetch_records_ahead<RW>(L.he, L.H, blockIdx.x, CCS_B_PREFETCH_AHEAD);
     tile_level_b_exact<RW, CREASED>(L, pin, pout, (int64_t)blockIdx.x * kBlockL);
 }
 
