@@ -13,8 +13,10 @@
 // file computes dL/d(points of depth d) += S_d^T g.
 //
 // Quad levels d >= 2 (cages with the twin relation, ring statistics kept):
-// one halfedge-parallel pass, adj_quad_step_tile, which completes each
-// edge's gradient in both of its halves and then adds the vertex terms.
+// one pass with one thread per depth-d face, adj_face_step_tile, which
+// completes each edge's gradient once and then adds the vertex terms (the
+// batched path runs the halfedge-parallel form of the same pass,
+// adj_quad_step_tile).
 // Depth 1: two halfedge-parallel passes with the forward's lane layout
 // (ccs_tiles.cuh adj_quad_*):
 //   1. gE[e] += the cE / dE terms, completed by the pair's larger halfedge
@@ -107,6 +109,33 @@ k_adj_quad_step(QuadView<RW> L, const float* __restrict__ gNew, float* __restric
     adj_quad_step_tile<RW>(L, gNew, gOld, (int64_t)blockIdx.x * kBlockA);
 }
 
+// quad levels d >= 2, one thread per face (adj_face_step_tile)
+static constexpr int kBlockAF = 128;
+#ifndef CCS_ADJ_FQ
+#define CCS_ADJ_FQ 1
+#endif
+#ifndef CCS_ADJ_FQ_MIN_BLOCKS
+#define CCS_ADJ_FQ_MIN_BLOCKS 6
+#endif
+#ifndef CCS_ADJ_FQ_PREFETCH_AHEAD
+#define CCS_ADJ_FQ_PREFETCH_AHEAD 888
+#endif
+template <int RW>
+__global__ void __launch_bounds__(kBlockAF, CCS_ADJ_FQ_MIN_BLOCKS)
+k_adj_face_step(QuadView<RW> L, const float* __restrict__ gNew, float* __restrict__ gOld) {
+    chain_wait_then_release();
+    const int64_t nF = (int64_t)L.H >> 2;
+    if (CCS_ADJ_FQ_PREFETCH_AHEAD > 0 && threadIdx.x == 0) {
+        const int64_t p0 = ((int64_t)blockIdx.x + CCS_ADJ_FQ_PREFETCH_AHEAD) * kBlockAF;
+        if (p0 < nF) {
+            const int64_t n = (nF - p0) < kBlockAF ? (nF - p0) : kBlockAF;
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
+                         :: "l"(L.he + (int64_t)RW * 4 * p0), "r"((uint32_t)(n * 16 * RW)) : "memory");
+        }
+    }
+    adj_face_step_tile<RW, GradArray>(L, GradArray{gNew}, gOld, (int64_t)blockIdx.x * kBlockAF + threadIdx.x);
+}
+
 template <int RW, bool STRUCT>
 __global__ void __launch_bounds__(kBlockA, 8)
 k_adj_quad_points(QuadView<RW> L, const float* __restrict__ gNew, float* __restrict__ gOld) {
@@ -120,7 +149,11 @@ static void adjoint_quad_level(const Ctx& c, const QuadView<RW>& L, float* gNew,
 #ifndef CCS_NO_ADJ_STEP
     if (L.d >= 2 && L.ostats) {
         c.prof->begin(c.stream, CCS_K_ADJ_STEP, L.d, L.H);
-        launch_chained(k_adj_quad_step<RW>, nblocksA(L.H), kBlockA, c.stream, L, gNew, gOld);
+        if (CCS_ADJ_FQ)
+            launch_chained(k_adj_face_step<RW>, (unsigned)((((int64_t)L.H >> 2) + kBlockAF - 1) / kBlockAF),
+                           kBlockAF, c.stream, L, gNew, gOld);
+        else
+            launch_chained(k_adj_quad_step<RW>, nblocksA(L.H), kBlockA, c.stream, L, gNew, gOld);
         c.prof->end(c.stream);
         return;
     }

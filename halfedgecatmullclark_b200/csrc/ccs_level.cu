@@ -1,26 +1,27 @@
 // ccs_level.cu -- refinement steps for quad levels (depth d >= 1).
 //
-// Default pass, depth d >= 2: one launch per step, k_level_ab
-// (tile_level_ab in ccs_tiles.cuh; one thread per parent halfedge, the 4
-// lanes of a face adjacent, a parent quad's 16 children in a 16-lane group):
-//   - every load that needs only the record (one 16-byte load) is issued
-//     first: the vertex point, crease sharpness, the older vertex's ring
-//     statistics, across a parent edge the twin quad's two other vertices;
-//   - face point of its face (quad shuffles, halfedge order), stored by the
-//     face's first lane;
-//   - edge point of its edge by both halves (the twin face from a sibling
-//     quad's lanes inside the parent quad, else rebuilt), stored by the
-//     pair's larger halfedge -- the owner's value bit for bit;
-//   - its vertex share: ring statistics from the structure (face centre,
-//     edge midpoint) or the per-level table of older vertices; a face
-//     centre's four shares summed in the warp and stored, the others by float
+// Default pass, depth d >= 2: one launch per step, k_level_fq (one thread
+// per depth-d face, the four faces of a parent quad in a quad of lanes):
+//   - the face's four records (one 64-byte read), then every load they
+//     allow: the four vertex points, crease sharpness, the corner's ring
+//     statistics, across the two parent edges the twin quads' other
+//     vertices;
+//   - the face's 16 child records (+ UV codes) through a 32 KB swizzled
+//     shared tile and two TMA tensor stores per block, issued first and left
+//     to drain while the points are computed (no multicast);
+//   - its face point, the inner edge it shares with the next lane (that
+//     lane's face point by shuffle), its two outer edge points (the twin
+//     face rebuilt), all in the reference's operation order and stored once;
+//   - its four vertex shares: a face centre's four summed by the quad's lane
+//     0 and stored, an edge midpoint's pair and the corner's share by float
 //     atomics into slots the previous step cleared; it clears the slots of
 //     the next step;
-//   - the 4 child records (+ UV codes) through a 16 KB shared tile and one
-//     TMA store per block (a tensor store from a 128-byte swizzled tile when
-//     the level's tensor map exists, else a bulk store; no multicast);
 //   - extra blocks refine the creases and add the next level's crease
 //     statistics.
+// The points-only call runs the same kernel without the records.  k_level_ab
+// (tile_level_ab: one thread per parent halfedge, a parent quad's 16
+// children in a 16-lane group) is the same step for 12-byte records and for
+// levels without a tensor map.
 // Depth 1 (children of n-gons, no 16-lane structure), cages without kept
 // statistics, and the deterministic pass run the step as kernel A
 // (k_level_a: records, face and edge points, clearing) then a vertex pass:
@@ -148,6 +149,244 @@ k_level_ab(LevelArgs a, const __grid_constant__ CUtensorMap childMap) {
     // to drain while the points are computed
     tile_level_ab<kBlockL, RW, TOPO, UV, CREASED, TMAP, CCS_AB_EARLY_STORE>(
         a, (int64_t)blockIdx.x * kBlockL, tile, (int64_t)nbH * kBlockL, &childMap);
+}
+
+// ---------------------------------------------------------------------------
+// quad level d >= 2, one thread per depth-d face: the whole step d -> d+1
+// (TOPO) or its points only
+// ---------------------------------------------------------------------------
+// At depth d >= 2 the halfedges 16 G + 4 j + k are child k of the children
+// j = 0..3 of the depth-(d-1) face G (CatmullClark.h:2760-2795), on 9
+// points: the corner C_j = vertex(16 G + 4 j) (an older vertex: its ring
+// statistics are in `ostats`), the midpoint M_j = vertex(16 G + 4 j + 1) =
+// vertex(16 G + 4 (j+1) + 3) of parent edge j and the centre Z = vertex(16 G
+// + 4 j + 2); face j runs C_j, M_j, Z, M_{j-1}.  The refinement also fixes
+// the inner twins (twin(4 j + 1) = 4 (j+1) + 2: one edge, inner edge j), the
+// two halves of parent edge j (edges e(4 j) and e(4 (j+1) + 3) = e(4 j) ^ 1)
+// and the twin side of parent edge j: child 3 of one face and child 0 of the
+// next face of one parent quad, whose centre the two rebuilt twin faces
+// share (CatmullClark.h:2778-2781).
+// Lane j of a quad of lanes takes face j: its face point, inner edge j with
+// the next lane's face point, its two outer edges (the twin face rebuilt from
+// the twin quad's other two vertices, as tile_level_ab does) and its four
+// vertex shares.  The values of other lanes it needs -- the next lane's face
+// point and midpoint share, the previous lane's inner edge point and twin
+// centre, the centre's four shares -- come by shuffles.  Every value is
+// evaluated with the same operations in the same order as tile_level_ab.
+// Stores: the face point, inner edge j, the outer edge points it owns and,
+// by lane 0, the centre (shares summed in face order); float atomics: the
+// corner's share and midpoint M_j's pair (j, 1) + (j+1, 3).  Against the
+// lane-per-halfedge tile this evaluates every face and inner edge point once,
+// needs 24 shuffles per face instead of about 36 per halfedge and takes no
+// per-lane branches on the child position.
+// TOPO (16-byte records): the face's 16 child records (tile_level_ab's rules)
+// go through a 128-byte swizzled shared tile to two TMA tensor stores (128
+// rows of 128 bytes each) issued before the points are evaluated; the extra
+// blocks refine the creases.  The vertex slots [0, V) of depth d+1 must be
+// zero on entry; every thread clears its share of `zeroNext`.
+static constexpr int kBlockF = 128;                      // faces per block
+
+// the full step (TOPO) by k_level_fq instead of k_level_ab
+#ifndef CCS_STEP_FQ
+#define CCS_STEP_FQ 1
+#endif
+
+#ifndef CCS_FQ_MIN_BLOCKS
+#define CCS_FQ_MIN_BLOCKS 7
+#endif
+#ifndef CCS_FQ_PREFETCH_AHEAD
+#define CCS_FQ_PREFETCH_AHEAD 1036
+#endif
+
+template <int RW, bool TOPO, bool UV, bool CREASED>
+__global__ void __launch_bounds__(kBlockF, CCS_FQ_MIN_BLOCKS)
+k_level_fq(LevelArgs a, const __grid_constant__ CUtensorMap childMap) {
+    static_assert(!TOPO || RW == 4, "the child records go out through the 16-byte record tensor map");
+    chain_wait_then_release();
+    const unsigned full = 0xffffffffu;
+    const int64_t nF = (int64_t)a.H >> 2;                  // depth-d faces (H = 16 n at d >= 2)
+    const int nbF = (int)((nF + kBlockF - 1) / kBlockF);
+    if (TOPO && (int)blockIdx.x >= nbF) {
+        const int64_t i = (int64_t)(blockIdx.x - nbF) * kBlockF + threadIdx.x;
+        if (i < a.C) {
+            const float2 sh = crease_item(a.crIn, a.crOut, (int32_t)i);
+            if (a.statsNext) crease_stats_next<RW>(a, (int32_t)i, sh);
+        }
+        return;
+    }
+    const int64_t f = (int64_t)blockIdx.x * kBlockF + threadIdx.x;
+    if (threadIdx.x == 0 && CCS_FQ_PREFETCH_AHEAD > 0) {
+        const int64_t p0 = ((int64_t)blockIdx.x + CCS_FQ_PREFETCH_AHEAD) * kBlockF;
+        if (p0 < nF) {
+            const int64_t n = (nF - p0) < kBlockF ? (nF - p0) : kBlockF;
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
+                         :: "l"(a.in + (int64_t)RW * 4 * p0), "r"((uint32_t)(n * 16 * RW)) : "memory");
+        }
+    }
+    const bool valid = f < nF;                             // the four lanes of a quad agree
+    const int lane = threadIdx.x & 31, qb = lane & ~3, j = lane & 3;
+    const int ln = qb | ((j + 1) & 3), lp = qb | ((j + 3) & 3);
+    const int32_t h0 = (int32_t)(4 * f);
+    int4 r[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) r[k] = make_int4(-1, 0, 0, 0);
+    if (valid) load_face_records<RW>(a.in, f, r);
+
+    if constexpr (TOPO) {
+        // child m of halfedge h0 + k is child record 16 f + 4 k + m: row 2 f + k / 2
+        // of the level's 128-byte rows, chunk 4 (k & 1) + m
+        __shared__ __align__(1024) int4 tile[kBlockF * 16];
+        float u[4], v[4];
+        if (UV) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                u[k] = uv_dec_fast((uint32_t)r[k].w);
+                v[k] = uv_dec_fast((uint32_t)r[k].w >> 16);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int kn = (k + 1) & 3, ko = (k + 2) & 3, kp = (k + 3) & 3;
+            const int32_t h = h0 + k, next = h0 + kn, prev = h0 + kp;
+            const int32_t tw = r[k].x, ed = r[k].y, ptw = r[kp].x, ped = r[kp].y;
+            int4 c[4];
+            c[0] = make_int4(child(qnext(tw), 3), 2 * ed + (h > tw ? 0 : 1), r[k].z, r[k].w);
+            c[1] = make_int4(child(next, 2), 2 * a.E + h, a.V + a.F + ed, 0);
+            c[2] = make_int4(child(prev, 1), 2 * a.E + prev, a.V + (int32_t)f, 0);
+            c[3] = make_int4(child(ptw, 0), 2 * ped + (prev > ptw ? 1 : 0), a.V + a.F + ped, 0);
+            if (UV) {
+                c[1].w = (int32_t)uv_enc_fast(flerp(u[k], u[kn], 0.5f), flerp(v[k], v[kn], 0.5f));
+                c[2].w = (int32_t)uv_enc_fast(fquarter(fadd(fadd(fadd(u[k], u[kn]), u[ko]), u[kp])),
+                                              fquarter(fadd(fadd(fadd(v[k], v[kn]), v[ko]), v[kp])));
+                c[3].w = (int32_t)uv_enc_fast(flerp(u[k], u[kp], 0.5f), flerp(v[k], v[kp], 0.5f));
+            }
+            const int row = 2 * threadIdx.x + (k >> 1), box = row >> 7, rr = row & 127;
+#pragma unroll
+            for (int m = 0; m < 4; ++m) tile[box * 1024 + rr * 8 + ((4 * (k & 1) + m) ^ (rr & 7))] = c[m];
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const int32_t row0 = (int32_t)(2 * (int64_t)blockIdx.x * kBlockF), rows = (int32_t)(a.H >> 1);
+            tensor_store_tile_async(&childMap, tile, row0);
+            if (row0 + 128 < rows) tensor_store_tile_async(&childMap, tile + 1024, row0 + 128);
+        }
+    }
+
+    const int32_t tw0 = r[0].x, e0 = r[0].y, C = r[0].z;  // (j, 0): C_j -> M_j
+    const int32_t e1 = r[1].y, Mj = r[1].z;               // (j, 1): M_j -> Z, inner edge j
+    const int32_t Z = r[2].z;                             // (j, 2): Z -> M_{j-1}
+    const int32_t tw3 = r[3].x, e3 = r[3].y, Mp = r[3].z; // (j, 3): M_{j-1} -> C_j
+    // across parent edge j: the far vertex of (j, 0)'s twin quad and that
+    // quad's centre; across parent edge j-1: the far vertex of (j, 3)'s
+    int32_t vX0 = 0, vF0 = 0, vX3 = 0;
+    if (valid && tw0 >= 0) {
+        vX0 = __ldg(a.in + (int64_t)RW * ((tw0 & ~3) + 1) + 2);
+        vF0 = __ldg(a.in + (int64_t)RW * ((tw0 & ~3) + 2) + 2);
+    }
+    if (valid && tw3 >= 0) vX3 = __ldg(a.in + (int64_t)RW * ((tw3 & ~3) + 3) + 2);
+    f3 pC = zero3(), pM = zero3(), pZ = zero3(), pMp = zero3(), qX0 = zero3(), qF0 = zero3(), qX3 = zero3();
+    float4 st = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    float s0 = 0.0f, s1 = 0.0f, s3 = 0.0f;
+    if (valid) {
+        pC = ld3(a.pin + 3 * (int64_t)C);
+        pM = ld3(a.pin + 3 * (int64_t)Mj);
+        pZ = ld3(a.pin + 3 * (int64_t)Z);
+        pMp = ld3(a.pin + 3 * (int64_t)Mp);
+        st = a.ostats[C];
+        if (CREASED) {
+            s0 = e0 < a.C ? __ldg(&a.crIn[e0].sharpness) : 0.0f;
+            s1 = e1 < a.C ? __ldg(&a.crIn[e1].sharpness) : 0.0f;
+            s3 = e3 < a.C ? __ldg(&a.crIn[e3].sharpness) : 0.0f;
+        }
+        if (tw0 >= 0) {
+            qX0 = ld3(a.pin + 3 * (int64_t)vX0);
+            qF0 = ld3(a.pin + 3 * (int64_t)vF0);
+        }
+        if (tw3 >= 0) qX3 = ld3(a.pin + 3 * (int64_t)vX3);
+    }
+    // the other half of parent edge j is (j+1, 3), of parent edge j-1 is
+    // (j-1, 0); the edge of (j, 2) is inner edge j-1
+    const float s3n = __shfl_sync(full, s3, ln), s0p = __shfl_sync(full, s0, lp), s1p = __shfl_sync(full, s1, lp);
+
+    // face point
+    const f3 F = add3(add3(add3(add3(zero3(), quarter3(pC)), quarter3(pM)), quarter3(pZ)), quarter3(pMp));
+    if (valid) st3(a.pout + 3 * ((int64_t)a.V + f), F);
+    const int64_t eOut = (int64_t)a.V + a.F;
+    // inner edge j: (j, 1) and its twin (j+1, 2), with the next lane's face point
+    const f3 Fn = shfl3(F, ln);
+    f3 I;
+    {
+        const float w = CREASED ? fsat(s1) : 0.0f;
+        I = add3(add3(zero3(), edge_share_fast<CREASED>(pM, pZ, F, false, w)),
+                 edge_share_fast<CREASED>(pZ, pM, Fn, false, w));
+        if (valid) st3(a.pout + 3 * (eOut + e1), I);
+    }
+    const f3 Ip = shfl3(I, lp);                            // inner edge j-1
+    // (j, 0): C_j -> M_j, half of parent edge j
+    f3 Eo0;
+    {
+        const float w = CREASED ? fsat(s0) : 0.0f;
+        const f3 sh = edge_share_fast<CREASED>(pC, pM, F, tw0 < 0, w);
+        if (tw0 >= 0) {
+            const f3 Ft = add3(add3(add3(add3(zero3(), quarter3(pC)), quarter3(qX0)), quarter3(qF0)), quarter3(pM));
+            Eo0 = add3(add3(zero3(), sh), edge_share_fast<CREASED>(pM, pC, Ft, false, w));
+        } else {
+            Eo0 = add3(zero3(), sh);
+        }
+        if (valid && h0 > tw0) st3(a.pout + 3 * (eOut + e0), Eo0);
+    }
+    // (j, 3): M_{j-1} -> C_j, half of parent edge j-1, whose twin quad's
+    // centre the previous lane read
+    const f3 qFp = shfl3(qF0, lp);
+    f3 Eo3;
+    {
+        const float w = CREASED ? fsat(s3) : 0.0f;
+        const f3 sh = edge_share_fast<CREASED>(pMp, pC, F, tw3 < 0, w);
+        if (tw3 >= 0) {
+            const f3 Ft = add3(add3(add3(add3(zero3(), quarter3(pC)), quarter3(pMp)), quarter3(qFp)), quarter3(qX3));
+            Eo3 = add3(add3(zero3(), sh), edge_share_fast<CREASED>(pC, pMp, Ft, false, w));
+        } else {
+            Eo3 = add3(zero3(), sh);
+        }
+        if (valid && h0 + 3 > tw3) st3(a.pout + 3 * (eOut + e3), Eo3);
+    }
+    // vertex shares (tile_level_b's rules)
+    {   // (j, 0): the corner; on a boundary the walk from it skips its own edge
+        const bool bnd = st.w != 0.0f;
+        const float avgS = CREASED ? (bnd ? fsub(st.y, s0) : st.y) : 0.0f;
+        const float cpre = CREASED ? (bnd ? fsub(st.z, fsign(s0)) : st.z) : 0.0f;
+        const f3 s = quad_vertex_rule<CREASED>(pC, F, Eo0, Eo3, st.x, cpre, avgS, bnd,
+                                               CREASED ? fsign(s0) : 0.0f, CREASED ? fsign(s3) : 0.0f);
+        if (valid) atomic_add3(a.pout + 3 * (int64_t)C, s);
+    }
+    f3 sM3;
+    {   // (j, 3): midpoint M_{j-1}; the walk from it skips its own edge
+        const bool bnd = tw3 < 0;
+        const float avgS = CREASED ? (bnd ? s0p : fadd(s3, s0p)) : 0.0f;
+        const float cpre = CREASED ? (bnd ? fsign(s0p) : fadd(fsign(s3), fsign(s0p))) : 0.0f;
+        sM3 = quad_vertex_rule<CREASED>(pMp, F, Eo3, Ip, bnd ? 2.0f : 4.0f, cpre, avgS, bnd,
+                                        CREASED ? fsign(s3) : 0.0f, CREASED ? fsign(s1p) : 0.0f);
+    }
+    {   // (j, 1): midpoint M_j, added with the next lane's (j+1, 3) share
+        const bool bnd = tw0 < 0;
+        const float avgS = CREASED ? fadd(s0, s3n) : 0.0f;
+        const float cpre = CREASED ? fadd(fsign(s0), fsign(s3n)) : 0.0f;
+        const f3 s = quad_vertex_rule<CREASED>(pM, F, I, Eo0, bnd ? 2.0f : 4.0f, cpre, avgS, bnd,
+                                               CREASED ? fsign(s1) : 0.0f, CREASED ? fsign(s0) : 0.0f);
+        const f3 sn = shfl3(sM3, ln);
+        if (valid) atomic_add3(a.pout + 3 * (int64_t)Mj, add3(s, sn));
+    }
+    {   // (j, 2): the centre, summed by lane 0 of the quad in face order
+        const f3 s = quad_vertex_rule<CREASED>(pZ, F, Ip, I, 4.0f, 0.0f, 0.0f, false,
+                                               CREASED ? fsign(s1p) : 0.0f, CREASED ? fsign(s1) : 0.0f);
+        const f3 a1 = shfl3(s, qb + 1), a2 = shfl3(s, qb + 2), a3 = shfl3(s, qb + 3);
+        if (valid && j == 0) st3(a.pout + 3 * (int64_t)Z, add3(add3(add3(add3(zero3(), s), a1), a2), a3));
+    }
+    // the slots the step after next accumulates into
+    const int64_t nT = (int64_t)nbF * kBlockF;
+    for (int64_t i = f; i < a.zeroNextN; i += nT) a.zeroNext[i] = 0.0f;
+    if (TOPO && threadIdx.x == 0) bulk_wait_read();
 }
 
 // default vertex pass: one tile of halfedges per block
@@ -378,14 +617,19 @@ static void level_ab(const Ctx& c, int d, bool topo, bool uv, float* pts) {
     CUtensorMap none;
     memset(&none, 0, sizeof none);
     const CUtensorMap& map = tmap ? c.childMaps[d] : none;
-    if (topo && tmap) {
+    const unsigned nbf = (unsigned)((((int64_t)lv.H >> 2) + kBlockF - 1) / kBlockF);
+    if (RW == 4 && topo && tmap && CCS_STEP_FQ) {
+        const unsigned nbc = nbf + (unsigned)(((int64_t)lv.C + kBlockF - 1) / kBlockF);
+        if (uv) launch_chained(k_level_fq<4, true, true, CREASED>, nbc, kBlockF, c.stream, a, map);
+        else launch_chained(k_level_fq<4, true, false, CREASED>, nbc, kBlockF, c.stream, a, map);
+    } else if (topo && tmap) {
         if (uv) launch_chained(k_level_ab<RW, true, true, CREASED, RW == 4>, nb, kBlockL, c.stream, a, map);
         else launch_chained(k_level_ab<RW, true, false, CREASED, RW == 4>, nb, kBlockL, c.stream, a, map);
     } else if (topo) {
         if (RW == 4 && uv) launch_chained(k_level_ab<RW, true, true, CREASED, false>, nb, kBlockL, c.stream, a, map);
         else launch_chained(k_level_ab<RW, true, false, CREASED, false>, nb, kBlockL, c.stream, a, map);
     } else {
-        launch_chained(k_level_ab<RW, false, false, CREASED, false>, nb, kBlockL, c.stream, a, map);
+        launch_chained(k_level_fq<RW, false, false, CREASED>, nbf, kBlockF, c.stream, a, map);
     }
     c.prof->end(c.stream);
 }

@@ -214,6 +214,20 @@ __device__ __forceinline__ void crease_stats_next(const LevelArgs& a, int32_t e,
 struct ARec {
     int32_t tw, ed, vx, uv;
 };
+// The four records of quad face f (RW = 3: three 16-byte loads of the 48
+// bytes; the fourth word is then 0)
+template <int RW>
+__device__ __forceinline__ void load_face_records(const int32_t* __restrict__ in, int64_t f, int4 (&r)[4]) {
+    const int4* q = reinterpret_cast<const int4*>(in + (int64_t)RW * 4 * f);
+    if constexpr (RW == 4) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) r[k] = __ldg(q + k);
+    } else {
+        const int4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
+        r[0] = make_int4(a.x, a.y, a.z, 0); r[1] = make_int4(a.w, b.x, b.y, 0);
+        r[2] = make_int4(b.z, b.w, c.x, 0); r[3] = make_int4(c.y, c.z, c.w, 0);
+    }
+}
 template <int RW>
 __device__ __forceinline__ ARec load_arec(const int32_t* __restrict__ in, int64_t h64, int64_t H) {
     ARec r{0, 0, 0, 0};
@@ -1725,6 +1739,114 @@ __device__ __forceinline__ void adj_quad_step_tile_g(const QuadView<RW>& L, cons
         atomic_add3(o, add3(s, sA2));
     } else if (k == 0) {
         atomic_add3(o, s);
+    }
+}
+
+// The same pass with one thread per depth-d face: lane j of a quad of lanes
+// takes face j of a parent quad (the structure k_level_fq relies on: face j
+// runs C_j, M_j, Z, M_{j-1}; inner edge j = (j, 1) | (j+1, 2); the halves of
+// parent edge j are (j, 0) and (j+1, 3)).  The terms of adj_quad_step_tile,
+// per halfedge k of the face: coefficients kc(k), ke(k) and own(k) =
+// cE(k) gV[v(k)] + dE(k+1) gV[v(k+1)]; the edge gradients
+//   gEt(0) = gE + own(0) + cE(t) gV[M_j] + dE(next t) gV[C_j]  (across parent edge j)
+//   gEt(1) = gE + own(1) + own(2) of the next lane              (inner edge j)
+//   gEt(2) = gEt(1) of the previous lane                        (inner edge j-1)
+//   gEt(3) = gE + own(3) + cB gV[C_j]                           (across parent edge j-1)
+// then the face gradient gF + sum_k (bF(k) gV[v(k)] + ga(k) gEt(k)) and the
+// four vertex terms a gV + al gEt + gF/4 + be(prev) gEt(prev): the corner's
+// and midpoint M_j's pair (with the next lane's (j+1, 3) term) by float
+// atomics, the centre's four by lane 0 of the quad.  Every coefficient and
+// edge term is evaluated once per face instead of once per lane of a
+// 16-lane group, with 15 shuffles per face.
+__device__ __forceinline__ ECoef ecoef_of(float s, bool bnd) {
+    const float w = fsat(s), b = bnd ? 1.0f : 0.5f;
+    return ECoef{(1.0f - w) * 0.25f + w * b * 0.5f, w * b * 0.5f, (1.0f - w) * 0.25f};
+}
+template <int RW, class GradIn>
+__device__ __forceinline__ void adj_face_step_tile(const QuadView<RW>& L, const GradIn gin,
+                                                   float* __restrict__ gOld, int64_t f) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31, qb = lane & ~3, j = lane & 3;
+    const int ln = qb | ((j + 1) & 3), lp = qb | ((j + 3) & 3);
+    const bool valid = f < ((int64_t)L.H >> 2);            // the four lanes of a quad agree
+    const int64_t fBase = L.V, eBase = (int64_t)L.V + L.F;
+    int4 r[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) r[k] = make_int4(-1, 0, 0, 0);
+    if (valid) load_face_records<RW>(L.he, f, r);
+    const int32_t tw0 = r[0].x, e0 = r[0].y, C = r[0].z;
+    const int32_t e1 = r[1].y, Mj = r[1].z, Z = r[2].z;
+    const int32_t tw3 = r[3].x, e3 = r[3].y, Mp = r[3].z;
+    f3 gC = zero3(), gM = zero3(), gZ = zero3(), gMp = zero3(), ge0 = zero3(), ge1 = zero3(), ge3 = zero3(),
+       gf = zero3();
+    float4 st = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    float s0 = 0.0f, s1 = 0.0f, s3 = 0.0f;
+    if (valid) {
+        gC = gin.at(C); gM = gin.at(Mj); gZ = gin.at(Z); gMp = gin.at(Mp);
+        ge0 = gin.at(eBase + e0); ge1 = gin.at(eBase + e1); ge3 = gin.at(eBase + e3);
+        gf = gin.at(fBase + f);
+        st = L.ostats[C];
+        s0 = L.sharp(e0); s1 = L.sharp(e1); s3 = L.sharp(e3);
+    }
+    // the other half of parent edge j is (j+1, 3), of parent edge j-1 is
+    // (j-1, 0); the edge of (j, 2) is inner edge j-1
+    const float s3n = __shfl_sync(full, s3, ln), s0p = __shfl_sync(full, s0, lp), s1p = __shfl_sync(full, s1, lp);
+    const bool obnd = st.w != 0.0f;                      // the older vertex C_j's ring is open
+    // vertex coefficients (lane_vertex_coef's cases) and edge coefficients
+    const VCoef k0 = coef_from_stats(st.x, obnd ? st.z - fsign(s0) : st.z, obnd ? st.y - s0 : st.y, obnd,
+                                     fsign(s0), fsign(s3));
+    const VCoef k1 = coef_from_stats(tw0 < 0 ? 2.0f : 4.0f, fsign(s0) + fsign(s3n), s0 + s3n, tw0 < 0,
+                                     fsign(s1), fsign(s0));
+    const VCoef k2 = coef_from_stats(4.0f, 0.0f, 0.0f, false, fsign(s1p), fsign(s1));
+    const VCoef k3 = coef_from_stats(tw3 < 0 ? 2.0f : 4.0f, tw3 < 0 ? fsign(s0p) : fsign(s3) + fsign(s0p),
+                                     tw3 < 0 ? s0p : s3 + s0p, tw3 < 0, fsign(s3), fsign(s1p));
+    const ECoef q0 = ecoef_of(s0, tw0 < 0), q1 = ecoef_of(s1, false), q2 = ecoef_of(s1p, false),
+                q3 = ecoef_of(s3, tw3 < 0);
+    // the edge gradients
+    const f3 own2 = add3(mul3(gZ, k2.cE), mul3(gMp, k3.dE));
+    f3 gEt1 = add3(add3(ge1, add3(mul3(gM, k1.cE), mul3(gZ, k2.dE))), shfl3(own2, ln));
+    f3 gEt0 = add3(ge0, add3(mul3(gC, k0.cE), mul3(gM, k1.dE)));
+    if (tw0 >= 0) {
+        // cE(t) at the midpoint (interior, valence 4); dE(next t) at C_j,
+        // non-zero only on an open ring in the crease branch
+        const VCoef ct = coef_from_stats(4.0f, fsign(s0) + fsign(s3n), s0 + s3n, false, fsign(s0), 0.0f);
+        float dEt = 0.0f;
+        const float valence = obnd ? st.x + 1.0f : st.x;
+        if (valid && obnd && !(st.z >= 3.0f || valence == 2.0f) && !(st.z <= 1.0f) && s0 != 0.0f) {
+            const float sn = L.sharp(L.edge(tw0 & ~3));  // next(t) = child 0 of t's quad
+            dEt = fsat((st.y - sn) * 0.5f) * 0.25f * fsign(s0);
+        }
+        gEt0 = add3(gEt0, add3(mul3(gM, ct.cE), mul3(gC, dEt)));
+    }
+    f3 gEt3 = add3(ge3, add3(mul3(gMp, k3.cE), mul3(gC, k0.dE)));
+    if (tw3 >= 0) {
+        // cE(t) at C_j seen from t, whose edge is (j, 3)'s
+        const float cB = coef_from_stats(st.x, obnd ? st.z - fsign(s3) : st.z, obnd ? st.y - s3 : st.y, obnd,
+                                         fsign(s3), 0.0f).cE;
+        gEt3 = add3(gEt3, mul3(gC, cB));
+    }
+    const f3 gEt2 = shfl3(gEt1, lp);
+    // the face gradient, then the four vertex terms
+    f3 gFt = add3(gf, add3(mul3(gC, k0.bF), mul3(gEt0, q0.ga)));
+    gFt = add3(gFt, add3(mul3(gM, k1.bF), mul3(gEt1, q1.ga)));
+    gFt = add3(gFt, add3(mul3(gZ, k2.bF), mul3(gEt2, q2.ga)));
+    gFt = add3(gFt, add3(mul3(gMp, k3.bF), mul3(gEt3, q3.ga)));
+    const f3 gF4 = mul3(gFt, 0.25f);
+    const f3 t0 = add3(add3(mul3(gC, k0.a), mul3(gEt0, q0.al)), add3(gF4, mul3(gEt3, q3.be)));
+    const f3 t1 = add3(add3(mul3(gM, k1.a), mul3(gEt1, q1.al)), add3(gF4, mul3(gEt0, q0.be)));
+    const f3 t2 = add3(add3(mul3(gZ, k2.a), mul3(gEt2, q2.al)), add3(gF4, mul3(gEt1, q1.be)));
+    const f3 t3 = add3(add3(mul3(gMp, k3.a), mul3(gEt3, q3.al)), add3(gF4, mul3(gEt2, q2.be)));
+    const f3 t3n = shfl3(t3, ln);
+    const f3 c1 = shfl3(t2, qb + 1), c2 = shfl3(t2, qb + 2), c3 = shfl3(t2, qb + 3);
+    if (!valid) return;
+    atomic_add3(gOld + 3 * (int64_t)C, t0);
+    atomic_add3(gOld + 3 * (int64_t)Mj, add3(t1, t3n));
+    if (j == 0) {
+        const f3 t = add3(add3(t2, c1), add3(c2, c3));
+        float* o = gOld + 3 * (int64_t)Z;
+        o[0] += t.x;
+        o[1] += t.y;
+        o[2] += t.z;
     }
 }
 

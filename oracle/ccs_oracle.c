@@ -558,6 +558,26 @@ void or_refine_points_scatter(or_subd *s, const real *cagePts)             /* :2
     }
 }
 
+/* One step d -> d+1 of the scatter rules (the loop body of :2631-2643 or
+ * :2645-2657) on the level-d points already in s->pts (d = 0: cagePts):
+ * level d+1's rows are cleared and recomputed.  With it a test holds one
+ * step of a float-atomic pass to the reference's arithmetic, on the level-d
+ * points that pass produced itself. */
+void or_step_points_scatter(or_subd *s, int32_t d, int32_t creased, const real *cagePts)
+{
+    lvl L;
+    lvl_init(&L, s, d, cagePts);
+    memset(L.out, 0, sizeof(real) * 3 * (size_t)or_V_at(s->cage, d + 1));
+    face_points_scatter(&L);
+    if (creased) {
+        creased_edge_points_scatter(&L);
+        creased_vertex_points_scatter(&L);
+    } else {
+        edge_points_scatter(&L);
+        vertex_points_scatter(&L);
+    }
+}
+
 void or_refine_points_nocreases_scatter(or_subd *s, const real *cagePts)   /* :2645-2657 */
 {
     int32_t d;

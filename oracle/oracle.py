@@ -59,6 +59,8 @@ def _lib(real) -> ctypes.CDLL:
                "or_refine_points_nocreases_scatter", "or_refine_points_nocreases_gather"):
         getattr(lib, fn).argtypes = [P, P]
         getattr(lib, fn).restype = None
+    lib.or_step_points_scatter.argtypes = [P, I, I, P]
+    lib.or_step_points_scatter.restype = None
     lib.or_adjoint_points_scatter.argtypes = [P, P, P, P]
     lib.or_adjoint_points_scatter.restype = None
     lib.or_edge_to_halfedge.argtypes = [P, I, I]
@@ -142,6 +144,21 @@ def refine_points(cage, depth: int, he, cr, mode: str = "scatter", real=np.float
     s = _Subd(c.addr, depth, stride, _ptr(he), _ptr(cr), _ptr(pts))
     getattr(_lib(real), _POINT_FNS[mode])(ctypes.addressof(s), _ptr(cp))
     return pts
+
+
+def step_points(cage, depth: int, he, cr, pts, d: int, creased: bool = True, cage_points=None,
+                stride: int = 4):
+    """Level d+1 of `pts` (sum_V x 3, levels 1..depth, FP32) recomputed by the
+    scatter rules from the level-d rows already in `pts` (d = 0: the cage
+    points): returns a copy of `pts` with only level d+1 replaced."""
+    out = np.array(pts, np.float32, copy=True, order="C")
+    cp = np.ascontiguousarray(cage.vertex_points if cage_points is None else cage_points, np.float32)
+    he = np.ascontiguousarray(he, np.int32)
+    cr = np.ascontiguousarray(cr, CREASE_DTYPE)
+    c = _CageRef(cage)
+    s = _Subd(c.addr, depth, stride, _ptr(he), _ptr(cr), _ptr(out))
+    _lib(np.float32).or_step_points_scatter(ctypes.addressof(s), d, 1 if creased else 0, _ptr(cp))
+    return out
 
 
 def refine(cage, depth: int, mode: str = "scatter", real=np.float32, stride: int = 4,

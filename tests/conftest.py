@@ -99,3 +99,25 @@ def small_cages():
         ("creased_quad_uv", build_cage(quad, [[0, 1, 2, 3]], uvs=uvs, face_uvs=[[0, 1, 2, 3]],
                                        crease_tags=[(0, 1, 1.5)])),
     ]
+
+
+def check_steps(cage, depth, he, cr, pts, creased, steps=None, tol=2e-6):
+    """Steps d -> d+1 (default: all but the cage step, d >= 1) of a default
+    (float-atomic) pass against the reference's own step on the pass's
+    level-d points: face and edge points bit for bit (their sums have a fixed
+    order), vertex points within `tol` of the level's largest coordinate (the
+    atomics' order).  The default cage step applies the step as a sparse map
+    with double sums, so its face and edge points are only within `tol`."""
+    from oracle import oracle
+    cnt = oracle.counts(cage, depth)
+    for d in (range(1, depth) if steps is None else steps):
+        ref = oracle.step_points(cage, depth, he, cr, pts, d, creased)
+        a, V0, V1 = cnt["cumV"][d], cnt["V"][d], cnt["V"][d + 1]
+        got, want = pts[a:a + V1], ref[a:a + V1]
+        if d == 0:
+            V0 = V1
+        i = np.flatnonzero((got[V0:].view(np.uint32) != want[V0:].view(np.uint32)).any(axis=1))
+        assert i.size == 0, "step %d: face/edge point %d not bit-exact" % (d, V0 + i[0])
+        scale = float(np.abs(want).max())
+        err = float(np.abs(got[:V0].astype(np.float64) - want[:V0]).max()) / scale
+        assert err <= tol, "step %d: vertex points off by %.3g" % (d, err)

@@ -149,6 +149,26 @@ def test_mixed_torus_depth6_every_level_vs_reference():
     print("mixed_torus depth 6: default points max-norm rel err vs reference %.3g" % err)
 
 
+def test_mixed_torus_depth6_default_steps_vs_reference_steps():
+    """The default pass's two largest steps (depth 4 -> 5 and 5 -> 6: 17.8 M
+    parent halfedges in the last) against the reference's step rules
+    (oracle.step_points, pinned to the reference) applied to the pass's own
+    previous level: face and edge points bit for bit, vertex points within
+    2e-6 -- for the full refine and for the points-only call."""
+    from conftest import check_steps
+    from halfedgecatmullclark_b200 import configs
+    from halfedgecatmullclark_b200.subd import Subd
+    w = configs.mixed_torus()
+    with Subd(w.cage, w.depth) as s:
+        s.refine_scatter()
+        s.download()
+        he, cr, pts = s.halfedges(), s.creases(), s.points()
+        check_steps(w.cage, w.depth, he, cr, pts, True, steps=[4, 5])
+        s.refine_vertex_points("scatter")
+        s.download()
+        check_steps(w.cage, w.depth, he, cr, s.points(), True, steps=[4, 5])
+
+
 def test_height_grid_depth5_every_level_vs_reference():
     """Config 3 at its full depth 5: 393 M refined halfedges (6.3 GB of
     records), where 64-bit byte offsets meet int32 element ids, every level

@@ -189,3 +189,32 @@ def test_maps_are_consistent(small_workloads):
             for v in range(0, cnt["V"][d], max(1, cnt["V"][d] // 200)):
                 h = oracle.vertex_to_halfedge(w.cage, v, d)
                 assert lv[h, 2] == v
+
+
+@pytest.mark.parametrize("mode", ["scatter", "nocreases_scatter"])
+def test_step_points_compose_to_the_full_pass(small_workloads, mode):
+    """oracle.step_points (one step of the scatter rules on given level-d
+    points) applied depth by depth reproduces the full points pass bit for
+    bit, and the per-step checker passes it and catches a planted error in
+    an edge point and in a vertex point."""
+    from conftest import check_steps
+    from oracle import oracle
+    creased = mode == "scatter"
+    for w in small_workloads:
+        he, cr, pts = oracle.refine(w.cage, w.depth, mode)
+        acc = np.zeros_like(pts)
+        for d in range(w.depth):
+            acc = oracle.step_points(w.cage, w.depth, he, cr, acc, d, creased)
+        assert np.array_equal(acc.view(np.uint32), pts.view(np.uint32)), w.name
+        check_steps(w.cage, w.depth, he, cr, pts, creased, steps=range(w.depth))
+    cnt = oracle.counts(w.cage, w.depth)
+    d = w.depth - 1
+    edge_row = cnt["cumV"][d] + cnt["V"][d + 1] - 1
+    bad = pts.copy()
+    bad[edge_row, 0] = np.nextafter(bad[edge_row, 0], np.float32(np.inf))
+    with pytest.raises(AssertionError, match="not bit-exact"):
+        check_steps(w.cage, w.depth, he, cr, bad, creased, steps=[d])
+    bad = pts.copy()
+    bad[cnt["cumV"][d], 1] += np.float32(1e-3) * np.abs(pts).max()
+    with pytest.raises(AssertionError, match="vertex points"):
+        check_steps(w.cage, w.depth, he, cr, bad, creased, steps=[d])

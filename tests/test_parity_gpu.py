@@ -10,7 +10,7 @@ alongside.
 import numpy as np
 import pytest
 
-from conftest import ccm_paths, gpu_available, rel_err
+from conftest import ccm_paths, check_steps, gpu_available, rel_err
 
 pytestmark = pytest.mark.gpu
 
@@ -89,6 +89,24 @@ def test_error_against_fp64_oracle(small_workloads):
         # the GPU is as accurate as the reference's own FP32 order
         assert e_gpu <= 4 * e_ref + 1e-7, "%s: gpu %.3g vs fp32 order %.3g" % (name, e_gpu, e_ref)
         assert rms <= e_gpu + 1e-12
+
+
+@pytest.mark.parametrize("mode", ["scatter", "nocreases_scatter"])
+def test_default_steps_match_reference_steps(small_workloads, mode):
+    """Each step of the default pass (the one-launch steps at depth >= 2 with
+    their float atomics, both the full refine and the points-only call)
+    reproduces the reference's step arithmetic on its own previous level
+    (the cage step, a sparse map with double sums, within tolerance)."""
+    from halfedgecatmullclark_b200.subd import Subd
+    for w in small_workloads:
+        with Subd(w.cage, w.depth) as s:
+            s.refine(mode)
+            s.download()
+            he, cr, pts = s.halfedges(), s.creases(), s.points()
+            check_steps(w.cage, w.depth, he, cr, pts, mode == "scatter", steps=range(w.depth))
+            s.refine_vertex_points(mode)
+            s.download()
+            check_steps(w.cage, w.depth, he, cr, s.points(), mode == "scatter", steps=range(w.depth))
 
 
 def test_separate_entry_points(small_workloads):
