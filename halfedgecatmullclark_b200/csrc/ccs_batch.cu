@@ -64,6 +64,8 @@ enum Phase {
     PH_CREASE_STATS_NEXT,  // C_(d+1) creases of depth d + 1 (their statistics, before depth d + 1)
     PH_DIST,            // d = 0: the points whose fitting gradient P - T the distance adjoint
                         // writes before its steps (every level but a depth >= 3 cage's finest)
+    PH_AF,              // d >= 2: F_d faces (the points-only step, one thread per face)
+    PH_ADJ_FSTEP,       // d >= 2: F_d faces (the adjoint step, one thread per face)
     PH_COUNT
 };
 
@@ -314,9 +316,31 @@ __device__ __forceinline__ void fwd_crease_stats(const BatchArgs& a, int d, int 
     });
 }
 
-// default pass, depth d >= 2, section 1
+// default pass, depth d >= 2, section 1 (the points-only step: one thread
+// per face, fq_points; with the topology: one thread per parent halfedge,
+// tile_level_ab)
 template <bool TOPO, bool CREASED>
 __device__ __forceinline__ void fwd_level_ab(const BatchArgs& a, int d, int32_t* tile) {
+        if (!TOPO) {
+            for_tiles(a, d, PH_AF, [&](const BatchCage& bc, int64_t lt) {
+                LevelArgs la = batch_level_args(a, bc, d);
+                la.ostats = a.stats + bc.stats[d];
+                const int64_t f = lt * kBatchBlock + threadIdx.x;
+                const bool valid = f < bc.lv[d].F;
+                int4 r[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) r[k] = make_int4(-1, 0, 0, 0);
+                if (valid) load_face_records<4>(la.in, f, r);
+                fq_points<4, CREASED>(la, f, valid, r);
+                if (d + 2 <= bc.depth) {
+                    float* z = a.pts + 3 * (bc.pt + bc.lv[d + 2].ptOff);
+                    const int64_t n = 3 * (int64_t)bc.lv[d + 1].V;
+                    const int64_t stride = (((int64_t)bc.lv[d].F + kBatchBlock - 1) / kBatchBlock) * kBatchBlock;
+                    for (int64_t i = f; i < n; i += stride) z[i] = 0.0f;
+                }
+            });
+            return;
+        }
         for_tiles(a, d, PH_A, [&](const BatchCage& bc, int64_t lt) {
             LevelArgs la = batch_level_args(a, bc, d);
             la.ostats = a.stats + bc.stats[d];
@@ -423,17 +447,18 @@ __device__ __forceinline__ void adj_cage_section(const BatchArgs& a) {
     }
 }
 
-// adjoint, d >= 2: one pass (adj_quad_step_tile)
+// adjoint, d >= 2: one pass, one thread per face (adj_face_step_tile)
 __device__ __forceinline__ void adj_level_step(const BatchArgs& a, int d) {
-    for_tiles(a, d, PH_ADJ_VERT, [&](const BatchCage& bc, int64_t lt) {
+    for_tiles(a, d, PH_ADJ_FSTEP, [&](const BatchCage& bc, int64_t lt) {
         float* gOld = a.work + 3 * (bc.pt + bc.lv[d].ptOff);
+        const QuadView<4> L = batch_quad_view_stats(a, bc, d);
+        const int64_t f = lt * kBatchBlock + threadIdx.x;
         if (a.target && d + 1 == bc.depth) {
             // distance adjoint, the cage's finest level: its gradient P - T as it is read
             const int64_t o = 3 * (bc.pt + bc.lv[d + 1].ptOff);
-            adj_quad_step_tile_g<4, GradDistance>(batch_quad_view_stats(a, bc, d),
-                                                  GradDistance{a.pts + o, a.target + o}, gOld, lt * kBatchBlock);
+            adj_face_step_tile<4, GradDistance>(L, GradDistance{a.pts + o, a.target + o}, gOld, f);
         } else {
-            adj_quad_step_tile<4>(batch_quad_view_stats(a, bc, d), adj_gnew(a, bc, d), gOld, lt * kBatchBlock);
+            adj_face_step_tile<4, GradArray>(L, GradArray{adj_gnew(a, bc, d)}, gOld, f);
         }
     });
 }
@@ -511,9 +536,8 @@ k_batch_adjoint(BatchArgs a, int d) {
 }
 
 // split schedule, adjoint, depth d >= 2: the one-pass step on its own register budget
-// (6 resident blocks of 256 measured 5 % faster than 5 on the uneven 512-cage batch)
 #ifndef CCS_BATCH_ADJ_STEP_MIN_BLOCKS
-#define CCS_BATCH_ADJ_STEP_MIN_BLOCKS 6
+#define CCS_BATCH_ADJ_STEP_MIN_BLOCKS 3
 #endif
 __global__ void __launch_bounds__(kBatchBlock, CCS_BATCH_ADJ_STEP_MIN_BLOCKS)
 k_batch_adj_step(BatchArgs a, int d) {
@@ -540,9 +564,10 @@ k_batch_forward_section(BatchArgs a, int d) {
 }
 
 // split schedule, default pass, depth d >= 2: section 1 on its own register
-// budget (the single-mesh one-pass step's)
+// budget (the single-mesh steps': 6 blocks of 256 for the per-halfedge tile,
+// 3 for the per-face one)
 template <bool TOPO, bool CREASED>
-__global__ void __launch_bounds__(kBatchBlock, 6)
+__global__ void __launch_bounds__(kBatchBlock, TOPO ? 6 : 3)
 k_batch_level_ab(BatchArgs a, int d) {
     __shared__ __align__(128) int32_t tile[kBatchBlock * 4 * 4];
     fwd_level_ab<TOPO, CREASED>(a, d, tile);
@@ -631,6 +656,8 @@ static int64_t phase_units(const BatchCage& bc, int d, int ph) {
         case PH_ZERO3: return d == 1 && bc.depth >= 3 ? bc.lv[2].V : 0;
         case PH_CREASE_STATS_NEXT: return d >= 1 && d + 1 < bc.depth ? bc.lv[d + 1].C : 0;
         case PH_DIST: return d == 0 ? dist_points(bc) : 0;
+        case PH_AF: return d >= 2 ? lv.F : 0;
+        case PH_ADJ_FSTEP: return d >= 2 ? lv.F : 0;
         default: return 0;
     }
 }
@@ -839,7 +866,8 @@ static cudaError_t forward_sections(ccs_Batch* b, const BatchArgs& a, int d) {
     }
     if (!DET && d >= 2) {
         e = launch_persistent(b, k_batch_level_ab<TOPO, CREASED>,
-                              max_tiles(b, d, {PH_A, PH_A_CREASE, PH_SHAPE_NEXT}), a, d, false);
+                              TOPO ? max_tiles(b, d, {PH_A, PH_A_CREASE, PH_SHAPE_NEXT}) : max_tiles(b, d, {PH_AF}),
+                              a, d, false);
         if (e == cudaSuccess && TOPO)
             e = launch_persistent(b, k_batch_forward_section<TOPO, CREASED, DET, SEC_LEVEL_2>,
                                   max_tiles(b, d, {PH_CREASE_STATS_NEXT}), a, d, false);
@@ -880,7 +908,7 @@ static cudaError_t enqueue_batch(ccs_Batch* b, int op, bool creased) {
                 if (e == cudaSuccess)
                     e = launch_persistent(b, k_batch_adjoint_section<SEC_CAGE_3>, max_tiles(b, 0, {PH_ADJ_VERT}), a, 0, false);
             } else if (d >= 2) {
-                e = launch_persistent(b, k_batch_adj_step, max_tiles(b, d, {PH_ADJ_VERT}), a, d, false);
+                e = launch_persistent(b, k_batch_adj_step, max_tiles(b, d, {PH_ADJ_FSTEP}), a, d, false);
             } else {
                 e = launch_persistent(b, k_batch_adjoint_section<SEC_LEVEL_1>, max_tiles(b, d, {PH_ADJ_EDGE}), a, d, false);
                 if (e == cudaSuccess)

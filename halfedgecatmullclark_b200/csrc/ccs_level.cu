@@ -203,7 +203,6 @@ __global__ void __launch_bounds__(kBlockF, CCS_FQ_MIN_BLOCKS)
 k_level_fq(LevelArgs a, const __grid_constant__ CUtensorMap childMap) {
     static_assert(!TOPO || RW == 4, "the child records go out through the 16-byte record tensor map");
     chain_wait_then_release();
-    const unsigned full = 0xffffffffu;
     const int64_t nF = (int64_t)a.H >> 2;                  // depth-d faces (H = 16 n at d >= 2)
     const int nbF = (int)((nF + kBlockF - 1) / kBlockF);
     if (TOPO && (int)blockIdx.x >= nbF) {
@@ -224,8 +223,6 @@ k_level_fq(LevelArgs a, const __grid_constant__ CUtensorMap childMap) {
         }
     }
     const bool valid = f < nF;                             // the four lanes of a quad agree
-    const int lane = threadIdx.x & 31, qb = lane & ~3, j = lane & 3;
-    const int ln = qb | ((j + 1) & 3), lp = qb | ((j + 3) & 3);
     const int32_t h0 = (int32_t)(4 * f);
     int4 r[4];
 #pragma unroll
@@ -281,116 +278,8 @@ k_level_fq(LevelArgs a, const __grid_constant__ CUtensorMap childMap) {
         }
     }
 
-    const int32_t tw0 = r[0].x, e0 = r[0].y, C = r[0].z;  // (j, 0): C_j -> M_j
-    const int32_t e1 = r[1].y, Mj = r[1].z;               // (j, 1): M_j -> Z, inner edge j
-    const int32_t Z = r[2].z;                             // (j, 2): Z -> M_{j-1}
-    const int32_t tw3 = r[3].x, e3 = r[3].y, Mp = r[3].z; // (j, 3): M_{j-1} -> C_j
-    // across parent edge j: the far vertex of (j, 0)'s twin quad and that
-    // quad's centre; across parent edge j-1: the far vertex of (j, 3)'s
-    int32_t vX0 = 0, vF0 = 0, vX3 = 0;
-    if (valid && tw0 >= 0) {
-        vX0 = __ldg(a.in + (int64_t)RW * ((tw0 & ~3) + 1) + 2);
-        vF0 = __ldg(a.in + (int64_t)RW * ((tw0 & ~3) + 2) + 2);
-    }
-    if (valid && tw3 >= 0) vX3 = __ldg(a.in + (int64_t)RW * ((tw3 & ~3) + 3) + 2);
-    f3 pC = zero3(), pM = zero3(), pZ = zero3(), pMp = zero3(), qX0 = zero3(), qF0 = zero3(), qX3 = zero3();
-    float4 st = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    float s0 = 0.0f, s1 = 0.0f, s3 = 0.0f;
-    if (valid) {
-        pC = ld3(a.pin + 3 * (int64_t)C);
-        pM = ld3(a.pin + 3 * (int64_t)Mj);
-        pZ = ld3(a.pin + 3 * (int64_t)Z);
-        pMp = ld3(a.pin + 3 * (int64_t)Mp);
-        st = a.ostats[C];
-        if (CREASED) {
-            s0 = e0 < a.C ? __ldg(&a.crIn[e0].sharpness) : 0.0f;
-            s1 = e1 < a.C ? __ldg(&a.crIn[e1].sharpness) : 0.0f;
-            s3 = e3 < a.C ? __ldg(&a.crIn[e3].sharpness) : 0.0f;
-        }
-        if (tw0 >= 0) {
-            qX0 = ld3(a.pin + 3 * (int64_t)vX0);
-            qF0 = ld3(a.pin + 3 * (int64_t)vF0);
-        }
-        if (tw3 >= 0) qX3 = ld3(a.pin + 3 * (int64_t)vX3);
-    }
-    // the other half of parent edge j is (j+1, 3), of parent edge j-1 is
-    // (j-1, 0); the edge of (j, 2) is inner edge j-1
-    const float s3n = __shfl_sync(full, s3, ln), s0p = __shfl_sync(full, s0, lp), s1p = __shfl_sync(full, s1, lp);
+    fq_points<RW, CREASED>(a, f, valid, r);
 
-    // face point
-    const f3 F = add3(add3(add3(add3(zero3(), quarter3(pC)), quarter3(pM)), quarter3(pZ)), quarter3(pMp));
-    if (valid) st3(a.pout + 3 * ((int64_t)a.V + f), F);
-    const int64_t eOut = (int64_t)a.V + a.F;
-    // inner edge j: (j, 1) and its twin (j+1, 2), with the next lane's face point
-    const f3 Fn = shfl3(F, ln);
-    f3 I;
-    {
-        const float w = CREASED ? fsat(s1) : 0.0f;
-        I = add3(add3(zero3(), edge_share_fast<CREASED>(pM, pZ, F, false, w)),
-                 edge_share_fast<CREASED>(pZ, pM, Fn, false, w));
-        if (valid) st3(a.pout + 3 * (eOut + e1), I);
-    }
-    const f3 Ip = shfl3(I, lp);                            // inner edge j-1
-    // (j, 0): C_j -> M_j, half of parent edge j
-    f3 Eo0;
-    {
-        const float w = CREASED ? fsat(s0) : 0.0f;
-        const f3 sh = edge_share_fast<CREASED>(pC, pM, F, tw0 < 0, w);
-        if (tw0 >= 0) {
-            const f3 Ft = add3(add3(add3(add3(zero3(), quarter3(pC)), quarter3(qX0)), quarter3(qF0)), quarter3(pM));
-            Eo0 = add3(add3(zero3(), sh), edge_share_fast<CREASED>(pM, pC, Ft, false, w));
-        } else {
-            Eo0 = add3(zero3(), sh);
-        }
-        if (valid && h0 > tw0) st3(a.pout + 3 * (eOut + e0), Eo0);
-    }
-    // (j, 3): M_{j-1} -> C_j, half of parent edge j-1, whose twin quad's
-    // centre the previous lane read
-    const f3 qFp = shfl3(qF0, lp);
-    f3 Eo3;
-    {
-        const float w = CREASED ? fsat(s3) : 0.0f;
-        const f3 sh = edge_share_fast<CREASED>(pMp, pC, F, tw3 < 0, w);
-        if (tw3 >= 0) {
-            const f3 Ft = add3(add3(add3(add3(zero3(), quarter3(pC)), quarter3(pMp)), quarter3(qFp)), quarter3(qX3));
-            Eo3 = add3(add3(zero3(), sh), edge_share_fast<CREASED>(pC, pMp, Ft, false, w));
-        } else {
-            Eo3 = add3(zero3(), sh);
-        }
-        if (valid && h0 + 3 > tw3) st3(a.pout + 3 * (eOut + e3), Eo3);
-    }
-    // vertex shares (tile_level_b's rules)
-    {   // (j, 0): the corner; on a boundary the walk from it skips its own edge
-        const bool bnd = st.w != 0.0f;
-        const float avgS = CREASED ? (bnd ? fsub(st.y, s0) : st.y) : 0.0f;
-        const float cpre = CREASED ? (bnd ? fsub(st.z, fsign(s0)) : st.z) : 0.0f;
-        const f3 s = quad_vertex_rule<CREASED>(pC, F, Eo0, Eo3, st.x, cpre, avgS, bnd,
-                                               CREASED ? fsign(s0) : 0.0f, CREASED ? fsign(s3) : 0.0f);
-        if (valid) atomic_add3(a.pout + 3 * (int64_t)C, s);
-    }
-    f3 sM3;
-    {   // (j, 3): midpoint M_{j-1}; the walk from it skips its own edge
-        const bool bnd = tw3 < 0;
-        const float avgS = CREASED ? (bnd ? s0p : fadd(s3, s0p)) : 0.0f;
-        const float cpre = CREASED ? (bnd ? fsign(s0p) : fadd(fsign(s3), fsign(s0p))) : 0.0f;
-        sM3 = quad_vertex_rule<CREASED>(pMp, F, Eo3, Ip, bnd ? 2.0f : 4.0f, cpre, avgS, bnd,
-                                        CREASED ? fsign(s3) : 0.0f, CREASED ? fsign(s1p) : 0.0f);
-    }
-    {   // (j, 1): midpoint M_j, added with the next lane's (j+1, 3) share
-        const bool bnd = tw0 < 0;
-        const float avgS = CREASED ? fadd(s0, s3n) : 0.0f;
-        const float cpre = CREASED ? fadd(fsign(s0), fsign(s3n)) : 0.0f;
-        const f3 s = quad_vertex_rule<CREASED>(pM, F, I, Eo0, bnd ? 2.0f : 4.0f, cpre, avgS, bnd,
-                                               CREASED ? fsign(s1) : 0.0f, CREASED ? fsign(s0) : 0.0f);
-        const f3 sn = shfl3(sM3, ln);
-        if (valid) atomic_add3(a.pout + 3 * (int64_t)Mj, add3(s, sn));
-    }
-    {   // (j, 2): the centre, summed by lane 0 of the quad in face order
-        const f3 s = quad_vertex_rule<CREASED>(pZ, F, Ip, I, 4.0f, 0.0f, 0.0f, false,
-                                               CREASED ? fsign(s1p) : 0.0f, CREASED ? fsign(s1) : 0.0f);
-        const f3 a1 = shfl3(s, qb + 1), a2 = shfl3(s, qb + 2), a3 = shfl3(s, qb + 3);
-        if (valid && j == 0) st3(a.pout + 3 * (int64_t)Z, add3(add3(add3(add3(zero3(), s), a1), a2), a3));
-    }
     // the slots the step after next accumulates into
     const int64_t nT = (int64_t)nbF * kBlockF;
     for (int64_t i = f; i < a.zeroNextN; i += nT) a.zeroNext[i] = 0.0f;
