@@ -109,16 +109,20 @@ k_adj_quad_step(QuadView<RW> L, const float* __restrict__ gNew, float* __restric
     adj_quad_step_tile<RW>(L, gNew, gOld, (int64_t)blockIdx.x * kBlockA);
 }
 
-// quad levels d >= 2, one thread per face (adj_face_step_tile)
+// quad levels d >= 2, one thread per face (adj_face_step_tile).  Depth 5 of
+// the headline workload: 0.364 ms with the per-halfedge tile; per face,
+// 6 resident blocks of 128 (78 registers) 0.187 ms, 8 (64 registers, a
+// 16-byte spill) 0.176 ms; the L2 prefetch of the records one wave ahead is
+// worth 1 % (the same from 592 to 2368 blocks ahead)
 static constexpr int kBlockAF = 128;
 #ifndef CCS_ADJ_FQ
 #define CCS_ADJ_FQ 1
 #endif
 #ifndef CCS_ADJ_FQ_MIN_BLOCKS
-#define CCS_ADJ_FQ_MIN_BLOCKS 6
+#define CCS_ADJ_FQ_MIN_BLOCKS 8
 #endif
 #ifndef CCS_ADJ_FQ_PREFETCH_AHEAD
-#define CCS_ADJ_FQ_PREFETCH_AHEAD 888
+#define CCS_ADJ_FQ_PREFETCH_AHEAD 1184
 #endif
 template <int RW>
 __global__ void __launch_bounds__(kBlockAF, CCS_ADJ_FQ_MIN_BLOCKS)

@@ -191,6 +191,12 @@ static constexpr int kBlockF = 128;                      // faces per block
 #define CCS_STEP_FQ 1
 #endif
 
+// Resident blocks of 128 and the L2 prefetch of the records one wave ahead.
+// Depth 5 of the headline workload: 7 blocks (70 registers) against 6 and 8
+// the same for the full step and 0.221 against 0.232 ms (8, 64 registers)
+// for the points-only step; the prefetch 0.236 -> 0.221 ms for the
+// points-only step, the full step the same at 1036 blocks ahead and 3 %
+// slower at 2072.
 #ifndef CCS_FQ_MIN_BLOCKS
 #define CCS_FQ_MIN_BLOCKS 7
 #endif
