@@ -414,9 +414,11 @@ def max_over_ranks(x, world):
     return float(t.item())
 
 
-def adjoint_timing(subd, w, stream, flush, steps, torch):
+def adjoint_timing(subd, w, stream, flush, steps, torch, peak=None):
     """Device ms of one adjoint pass (ccs_AdjointPointsDevice_cuda) and its
-    per-kernel profile, on the workload's subd (topology already refined)."""
+    per-kernel profile, on the workload's subd (topology already refined);
+    the one-pass steps at depth >= 2 carry their algorithmic bytes
+    (metrics.kernel_bytes("adj_step")) and fraction of `peak` GB/s."""
     import ctypes
     g = torch.randn((subd.cumV, 3), device="cuda")
     gc = torch.empty((w.cage.V, 3), device="cuda")
@@ -448,8 +450,15 @@ def adjoint_timing(subd, w, stream, flush, steps, torch):
     for r in recs:
         by[(r["kernel"], r["level"])] = by.get((r["kernel"], r["level"]), 0.0) + r["ms"]
     top = sorted(by.items(), key=lambda kv: -kv[1])[:10]
-    return {"ms_per_pass": mean, "halfedges_per_s": subd_halfedges(subd) / (mean / 1e3),
-            "kernels": [{"kernel": k[0], "level": k[1], "ms": v} for k, v in top]}
+    from halfedgecatmullclark_b200 import metrics
+    kernels = []
+    for (name, level), v in top:
+        e = {"kernel": name, "level": level, "ms": v}
+        if name == "adj_step" and peak:
+            nb = metrics.kernel_bytes("adj_step", subd.levels[level], 4 * subd.record_words)
+            e.update({"alg_bytes": nb, "gbs": nb / (v / 1e3) / 1e9, "frac_of_peak": nb / (v / 1e3) / 1e9 / peak})
+        kernels.append(e)
+    return {"ms_per_pass": mean, "halfedges_per_s": subd_halfedges(subd) / (mean / 1e3), "kernels": kernels}
 
 
 def subd_halfedges(subd):
@@ -803,7 +812,7 @@ def main():
 
     # adjoint of the same workload (points of every depth -> cage points),
     # through the C ABI on the subd's stream
-    adj = adjoint_timing(subd, w, stream, flush, args.steps, torch)
+    adj = adjoint_timing(subd, w, stream, flush, args.steps, torch, peak)
 
     # end to end through the C ABI with host buffers
     host_pts = torch.from_numpy(w.cage.vertex_points.copy()).pin_memory()

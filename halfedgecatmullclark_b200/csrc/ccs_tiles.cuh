@@ -735,7 +735,10 @@ __device__ __forceinline__ void fq_points(const LevelArgs& a, int64_t f, bool va
     int32_t vX0 = 0, vF0 = 0, vX3 = 0;
     if (valid && tw0 >= 0) {
         vX0 = __ldg(a.in + (int64_t)RW * ((tw0 & ~3) + 1) + 2);
-        vF0 = __ldg(a.in + (int64_t)RW * ((tw0 & ~3) + 2) + 2);
+        // the centre of parent quad T is vertex V(d-1) + T (the face points
+        // follow the older vertices), and Z - G = V(d-1): no record read
+        // (depth 5 of the headline workload: points-only step 0.221 -> 0.217 ms)
+        vF0 = Z - (int32_t)(f >> 2) + (tw0 >> 4);
     }
     if (valid && tw3 >= 0) vX3 = __ldg(a.in + (int64_t)RW * ((tw3 & ~3) + 3) + 2);
     f3 pC = zero3(), pM = zero3(), pZ = zero3(), pMp = zero3(), qX0 = zero3(), qF0 = zero3(), qX3 = zero3();
