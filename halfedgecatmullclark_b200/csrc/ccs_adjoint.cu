@@ -13,10 +13,9 @@
 // file computes dL/d(points of depth d) += S_d^T g.
 //
 // Quad levels d >= 2 (cages with the twin relation, ring statistics kept):
-// one pass with one thread per depth-d face, adj_face_step_tile, which
-// completes each edge's gradient once and then adds the vertex terms (the
-// batched path runs the halfedge-parallel form of the same pass,
-// adj_quad_step_tile).
+// one pass with one thread per depth-d face, adj_face_step_tile (the
+// batched path too), which completes each edge's gradient once and then adds
+// the vertex terms.
 // Depth 1: two halfedge-parallel passes with the forward's lane layout
 // (ccs_tiles.cuh adj_quad_*):
 //   1. gE[e] += the cE / dE terms, completed by the pair's larger halfedge
@@ -81,43 +80,12 @@ k_adj_quad_edges(QuadView<RW> L, float* __restrict__ gNew) {
     adj_quad_edge_tile<RW>(L, gNew, (int64_t)blockIdx.x * kBlockA);
 }
 
-// quad levels d >= 2 with the older vertices' statistics: one pass (6
-// resident blocks of 256 at 40 registers measured 2 % faster than 5 at 48)
-#ifndef CCS_ADJ_STEP_MIN_BLOCKS
-#define CCS_ADJ_STEP_MIN_BLOCKS 6
-#endif
-// blocks ahead whose records k_adj_quad_step asks L2 to fetch (0: none):
-// one wave, as k_level_ab (depth 5 of the headline workload: 0.362 ->
-// 0.352 ms)
-#ifndef CCS_ADJ_PREFETCH_AHEAD
-#define CCS_ADJ_PREFETCH_AHEAD 888
-#endif
-template <int RW>
-__global__ void __launch_bounds__(kBlockA, CCS_ADJ_STEP_MIN_BLOCKS)
-k_adj_quad_step(QuadView<RW> L, const float* __restrict__ gNew, float* __restrict__ gOld) {
-    chain_wait_then_release();
-#if CCS_ADJ_PREFETCH_AHEAD > 0
-    if (threadIdx.x == 0) {
-        const int64_t p0 = ((int64_t)blockIdx.x + CCS_ADJ_PREFETCH_AHEAD) * kBlockA;
-        if (p0 < L.H) {
-            const int64_t n = (L.H - p0) < kBlockA ? (L.H - p0) : kBlockA;
-            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
-                         :: "l"(L.he + (int64_t)RW * p0), "r"((uint32_t)(n * 4 * RW)) : "memory");
-        }
-    }
-#endif
-    adj_quad_step_tile<RW>(L, gNew, gOld, (int64_t)blockIdx.x * kBlockA);
-}
-
 // quad levels d >= 2, one thread per face (adj_face_step_tile).  Depth 5 of
 // the headline workload: 0.364 ms with the per-halfedge tile; per face,
 // 6 resident blocks of 128 (78 registers) 0.187 ms, 8 (64 registers, a
 // 16-byte spill) 0.176 ms; the L2 prefetch of the records one wave ahead is
 // worth 1 % (the same from 592 to 2368 blocks ahead)
 static constexpr int kBlockAF = 128;
-#ifndef CCS_ADJ_FQ
-#define CCS_ADJ_FQ 1
-#endif
 #ifndef CCS_ADJ_FQ_MIN_BLOCKS
 #define CCS_ADJ_FQ_MIN_BLOCKS 8
 #endif
@@ -153,11 +121,8 @@ static void adjoint_quad_level(const Ctx& c, const QuadView<RW>& L, float* gNew,
 #ifndef CCS_NO_ADJ_STEP
     if (L.d >= 2 && L.ostats) {
         c.prof->begin(c.stream, CCS_K_ADJ_STEP, L.d, L.H);
-        if (CCS_ADJ_FQ)
-            launch_chained(k_adj_face_step<RW>, (unsigned)((((int64_t)L.H >> 2) + kBlockAF - 1) / kBlockAF),
-                           kBlockAF, c.stream, L, gNew, gOld);
-        else
-            launch_chained(k_adj_quad_step<RW>, nblocksA(L.H), kBlockA, c.stream, L, gNew, gOld);
+        launch_chained(k_adj_face_step<RW>, (unsigned)((((int64_t)L.H >> 2) + kBlockAF - 1) / kBlockAF),
+                       kBlockAF, c.stream, L, gNew, gOld);
         c.prof->end(c.stream);
         return;
     }

@@ -1710,30 +1710,30 @@ __device__ __forceinline__ void adj_quad_point_tile(const QuadView<RW>& L, const
     }
 }
 
-// One pass for a quad level d >= 2 of the adjoint (tile of halfedges
-// [h0, h0 + blockDim), the forward's lane layout): pass 1's edge gradient is
-// completed by both halves of every edge instead of accumulated by atomics,
-// then pass 2's vertex terms follow in the same thread.
+// One pass for a quad level d >= 2 of the adjoint: the two-pass form's edge
+// gradient (pass 1) is completed whole where it is needed instead of
+// accumulated by atomics, and the vertex terms (pass 2) follow in the same
+// thread.  For halfedge h with twin t:
 //   gEt[e(h)] = gE[e] + cE(h) gV[v(h)] + dE(next h) gV[v(next h)]      (own side)
 //                     + cE(t) gV[v(t)] + dE(next t) gV[v(next t)]      (twin t)
 // with v(t) = v(next h), v(next t) = v(h).  The twin side (at depth >= 2 the
-// twins of children 0, 1, 2, 3 of g are children 3, 2, 1, 0:
+// twins of children 0, 1, 2, 3 of parent halfedge g are children 3, 2, 1, 0:
 // CatmullClark.h:2778-2781):
-//   * inside the parent quad (children 1, 2): the twin lane's own side;
+//   * inside the parent quad (children 1, 2): the sibling face's own side;
 //   * across a parent edge, child 0 of g (twin t = child 3 of next(twin g)):
 //     cE(t) at the parent edge's midpoint, an interior vertex of valence 4
 //     whose only creased edges are the parent edge's two halves; dE(next t)
 //     at the older vertex v(h), non-zero only on a boundary in the crease
 //     branch (the only case that reads next t's edge);
 //   * child 3 of g (twin t = child 0 of twin(prev g)): cE(t) at the older
-//     vertex v(next h) (its statistics from the quad's child-0 lane, the
-//     boundary correction with t's edge, which is h's); dE(next t) = 0, at
-//     the interior midpoint of prev(g)'s edge.
+//     vertex v(next h) (its statistics, the boundary correction with t's
+//     edge, which is h's); dE(next t) = 0, at the interior midpoint of
+//     prev(g)'s edge.
 // The vertex coefficients are lane_vertex_coef's with the statistics it
-// would read taken from the lanes: child 2 sits at a face centre (valence 4),
-// children 1 and 3 at edge midpoints whose creased edges are the halves of
-// one parent edge, child 0 at an older vertex (its statistics).
-// Both halves of an edge evaluate the same terms; gE is read, not written.
+// would read known from the structure: child 2 sits at a face centre
+// (valence 4), children 1 and 3 at edge midpoints whose creased edges are the
+// halves of one parent edge, child 0 at an older vertex (its statistics).
+// gE is read, not written.
 // Where the adjoint step reads the gradients of depth d+1's points (index =
 // the point's slot in the level: [vertices | faces | edges]): an array, or,
 // for the finest level of a fitting loss, the difference P - T of the
@@ -1751,127 +1751,11 @@ struct GradDistance {
     }
 };
 
-template <int RW, class GradIn>
-__device__ __forceinline__ void adj_quad_step_tile_g(const QuadView<RW>& L, const GradIn gin,
-                                                     float* __restrict__ gOld, int64_t h0) {
-    const unsigned full = 0xffffffffu;
-    const int lane = threadIdx.x & 31, k = lane & 3, qb = lane & ~3, j = (lane >> 2) & 3;
-    const int ln = qb | ((k + 1) & 3), lp = qb | ((k + 3) & 3);
-    const int64_t h64 = h0 + threadIdx.x;
-    const bool valid = h64 < L.H;
-    const int32_t h = (int32_t)h64;
-    const int64_t fBase = L.V, eBase = (int64_t)L.V + L.F;
-    int32_t tw = -1, ed = 0, vx = 0;
-    float4 st = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    f3 gv = zero3(), ge = zero3(), gf = zero3();
-    float sOwn = 0.0f, sOther = 0.0f;
-    if (valid) {
-        lane_record(L, h64, tw, ed, vx);
-        gv = gin.at(vx);
-        ge = gin.at(eBase + ed);
-        sOwn = L.sharp(ed);
-        if (k == 0) {
-            gf = gin.at(fBase + (h >> 2));
-            st = L.ostats[vx];
-        }
-    }
-    const int32_t ped = __shfl_sync(full, ed, lp), ptw = __shfl_sync(full, tw, lp);
-    // the other half of the parent edge at this lane's vertex (k = 0, 1, 3)
-    if (valid && k != 2) sOther = L.sharp((k == 1 ? ped : ed) ^ 1);
-    const float sPrev = __shfl_sync(full, sOwn, lp);
-    VCoef kc{0.0f, 0.0f, 0.0f, 0.0f};
-    ECoef ke{0.0f, 0.0f, 0.0f};
-    if (valid) {
-        float vp = 4.0f, cpre = 0.0f, avgS = 0.0f;
-        bool bnd = false;
-        if (k == 0) {
-            bnd = st.w != 0.0f;
-            vp = st.x;
-            avgS = bnd ? st.y - sOwn : st.y;
-            cpre = bnd ? st.z - fsign(sOwn) : st.z;
-        } else if (k != 2) {
-            const float sa = k == 1 ? sPrev : sOwn;   // this side's half of the parent edge
-            const bool own = k == 3;                  // the walk from h skips its own edge
-            bnd = (k == 1 ? ptw : tw) < 0;
-            vp = bnd ? 2.0f : 4.0f;
-            avgS = (bnd && own) ? sOther : sa + sOther;
-            cpre = (bnd && own) ? fsign(sOther) : fsign(sa) + fsign(sOther);
-        }
-        kc = coef_from_stats(vp, cpre, avgS, bnd, fsign(sOwn), fsign(sPrev));
-        const float w = fsat(sOwn), b = tw < 0 ? 1.0f : 0.5f;    // edge_coef
-        ke.al = (1.0f - w) * 0.25f + w * b * 0.5f;
-        ke.be = w * b * 0.5f;
-        ke.ga = (1.0f - w) * 0.25f;
-    }
-    const float dEn = __shfl_sync(full, kc.dE, ln);
-    const f3 gn = shfl3(gv, ln);
-    const f3 own = add3(mul3(gv, kc.cE), mul3(gn, dEn));
-    // child 3's twin coefficient cE(t) at the quad's older vertex, evaluated in
-    // the child-0 lane (its statistics; child 3's sharpness is its sPrev)
-    float cB = 0.0f;
-    if (valid && k == 0) {
-        const bool bnd = st.w != 0.0f;
-        const float avgS = bnd ? st.y - sPrev : st.y;
-        const float cpre = bnd ? st.z - fsign(sPrev) : st.z;
-        cB = coef_from_stats(st.x, cpre, avgS, bnd, fsign(sPrev), 0.0f).cE;
-    }
-    cB = __shfl_sync(full, cB, qb);
-    const int sibK = k == 1 ? ((((j + 1) & 3) << 2) | 2) : ((((j + 3) & 3) << 2) | 1);
-    const f3 ownSib = shfl3(own, (lane & ~15) | sibK);
-    f3 twinSide = zero3();
-    if (valid && tw >= 0) {
-        if (k == 1 || k == 2) {
-            twinSide = ownSib;
-        } else if (k == 0) {
-            // cE(t) at the midpoint (interior, valence 4)
-            const VCoef ct = coef_from_stats(4.0f, fsign(sOwn) + fsign(sOther), sOwn + sOther, false, fsign(sOwn), 0.0f);
-            // dE(next t) at the older vertex v(h) = this lane's
-            float dEt = 0.0f;
-            const bool bnd = st.w != 0.0f;
-            const float valence = bnd ? st.x + 1.0f : st.x;
-            if (bnd && !(st.z >= 3.0f || valence == 2.0f) && !(st.z <= 1.0f) && sOwn != 0.0f) {
-                const int32_t en = L.edge(tw & ~3);      // next(t) = child 0 of t's quad
-                const float sn = L.sharp(en);
-                const float t = fsat((st.y - sn) * 0.5f);
-                dEt = t * 0.25f * fsign(sOwn);
-            }
-            twinSide = add3(mul3(gn, ct.cE), mul3(gv, dEt));
-        } else {
-            // cE(t) at the older vertex v(next h), seen from t (its edge is h's)
-            twinSide = mul3(gn, cB);
-        }
-    }
-    const f3 gEt = add3(add3(ge, own), twinSide);
-    // pass 2: face gradient over the quad, then this halfedge's vertex term
-    f3 ft = add3(mul3(gv, kc.bF), mul3(gEt, ke.ga));
-    ft = add3(ft, shfl_xor3(ft, 1));
-    ft = add3(ft, shfl_xor3(ft, 2));
-    const f3 gFt = add3(shfl3(gf, qb), ft);
-    const float bep = __shfl_sync(full, ke.be, lp);
-    const f3 gep = shfl3(gEt, lp);
-    const f3 s = add3(add3(mul3(gv, kc.a), mul3(gEt, ke.al)), add3(mul3(gFt, 0.25f), mul3(gep, bep)));
-    float* o = gOld + 3 * (int64_t)vx;
-    const f3 s4 = shfl_down3(s, 4), s8 = shfl_down3(s, 8), s12 = shfl_down3(s, 12);
-    const int partner = (lane & ~15) | ((((lane >> 2) + 1) & 3) << 2) | 3;
-    const f3 sA2 = shfl3(s, partner);
-    if (!valid) return;
-    if ((lane & 15) == 2) {
-        const f3 t = add3(add3(s, s4), add3(s8, s12));
-        o[0] += t.x;
-        o[1] += t.y;
-        o[2] += t.z;
-    } else if (k == 1) {
-        atomic_add3(o, add3(s, sA2));
-    } else if (k == 0) {
-        atomic_add3(o, s);
-    }
-}
-
-// The same pass with one thread per depth-d face: lane j of a quad of lanes
+// The pass runs one thread per depth-d face: lane j of a quad of lanes
 // takes face j of a parent quad (the structure k_level_fq relies on: face j
 // runs C_j, M_j, Z, M_{j-1}; inner edge j = (j, 1) | (j+1, 2); the halves of
-// parent edge j are (j, 0) and (j+1, 3)).  The terms of adj_quad_step_tile,
-// per halfedge k of the face: coefficients kc(k), ke(k) and own(k) =
+// parent edge j are (j, 0) and (j+1, 3)).  The terms above, per halfedge k
+// of the face: coefficients kc(k), ke(k) and own(k) =
 // cE(k) gV[v(k)] + dE(k+1) gV[v(k+1)]; the edge gradients
 //   gEt(0) = gE + own(0) + cE(t) gV[M_j] + dE(next t) gV[C_j]  (across parent edge j)
 //   gEt(1) = gE + own(1) + own(2) of the next lane              (inner edge j)
@@ -1881,8 +1765,8 @@ __device__ __forceinline__ void adj_quad_step_tile_g(const QuadView<RW>& L, cons
 // four vertex terms a gV + al gEt + gF/4 + be(prev) gEt(prev): the corner's
 // and midpoint M_j's pair (with the next lane's (j+1, 3) term) by float
 // atomics, the centre's four by lane 0 of the quad.  Every coefficient and
-// edge term is evaluated once per face instead of once per lane of a
-// 16-lane group, with 15 shuffles per face.
+// edge term is evaluated once per face (a layout with one halfedge per lane
+// evaluates most of them in several lanes), with 15 shuffles per face.
 __device__ __forceinline__ ECoef ecoef_of(float s, bool bnd) {
     const float w = fsat(s), b = bnd ? 1.0f : 0.5f;
     return ECoef{(1.0f - w) * 0.25f + w * b * 0.5f, w * b * 0.5f, (1.0f - w) * 0.25f};
@@ -1975,11 +1859,5 @@ __device__ __forceinline__ void adj_face_step_tile(const QuadView<RW>& L, const 
     }
 }
 
-// the gradients of depth d+1 from an array gNew (the same slots)
-template <int RW>
-__device__ __forceinline__ void adj_quad_step_tile(const QuadView<RW>& L, const float* __restrict__ gNew,
-                                                   float* __restrict__ gOld, int64_t h0) {
-    adj_quad_step_tile_g<RW, GradArray>(L, GradArray{gNew}, gOld, h0);
-}
 
 }  // namespace ccs
