@@ -325,6 +325,7 @@ __device__ __forceinline__ void fwd_level_ab(const BatchArgs& a, int d, int32_t*
             for_tiles(a, d, PH_AF, [&](const BatchCage& bc, int64_t lt) {
                 LevelArgs la = batch_level_args(a, bc, d);
                 la.ostats = a.stats + bc.stats[d];
+                la.d = d;
                 const int64_t f = lt * kBatchBlock + threadIdx.x;
                 const bool valid = f < bc.lv[d].F;
                 int4 r[4];

@@ -511,6 +511,7 @@ static void level_ab(const Ctx& c, int d, bool topo, bool uv, float* pts) {
     a.pin = pts + 3 * lv.ptOff;
     a.pout = pts + 3 * c.lv[d + 1].ptOff;
     a.H = lv.H; a.V = lv.V; a.F = lv.F; a.E = lv.E; a.C = lv.C;
+    a.d = d;
     a.ostats = stats_at(c, d);
     if (topo) fold_crease_stats(c, d, a);
     next_slots(c, d, pts, a);

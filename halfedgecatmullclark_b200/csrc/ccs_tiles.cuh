@@ -814,7 +814,29 @@ __device__ __forceinline__ void fq_points(const LevelArgs& a, int64_t f, bool va
         const float cpre = CREASED ? (bnd ? fsub(st.z, fsign(s0)) : st.z) : 0.0f;
         const f3 s = quad_vertex_rule<CREASED>(pC, F, Eo0, Eo3, st.x, cpre, avgS, bnd,
                                                CREASED ? fsign(s0) : 0.0f, CREASED ? fsign(s3) : 0.0f);
-        if (valid) atomic_add3(a.pout + 3 * (int64_t)C, s);
+        if (a.d >= 3) {
+            // From depth 3 the parent quads G = 4 F' + j' of a grandparent face F'
+            // fill a 16-lane group (lane = 16 (F' & 1) + 4 j' + j), and parent
+            // quad j''s corners are F''s corner j', its midpoints j' and j'-1
+            // and its centre.  So the centre's four shares (corner 2 of every
+            // parent quad) are all in the group: summed and stored, no atomic;
+            // midpoint j' is corner 1 of quad j' and corner 3 of quad j'+1:
+            // one atomic for the pair.  Half the corner atomics go (depth 5 of the
+            // headline workload: full step 0.412 -> 0.382 ms, points-only
+            // 0.218 -> 0.199 ms).
+            const int jq = (lane >> 2) & 3;
+            const f3 t1 = add3(s, shfl_xor3(s, 4));
+            const f3 t2 = add3(t1, shfl_xor3(t1, 8));
+            const f3 pr = shfl3(s, (lane & 16) | (((jq + 1) & 3) << 2) | 3);
+            if (valid) {
+                float* o = a.pout + 3 * (int64_t)C;
+                if (j == 0) atomic_add3(o, s);
+                else if (j == 1) atomic_add3(o, add3(s, pr));
+                else if (j == 2 && jq == 0) st3(o, t2);
+            }
+        } else if (valid) {
+            atomic_add3(a.pout + 3 * (int64_t)C, s);
+        }
     }
     f3 sM3;
     {   // (j, 3): midpoint M_{j-1}; the walk from it skips its own edge
@@ -1847,8 +1869,26 @@ __device__ __forceinline__ void adj_face_step_tile(const QuadView<RW>& L, const 
     const f3 t3 = add3(add3(mul3(gMp, k3.a), mul3(gEt3, q3.al)), add3(gF4, mul3(gEt2, q2.be)));
     const f3 t3n = shfl3(t3, ln);
     const f3 c1 = shfl3(t2, qb + 1), c2 = shfl3(t2, qb + 2), c3 = shfl3(t2, qb + 3);
+    // from depth 3, the corners shared inside a grandparent's 16-lane group
+    // (fq_points): the grandparent centre's four terms added by one lane (no
+    // other thread touches its slot), a grandparent midpoint's pair by one
+    // atomic (depth 5 of the headline workload: 0.176 -> 0.171 ms)
+    const bool agg = L.d >= 3;
+    const int jq = (lane >> 2) & 3;
+    const f3 u1 = add3(t0, shfl_xor3(t0, 4));
+    const f3 u2 = add3(u1, shfl_xor3(u1, 8));
+    const f3 pr = shfl3(t0, (lane & 16) | (((jq + 1) & 3) << 2) | 3);
     if (!valid) return;
-    atomic_add3(gOld + 3 * (int64_t)C, t0);
+    if (!agg || j == 0) {
+        atomic_add3(gOld + 3 * (int64_t)C, t0);
+    } else if (j == 1) {
+        atomic_add3(gOld + 3 * (int64_t)C, add3(t0, pr));
+    } else if (j == 2 && jq == 0) {
+        float* o = gOld + 3 * (int64_t)C;
+        o[0] += u2.x;
+        o[1] += u2.y;
+        o[2] += u2.z;
+    }
     atomic_add3(gOld + 3 * (int64_t)Mj, add3(t1, t3n));
     if (j == 0) {
         const f3 t = add3(add3(t2, c1), add3(c2, c3));
