@@ -546,10 +546,10 @@ bool encode_child_map(CUtensorMap* map, int32_t* levelRecords, int64_t parentHal
     if (!fn || parentHalfedges < 2 || (parentHalfedges & 1) || (reinterpret_cast<uintptr_t>(levelRecords) & 15))
         return false;
     // rows of 32 int32 (128 bytes: the four 16-byte children of two parent
-    // halfedges), one row per two parents; boxes of 128 rows (256 parents)
+    // halfedges), one row per two parents; boxes of kChildBoxRows rows
     const cuuint64_t dims[2] = {32, (cuuint64_t)(parentHalfedges / 2)};
     const cuuint64_t strides[1] = {128};
-    const cuuint32_t box[2] = {32, 128};
+    const cuuint32_t box[2] = {32, (cuuint32_t)kChildBoxRows};
     const cuuint32_t elem[2] = {1, 1};
     return fn(map, CU_TENSOR_MAP_DATA_TYPE_INT32, 2, levelRecords, dims, strides, box, elem,
               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE,

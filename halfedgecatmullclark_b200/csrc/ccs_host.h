@@ -135,9 +135,14 @@ struct Ctx {
     const uint8_t* childMapOk = nullptr;
 };
 
+// Rows per box of the child-record tensor maps: 32 rows of 128 bytes (the
+// children of 64 parent halfedges).  A block stores its tile as consecutive
+// boxes, 4 KB apart in shared memory.
+static constexpr int kChildBoxRows = 32;
+
 // Encodes the tensor map of the child records written by the step d -> d+1
-// (rows of 128 bytes over level d+1's 16-byte records, 128-row boxes,
-// 128-byte swizzle); false when the driver entry point is missing or the
+// (rows of 128 bytes over level d+1's 16-byte records, kChildBoxRows-row
+// boxes, 128-byte swizzle); false when the driver entry point is missing or the
 // encoding is refused.
 bool encode_child_map(CUtensorMap* map, int32_t* levelRecords, int64_t parentHalfedges);
 

@@ -6,9 +6,10 @@
 //     allow: the four vertex points, crease sharpness, the corner's ring
 //     statistics, across the two parent edges the twin quads' other
 //     vertices;
-//   - the face's 16 child records (+ UV codes) through a 32 KB swizzled
-//     shared tile and two TMA tensor stores per block, issued first and left
-//     to drain while the points are computed (no multicast);
+//   - the face's 16 child records (+ UV codes) through a swizzled shared
+//     tile (24 KB for a block of 96 faces) and TMA tensor stores of 32-row
+//     boxes, issued first and left to drain while the points are computed (no
+//     multicast);
 //   - its face point, the inner edge it shares with the next lane (that
 //     lane's face point by shuffle), its two outer edge points (the twin
 //     face rebuilt), all in the reference's operation order and stored once;
@@ -186,11 +187,6 @@ k_level_ab(LevelArgs a, const __grid_constant__ CUtensorMap childMap) {
 // zero on entry; every thread clears its share of `zeroNext`.
 static constexpr int kBlockF = 128;                      // faces per block
 
-// the full step (TOPO) by k_level_fq instead of k_level_ab
-#ifndef CCS_STEP_FQ
-#define CCS_STEP_FQ 1
-#endif
-
 // Resident blocks of 128 and the L2 prefetch of the records one wave ahead.
 // Depth 5 of the headline workload: 7 blocks (70 registers) against 6 and 8
 // the same for the full step and 0.221 against 0.232 ms (8, 64 registers)
@@ -204,26 +200,39 @@ static constexpr int kBlockF = 128;                      // faces per block
 #define CCS_FQ_PREFETCH_AHEAD 1036
 #endif
 
-template <int RW, bool TOPO, bool UV, bool CREASED>
-__global__ void __launch_bounds__(kBlockF, CCS_FQ_MIN_BLOCKS)
+// The full step's blocks (BF faces: a multiple of 32 for whole warps and of
+// 16 for whole grandparent groups): the 16 BF child records' tile in shared
+// memory bounds the resident blocks (128 faces: 32 KB, 6 blocks per SM).
+// Depth 5 of the headline workload, with the tile stored as 32-row boxes:
+// 64 faces 0.375 ms, 96 (24 KB, 9 blocks) 0.373, 128 0.375, 160 0.379 ms;
+// with 128-row boxes 128 faces took 0.382 ms.
+#ifndef CCS_FQT_FACES
+#define CCS_FQT_FACES 96
+#endif
+#ifndef CCS_FQT_MIN_BLOCKS
+#define CCS_FQT_MIN_BLOCKS 9
+#endif
+template <int RW, bool TOPO, bool UV, bool CREASED, int BF>
+__global__ void __launch_bounds__(BF, TOPO ? CCS_FQT_MIN_BLOCKS : CCS_FQ_MIN_BLOCKS)
 k_level_fq(LevelArgs a, const __grid_constant__ CUtensorMap childMap) {
     static_assert(!TOPO || RW == 4, "the child records go out through the 16-byte record tensor map");
+    static_assert(BF % 32 == 0, "whole warps: every lane of a warp takes part in the shuffles");
     chain_wait_then_release();
     const int64_t nF = (int64_t)a.H >> 2;                  // depth-d faces (H = 16 n at d >= 2)
-    const int nbF = (int)((nF + kBlockF - 1) / kBlockF);
+    const int nbF = (int)((nF + BF - 1) / BF);
     if (TOPO && (int)blockIdx.x >= nbF) {
-        const int64_t i = (int64_t)(blockIdx.x - nbF) * kBlockF + threadIdx.x;
+        const int64_t i = (int64_t)(blockIdx.x - nbF) * BF + threadIdx.x;
         if (i < a.C) {
             const float2 sh = crease_item(a.crIn, a.crOut, (int32_t)i);
             if (a.statsNext) crease_stats_next<RW>(a, (int32_t)i, sh);
         }
         return;
     }
-    const int64_t f = (int64_t)blockIdx.x * kBlockF + threadIdx.x;
+    const int64_t f = (int64_t)blockIdx.x * BF + threadIdx.x;
     if (threadIdx.x == 0 && CCS_FQ_PREFETCH_AHEAD > 0) {
-        const int64_t p0 = ((int64_t)blockIdx.x + CCS_FQ_PREFETCH_AHEAD) * kBlockF;
+        const int64_t p0 = ((int64_t)blockIdx.x + CCS_FQ_PREFETCH_AHEAD * kBlockF / BF) * BF;
         if (p0 < nF) {
-            const int64_t n = (nF - p0) < kBlockF ? (nF - p0) : kBlockF;
+            const int64_t n = (nF - p0) < BF ? (nF - p0) : BF;
             asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
                          :: "l"(a.in + (int64_t)RW * 4 * p0), "r"((uint32_t)(n * 16 * RW)) : "memory");
         }
@@ -238,7 +247,7 @@ k_level_fq(LevelArgs a, const __grid_constant__ CUtensorMap childMap) {
     if constexpr (TOPO) {
         // child m of halfedge h0 + k is child record 16 f + 4 k + m: row 2 f + k / 2
         // of the level's 128-byte rows, chunk 4 (k & 1) + m
-        __shared__ __align__(1024) int4 tile[kBlockF * 16];
+        __shared__ __align__(1024) int4 tile[BF * 16];
         float u[4], v[4];
         if (UV) {
 #pragma unroll
@@ -267,27 +276,25 @@ k_level_fq(LevelArgs a, const __grid_constant__ CUtensorMap childMap) {
             // quarter-warp write the children in the order 1 0 3 2: the eight
             // 16-byte stores of a quarter-warp then land on distinct banks
             // (depth 5 of the headline workload: 0.421 -> 0.417 ms)
-            const int row = 2 * threadIdx.x + (k >> 1), box = row >> 7, rr = row & 127;
+            const int row = 2 * threadIdx.x + (k >> 1);
             const int flip = (threadIdx.x >> 2) & 1;
 #pragma unroll
             for (int m = 0; m < 4; ++m) {
                 const int4 cm = flip ? c[m ^ 1] : c[m];
-                tile[box * 1024 + rr * 8 + ((4 * (k & 1) + (m ^ flip)) ^ (rr & 7))] = cm;
+                tile[row * 8 + ((4 * (k & 1) + (m ^ flip)) ^ (row & 7))] = cm;
             }
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
-        if (threadIdx.x == 0) {
-            const int32_t row0 = (int32_t)(2 * (int64_t)blockIdx.x * kBlockF), rows = (int32_t)(a.H >> 1);
-            tensor_store_tile_async(&childMap, tile, row0);
-            if (row0 + 128 < rows) tensor_store_tile_async(&childMap, tile + 1024, row0 + 128);
-        }
+        if (threadIdx.x == 0)
+            tensor_store_rows_async(&childMap, tile, (int32_t)(2 * (int64_t)blockIdx.x * BF), 2 * BF,
+                                    (int32_t)(a.H >> 1));
     }
 
     fq_points<RW, CREASED>(a, f, valid, r);
 
     // the slots the step after next accumulates into
-    const int64_t nT = (int64_t)nbF * kBlockF;
+    const int64_t nT = (int64_t)nbF * BF;
     for (int64_t i = f; i < a.zeroNextN; i += nT) a.zeroNext[i] = 0.0f;
     if (TOPO && threadIdx.x == 0) bulk_wait_read();
 }
@@ -522,18 +529,17 @@ static void level_ab(const Ctx& c, int d, bool topo, bool uv, float* pts) {
     memset(&none, 0, sizeof none);
     const CUtensorMap& map = tmap ? c.childMaps[d] : none;
     const unsigned nbf = (unsigned)((((int64_t)lv.H >> 2) + kBlockF - 1) / kBlockF);
-    if (RW == 4 && topo && tmap && CCS_STEP_FQ) {
-        const unsigned nbc = nbf + (unsigned)(((int64_t)lv.C + kBlockF - 1) / kBlockF);
-        if (uv) launch_chained(k_level_fq<4, true, true, CREASED>, nbc, kBlockF, c.stream, a, map);
-        else launch_chained(k_level_fq<4, true, false, CREASED>, nbc, kBlockF, c.stream, a, map);
-    } else if (topo && tmap) {
-        if (uv) launch_chained(k_level_ab<RW, true, true, CREASED, RW == 4>, nb, kBlockL, c.stream, a, map);
-        else launch_chained(k_level_ab<RW, true, false, CREASED, RW == 4>, nb, kBlockL, c.stream, a, map);
+    if (RW == 4 && topo && tmap) {
+        constexpr int BF = CCS_FQT_FACES;
+        const unsigned nbc = (unsigned)((((int64_t)lv.H >> 2) + BF - 1) / BF + ((int64_t)lv.C + BF - 1) / BF);
+        if (uv) launch_chained(k_level_fq<4, true, true, CREASED, BF>, nbc, BF, c.stream, a, map);
+        else launch_chained(k_level_fq<4, true, false, CREASED, BF>, nbc, BF, c.stream, a, map);
     } else if (topo) {
+        // 12-byte records, or a level whose tensor map could not be encoded
         if (RW == 4 && uv) launch_chained(k_level_ab<RW, true, true, CREASED, false>, nb, kBlockL, c.stream, a, map);
         else launch_chained(k_level_ab<RW, true, false, CREASED, false>, nb, kBlockL, c.stream, a, map);
     } else {
-        launch_chained(k_level_fq<RW, false, false, CREASED>, nbf, kBlockF, c.stream, a, map);
+        launch_chained(k_level_fq<RW, false, false, CREASED, kBlockF>, nbf, kBlockF, c.stream, a, map);
     }
     c.prof->end(c.stream);
 }

@@ -45,20 +45,11 @@ __device__ __forceinline__ void bulk_store_tile(void* gdst, const void* ssrc, ui
     asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
 }
 
-// One thread writes a 256-halfedge tile of child records (128 rows of 128
-// bytes, 128-byte swizzled in shared memory) to rows [row, row + 128) of the
-// tensor `tmap` describes (TMA tensor store, no multicast; rows past the
-// tensor's end are not written) and waits until the tile has been read.
-__device__ __forceinline__ void tensor_store_tile(const void* tmap, const void* ssrc, int32_t row) {
-    const uint32_t s = (uint32_t)__cvta_generic_to_shared(ssrc);
-    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];"
-                 :: "l"(tmap), "r"(0), "r"(row), "r"(s) : "memory");
-    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
-    asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
-}
-
-// The same two copies issued without the wait: the issuing thread must call
-// bulk_wait_read() before the block ends (or reuses the tile).
+// The same copy issued without the wait, and one box of a 128-byte swizzled
+// child tile (1024-byte aligned in shared memory) to row `row` of the tensor
+// `tmap` describes (TMA tensor store, no multicast; rows past the tensor's end
+// are not written): the issuing thread must call bulk_wait_read() before the
+// block ends (or reuses the tile).
 __device__ __forceinline__ void bulk_store_tile_async(void* gdst, const void* ssrc, uint32_t bytes) {
     const uint32_t s = (uint32_t)__cvta_generic_to_shared(ssrc);
     asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;"
@@ -72,6 +63,20 @@ __device__ __forceinline__ void tensor_store_tile_async(const void* tmap, const 
     asm volatile("cp.async.bulk.commit_group;" ::: "memory");
 }
 __device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+
+// `nrows` rows of a 128-byte swizzled child tile, stored as consecutive boxes
+// of kChildBoxRows rows (4 KB apart, each 1024-byte aligned) to rows [row0,
+// row0 + nrows) of a child-record map with `limit` rows: boxes that start
+// past the end are skipped, one that runs past it is clipped by the copy.
+// The issuing thread calls bulk_wait_read() before the tile is reused or the
+// block ends.
+__device__ __forceinline__ void tensor_store_rows_async(const void* tmap, const void* tile, int32_t row0, int nrows,
+                                                        int32_t limit) {
+    for (int b = 0; b < nrows; b += kChildBoxRows) {
+        if (row0 + b >= limit) break;
+        tensor_store_tile_async(tmap, static_cast<const char*>(tile) + 128 * b, row0 + b);
+    }
+}
 
 __device__ __forceinline__ f3 shfl3(f3 v, int src) {
     return f3{__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src),
@@ -587,8 +592,8 @@ __device__ __forceinline__ void tile_level_ab(const LevelArgs& a, int64_t h0, in
         __syncthreads();
         if (tid == 0) {
             if constexpr (TMAP) {
-                if (EARLY != 0) tensor_store_tile_async(tmap, tile, (int32_t)(h0 >> 1));
-                else tensor_store_tile(tmap, tile, (int32_t)(h0 >> 1));
+                tensor_store_rows_async(tmap, tile, (int32_t)(h0 >> 1), BLOCK / 2, (int32_t)(a.H >> 1));
+                if (EARLY == 0) bulk_wait_read();
             } else {
                 const int64_t n = (a.H - h0) < BLOCK ? (a.H - h0) : BLOCK;
                 if (EARLY != 0) bulk_store_tile_async(a.out + 4 * RW * h0, tile, (uint32_t)(n * 16 * RW));
