@@ -176,18 +176,20 @@ k_level_ab(LevelArgs a, const __grid_constant__ CUtensorMap childMap) {
 // evaluated with the same operations in the same order as tile_level_ab.
 // Stores: the face point, inner edge j, the outer edge points it owns and,
 // by lane 0, the centre (shares summed in face order); float atomics: the
-// corner's share and midpoint M_j's pair (j, 1) + (j+1, 3).  Against the
+// corner's share and midpoint M_j's pair (j, 1) + (j+1, 3), except where
+// they meet inside a grandparent's 16 lanes (fq_points).  Against the
 // lane-per-halfedge tile this evaluates every face and inner edge point once,
 // needs 24 shuffles per face instead of about 36 per halfedge and takes no
 // per-lane branches on the child position.
 // TOPO (16-byte records): the face's 16 child records (tile_level_ab's rules)
-// go through a 128-byte swizzled shared tile to two TMA tensor stores (128
-// rows of 128 bytes each) issued before the points are evaluated; the extra
+// go through a 128-byte swizzled shared tile to TMA tensor stores of
+// kChildBoxRows-row boxes issued before the points are evaluated; the extra
 // blocks refine the creases.  The vertex slots [0, V) of depth d+1 must be
 // zero on entry; every thread clears its share of `zeroNext`.
-static constexpr int kBlockF = 128;                      // faces per block
+static constexpr int kBlockF = 128;                      // faces per block of the points-only step
 
-// Resident blocks of 128 and the L2 prefetch of the records one wave ahead.
+// Resident blocks and the L2 prefetch of the records one wave ahead (blocks
+// of 128 faces; the full step's own block size below).
 // Depth 5 of the headline workload: 7 blocks (70 registers) against 6 and 8
 // the same for the full step and 0.221 against 0.232 ms (8, 64 registers)
 // for the points-only step; the prefetch 0.236 -> 0.221 ms for the

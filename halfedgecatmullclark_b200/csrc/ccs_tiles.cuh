@@ -537,9 +537,10 @@ __device__ __forceinline__ void tile_level_b(const QuadView<RW>& L, const float*
 // The vertex slots [0, V) of depth d+1 must be zero on entry; the tile also
 // clears its share of `zeroNext` (the slots the next level accumulates into).
 // Requires BLOCK a multiple of 32 and h0 a multiple of 16.
-// TMAP (16-byte records, BLOCK = 256): the child records go out through the
-// TMA tensor store of `tmap` (rows of 128 bytes = the children of two parent
-// halfedges) from a 128-byte swizzled tile (1024-byte aligned): 16-byte chunk
+// TMAP (16-byte records, BLOCK = 256): the child records go out through TMA
+// tensor stores of `tmap` (rows of 128 bytes = the children of two parent
+// halfedges, kChildBoxRows rows a box) from a 128-byte swizzled tile
+// (1024-byte aligned): 16-byte chunk
 // c of row r sits at chunk c ^ (r & 7), which also spreads every
 // quarter-warp's stores over the 32 banks.
 template <int BLOCK, int RW, bool TOPO, bool UV, bool CREASED, bool TMAP = false, int EARLY = 0>
