@@ -25,7 +25,8 @@
 // levels without a tensor map.
 // Depth 1 (children of n-gons, no 16-lane structure), cages without kept
 // statistics, and the deterministic pass run the step as kernel A
-// (k_level_a: records, face and edge points, clearing) then a vertex pass:
+// (k_level_a: records, face and edge points, clearing; for the exact pass at
+// depth >= 2 k_level_fq without its vertex shares) then a vertex pass:
 //   default (k_level_b): the vertex shares as above, read back from memory;
 //   deterministic (CCS_FLAG_DETERMINISTIC): every vertex summed by one thread
 //      in increasing halfedge order, the reference's one-thread order --
@@ -214,7 +215,9 @@ static constexpr int kBlockF = 128;                      // faces per block of t
 #ifndef CCS_FQT_MIN_BLOCKS
 #define CCS_FQT_MIN_BLOCKS 9
 #endif
-template <int RW, bool TOPO, bool UV, bool CREASED, int BF>
+// VERTS = false: kernel A of the exact pass (child records, face and edge
+// points; the vertex points are summed afterwards in the reference's order).
+template <int RW, bool TOPO, bool UV, bool CREASED, int BF, bool VERTS = true>
 __global__ void __launch_bounds__(BF, TOPO ? CCS_FQT_MIN_BLOCKS : CCS_FQ_MIN_BLOCKS)
 k_level_fq(LevelArgs a, const __grid_constant__ CUtensorMap childMap) {
     static_assert(!TOPO || RW == 4, "the child records go out through the 16-byte record tensor map");
@@ -293,11 +296,12 @@ k_level_fq(LevelArgs a, const __grid_constant__ CUtensorMap childMap) {
                                     (int32_t)(a.H >> 1));
     }
 
-    fq_points<RW, CREASED>(a, f, valid, r);
+    fq_points<RW, CREASED, VERTS>(a, f, valid, r);
 
     // the slots the step after next accumulates into
     const int64_t nT = (int64_t)nbF * BF;
-    for (int64_t i = f; i < a.zeroNextN; i += nT) a.zeroNext[i] = 0.0f;
+    if (VERTS)
+        for (int64_t i = f; i < a.zeroNextN; i += nT) a.zeroNext[i] = 0.0f;
     if (TOPO && threadIdx.x == 0) bulk_wait_read();
 }
 
@@ -563,7 +567,24 @@ static void level_a(const Ctx& c, int d, bool topo, bool uv, const float* pin, f
     if (clearNext) next_slots(c, d, clearNext, a);   // clearNext = the points of every depth
     const unsigned nb = nblocksL(lv.H) + (topo ? nblocksL(lv.C) : 0u);
     c.prof->begin(c.stream, topo ? CCS_K_LEVEL_FUSED : CCS_K_FACE_POINTS, d, lv.H);
-    if (topo) {
+    const bool tmap = RW == 4 && topo && c.childMaps && c.childMapOk && c.childMapOk[d];
+    if (RW == 4 && d >= 2 && !zeroV && !clearNext && c.fusable && (tmap || !topo)) {
+        // depth >= 2 of the exact pass: the per-face kernel without the
+        // vertex shares (the same records, face and edge points).  Depth 5 of
+        // the headline workload: 0.347 -> 0.317 ms with the records, 0.324 ->
+        // 0.134 ms for the points-only call's face and edge points
+        if (topo) {
+            constexpr int BF = CCS_FQT_FACES;
+            const unsigned nbc = (unsigned)((((int64_t)lv.H >> 2) + BF - 1) / BF + ((int64_t)lv.C + BF - 1) / BF);
+            if (uv) launch_chained(k_level_fq<4, true, true, CREASED, BF, false>, nbc, BF, c.stream, a, c.childMaps[d]);
+            else launch_chained(k_level_fq<4, true, false, CREASED, BF, false>, nbc, BF, c.stream, a, c.childMaps[d]);
+        } else {
+            CUtensorMap none;
+            memset(&none, 0, sizeof none);
+            const unsigned nbf = (unsigned)((((int64_t)lv.H >> 2) + kBlockF - 1) / kBlockF);
+            launch_chained(k_level_fq<4, false, false, CREASED, kBlockF, false>, nbf, kBlockF, c.stream, a, none);
+        }
+    } else if (topo) {
         if (RW == 4 && uv) k_level_a<RW, true, true, CREASED><<<nb, kBlockL, 0, c.stream>>>(a);
         else k_level_a<RW, true, false, CREASED><<<nb, kBlockL, 0, c.stream>>>(a);
     } else {

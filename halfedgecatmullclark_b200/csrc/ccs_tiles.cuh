@@ -726,7 +726,9 @@ __device__ __forceinline__ void tile_level_ab(const LevelArgs& a, int64_t h0, in
 // its four records, valid = f is a face of the level; every lane of the warp
 // calls it): face point, inner edge j, the two outer edge points it owns,
 // the four vertex shares (see k_level_fq in ccs_level.cu).
-template <int RW, bool CREASED>
+// VERTS = false: face and edge points only (kernel A of the exact pass; no
+// ring statistics read, no vertex slot touched).
+template <int RW, bool CREASED, bool VERTS = true>
 __device__ __forceinline__ void fq_points(const LevelArgs& a, int64_t f, bool valid, const int4 (&r)[4]) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31, qb = lane & ~3, j = lane & 3;
@@ -755,7 +757,7 @@ __device__ __forceinline__ void fq_points(const LevelArgs& a, int64_t f, bool va
         pM = ld3(a.pin + 3 * (int64_t)Mj);
         pZ = ld3(a.pin + 3 * (int64_t)Z);
         pMp = ld3(a.pin + 3 * (int64_t)Mp);
-        st = a.ostats[C];
+        if (VERTS) st = a.ostats[C];
         if (CREASED) {
             s0 = e0 < a.C ? __ldg(&a.crIn[e0].sharpness) : 0.0f;
             s1 = e1 < a.C ? __ldg(&a.crIn[e1].sharpness) : 0.0f;
@@ -813,6 +815,7 @@ __device__ __forceinline__ void fq_points(const LevelArgs& a, int64_t f, bool va
         }
         if (valid && h0 + 3 > tw3) st3(a.pout + 3 * (eOut + e3), Eo3);
     }
+    if constexpr (!VERTS) return;
     // vertex shares (tile_level_b's rules)
     {   // (j, 0): the corner; on a boundary the walk from it skips its own edge
         const bool bnd = st.w != 0.0f;
