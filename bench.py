@@ -783,6 +783,8 @@ def main():
     dom_ms = statistics.mean(by[dom_key])
     def kbytes(kernel, d):
         u = units.get((kernel, d)) if kernel in ("cage_side", "ring_stats") and d == 0 else None
+        if kernel in ("exact_points", "old_vertices"):
+            u = units.get(("old_vertices", d))
         return metrics.kernel_bytes(kernel, levels[d], rec_bytes, levels[d - 1] if d >= 1 else None, u)
     dom_bytes = kbytes(*dom_key)
     peak, peak_kind = measured_peak()

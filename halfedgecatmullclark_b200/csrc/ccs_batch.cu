@@ -64,7 +64,7 @@ enum Phase {
     PH_CREASE_STATS_NEXT,  // C_(d+1) creases of depth d + 1 (their statistics, before depth d + 1)
     PH_DIST,            // d = 0: the points whose fitting gradient P - T the distance adjoint
                         // writes before its steps (every level but a depth >= 3 cage's finest)
-    PH_AF,              // d >= 2: F_d faces (the points-only step, one thread per face)
+    PH_AF,              // d >= 2: F_d faces (the points-only step and the exact vertex pass)
     PH_ADJ_FSTEP,       // d >= 2: F_d faces (the adjoint step, one thread per face)
     PH_COUNT
 };
@@ -396,6 +396,12 @@ __device__ __forceinline__ void fwd_level_s2(const BatchArgs& a, int d) {
                 old_vertex_item<4, CREASED>(batch_quad_view(a, bc, d), a.pts + 3 * (bc.pt + bc.lv[d].ptOff),
                                             a.pts + 3 * (bc.pt + bc.lv[d + 1].ptOff), (int32_t)v);
         });
+        for_tiles(a, d, PH_AF, [&](const BatchCage& bc, int64_t lt) {
+            tile_face_exact<4, CREASED, false>(batch_quad_view(a, bc, d), a.pts + 3 * (bc.pt + bc.lv[d].ptOff),
+                                        a.pts + 3 * (bc.pt + bc.lv[d + 1].ptOff), lt * kBatchBlock);
+        });
+        fwd_shape_next<TOPO>(a, d);
+        return;
     }
     for_tiles(a, d, PH_B, [&](const BatchCage& bc, int64_t lt) {
         const float* pin = a.pts + 3 * (bc.pt + bc.lv[d].ptOff);
@@ -404,8 +410,6 @@ __device__ __forceinline__ void fwd_level_s2(const BatchArgs& a, int d) {
             const QuadView<4> L = batch_quad_view_stats(a, bc, d);
             if (d >= 2) tile_level_b<4, CREASED, true>(L, pin, pout, lt * kBatchBlock);
             else tile_level_b<4, CREASED, false>(L, pin, pout, lt * kBatchBlock);
-        } else if (d >= 2) {
-            tile_level_b_exact<4, CREASED>(batch_quad_view(a, bc, d), pin, pout, lt * kBatchBlock);
         } else {
             const QuadView<4> L = batch_quad_view(a, bc, d);
             const int64_t v = lt * kBatchBlock + tid;

@@ -31,9 +31,10 @@
 //   deterministic (CCS_FLAG_DETERMINISTIC): every vertex summed by one thread
 //      in increasing halfedge order, the reference's one-thread order --
 //      bit-identical points.  Depth >= 2: k_level_v (one thread per older
-//      vertex, one ring walk, on a second stream) beside k_level_b_exact
-//      (face centres in the warp, edge midpoints by the parent pair's owner
-//      with the twin side's shares rebuilt).  Depth 1: k_vertex_det.
+//      vertex, one ring walk, on a second stream) beside k_level_fq_exact
+//      (one thread per face: face centres summed in the quad of lanes, edge
+//      midpoints by the parent pair's owner with the twin side's shares
+//      rebuilt).  Depth 1: k_vertex_det.
 //
 // Face and edge points are evaluated in the reference's operation order in
 // every kernel; topology, creases, UVs, face and edge points are
@@ -313,16 +314,31 @@ k_level_b(QuadView<RW> L, const float* __restrict__ pin, float* __restrict__ pou
     tile_level_b<RW, CREASED, STRUCT>(L, pin, pout, (int64_t)blockIdx.x * kBlockL);
 }
 
-// exact vertex pass (d >= 2): face centres and edge midpoints
-template <int RW, bool CREASED>
-__global__ void __launch_bounds__(kBlockL, 5)
-k_level_b_exact(QuadView<RW> L, const float* __restrict__ pin, float* __restrict__ pout) {
-    prefetch_records_ahead<RW>(L.he, L.H, blockIdx.x, CCS_B_PREFETCH_AHEAD);
-    tile_level_b_exact<RW, CREASED>(L, pin, pout, (int64_t)blockIdx.x * kBlockL);
+// exact vertex pass (d >= 2): face centres and edge midpoints, one thread
+// per depth-d face, its records prefetched into L2 one wave ahead
+#ifndef CCS_FQ_EXACT_PREFETCH_AHEAD
+#define CCS_FQ_EXACT_PREFETCH_AHEAD 1036
+#endif
+#ifndef CCS_FQ_EXACT_MIN_BLOCKS
+#define CCS_FQ_EXACT_MIN_BLOCKS 7
+#endif
+template <int RW, bool CREASED, bool GRAND>
+__global__ void __launch_bounds__(kBlockF, CCS_FQ_EXACT_MIN_BLOCKS)
+k_level_fq_exact(QuadView<RW> L, const float* __restrict__ pin, float* __restrict__ pout) {
+    if (threadIdx.x == 0 && CCS_FQ_EXACT_PREFETCH_AHEAD > 0) {
+        const int64_t nF = (int64_t)L.H >> 2;
+        const int64_t p0 = ((int64_t)blockIdx.x + CCS_FQ_EXACT_PREFETCH_AHEAD) * kBlockF;
+        if (p0 < nF) {
+            const int64_t n = (nF - p0) < kBlockF ? (nF - p0) : kBlockF;
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
+                         :: "l"(L.he + 4 * RW * p0), "r"((uint32_t)(n * 16 * RW)) : "memory");
+        }
+    }
+    tile_face_exact<RW, CREASED, GRAND>(L, pin, pout, (int64_t)blockIdx.x * kBlockF);
 }
 
 // exact vertex pass (d >= 2): one thread per older vertex (its own launch,
-// so that k_level_b_exact keeps its small register footprint)
+// on a second stream beside k_level_fq_exact)
 template <int RW, bool CREASED>
 __global__ void __launch_bounds__(kBlockL)
 k_level_v(QuadView<RW> L, const float* __restrict__ pin, float* __restrict__ pout, int32_t Vold) {
@@ -609,13 +625,18 @@ static void level_b(const Ctx& c, int d, const float* pin, float* pout) {
 template <int RW, bool CREASED>
 static void level_b_exact(const Ctx& c, int d, const float* pin, float* pout) {
     const QuadView<RW> L = quad_view_l<RW>(c, d);
-    const int32_t Vold = c.lv[d - 1].V;
+    // from depth 3 the per-face pass also sums the corners that are centres
+    // and edge midpoints of depth d-2 faces (vertex ids V(d-2) .. V(d-1))
+    const bool grand = d >= 3 && c.fusable;
+    const int32_t Vold = grand ? c.lv[d - 2].V : c.lv[d - 1].V;
     Fork f(c);
     c.prof->begin(f.stream(), CCS_K_OLD_VERTICES, d, Vold);
     k_level_v<RW, CREASED><<<nblocksL(Vold), kBlockL, 0, f.stream()>>>(L, pin, pout, Vold);
     c.prof->end(f.stream());
     c.prof->begin(c.stream, CCS_K_EXACT_POINTS, d, L.H);
-    k_level_b_exact<RW, CREASED><<<nblocksL(L.H), kBlockL, 0, c.stream>>>(L, pin, pout);
+    const unsigned nb = (unsigned)((((int64_t)L.H >> 2) + kBlockF - 1) / kBlockF);
+    if (grand) k_level_fq_exact<RW, CREASED, true><<<nb, kBlockF, 0, c.stream>>>(L, pin, pout);
+    else k_level_fq_exact<RW, CREASED, false><<<nb, kBlockF, 0, c.stream>>>(L, pin, pout);
     c.prof->end(c.stream);
     f.join();
 }

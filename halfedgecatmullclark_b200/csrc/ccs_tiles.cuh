@@ -893,66 +893,83 @@ __device__ __forceinline__ void fq_points(const LevelArgs& a, int64_t f, bool va
 // face-centre and edge-midpoint vertex points of depth d+1 from the
 // halfedges [h0, h0 + blockDim) of depth d.
 // ---------------------------------------------------------------------------
-// At depth d >= 2 halfedge h = 16 f + 4 j + k is child k of parent halfedge
-// g = 4 f + j of the parent quad f, and a 16-lane group holds the 16 children
-// of f.  Vertex(h) is known from k:
-//   k = 2: the centre of f; its four shares are lanes 2, 6, 10, 14 of the
-//          group, in increasing halfedge order;
-//   k = 1, 3: the midpoint of a parent edge (valence 4, or 2 on a boundary;
-//          its only creased edges are the two halves e, e^1 of the parent
-//          edge).  Its shares are child 1 of g and child 3 of next(g), here,
-//          and child 1 of t = twin(g) and child 3 of next(t) in t's group.
-//          The lane of child 1 of the pair's owner (g > t, or t < 0) sums
-//          all of them: the twin side's two shares are rebuilt from face and
-//          edge points alone, since their ring statistics equal this side's;
-//   k = 0: an older vertex; old_vertex_item takes those.
+// Exact vertex pass at depth d >= 2, one thread per depth-d face f = 4 g + j
+// (face j of the parent quad g; lane j of a quad of lanes, the layout of
+// fq_points).  Face j has halfedges (j, k) = 4 f + k at the corner C_j
+// (k = 0), the midpoint M_j of parent edge j (k = 1), the centre Z of g
+// (k = 2) and M_{j-1} (k = 3).  The thread evaluates the shares of (j, 1),
+// (j, 2) and (j, 3) from kernel A's face and edge points:
+//   Z: its four shares are the (j, 2) of the quad's lanes, summed by lane 0
+//      in increasing halfedge order;
+//   M_j (valence 4, or 2 on a boundary; its only creased edges are the two
+//      halves e, e^1 of parent edge j): its shares are (j, 1) and (j+1, 3)
+//      here, and child 1 of t = twin(g) and child 3 of next(t) across the
+//      parent edge.  The thread of the pair's owner (g > t, or t < 0) sums
+//      all of them: the twin side's two shares are rebuilt from face and
+//      edge points alone, since their ring statistics equal this side's;
+//   C_j: an older vertex.  With GRAND (d >= 3, g = 4 G + J a child of the
+//      grandparent face G) the corners that are G's centre (j = 2) or the
+//      midpoint of G's edge J (j = 1 of quad J, j = 3 of quad J+1) are
+//      summed here too, by the statistics and arithmetic of
+//      old_vertex_item: the centre's four members (child 0 of the lanes
+//      j = 2) by the lane of quad 0, the midpoint's four by the j = 1 lane
+//      of the pair's owner (G's halfedge > its twin T, or no twin), the
+//      twin side's two (child 0 of faces 4 T + 1 and 4 next(T) + 3) rebuilt.
+//      Corners older than G go to old_vertex_item (vertex ids below V(d-2)).
 // Every vertex is summed by one thread in increasing halfedge order, starting
 // from zero, so the result is bit-identical to the reference's one-thread
 // scatter loop (:2496-2615) and needs neither atomics nor cleared slots.
 // Sharpness at depth >= 1 is +0 or positive, so the structural sums of
-// sharpness equal the walk's, zeros and order notwithstanding.
-// Requires H to be a multiple of 16 (true at depth >= 2) and blockDim a
-// multiple of 32 with h0 a multiple of 32.
-template <int RW, bool CREASED>
-__device__ __forceinline__ void tile_level_b_exact(const QuadView<RW>& L, const float* __restrict__ pin,
-                                                   float* __restrict__ pout, int64_t h0) {
-    const unsigned full = 0xffffffffu;
-    const int tid = threadIdx.x, lane = tid & 31;
-    const int64_t h64 = h0 + tid;
-    const bool valid = h64 < L.H;
-    const int32_t h = (int32_t)h64;
-    const int k = lane & 3, qb = lane & ~3, lp = qb | ((k + 3) & 3);
-    const int gb = lane & ~15, j = (lane >> 2) & 3;
+// sharpness equal the walk's, zeros and order notwithstanding (a sum is read
+// only where two terms are nonzero).
+// Requires f0 and blockDim to be multiples of 32 (the quad's lanes agree on
+// validity: the face count is a multiple of 4 at depth >= 2; with GRAND a
+// multiple of 16).
+template <int RW, bool CREASED, bool GRAND>
+__device__ __forceinline__ void tile_face_exact(const QuadView<RW>& L, const float* __restrict__ pin,
+                                                float* __restrict__ pout, int64_t f0) {
+    const int64_t nF = (int64_t)L.H >> 2;
+    const int64_t f = f0 + threadIdx.x;
+    const bool valid = f < nF;
+    const int lane = threadIdx.x & 31, qb = lane & ~3, j = lane & 3;
+    const int ln = qb | ((j + 1) & 3), lp = qb | ((j + 3) & 3);
     const float* fpt = pout + 3 * (int64_t)L.V;
     const float* ept = pout + 3 * ((int64_t)L.V + L.F);
-    int32_t tw = -1, ed = 0, vx = 0;
+    int4 r[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) r[k] = make_int4(-1, 0, 0, 0);
+    if (valid) load_face_records<RW>(L.he, f, r);
+    const int32_t tw0 = r[0].x, e0 = r[0].y, C = r[0].z;   // (j, 0): a half of parent edge j
+    const int32_t e1 = r[1].y, Mj = r[1].z;                // (j, 1): inner edge j
+    const int32_t e2 = r[2].y, Z = r[2].z;                 // (j, 2): inner edge j-1
+    const int32_t tw3 = r[3].x, e3 = r[3].y, Mp = r[3].z;  // (j, 3): a half of parent edge j-1
+    const int32_t g = (int32_t)(f >> 2);
+    const bool own = (e0 & 1) == 0;                        // g owns parent edge j (g > t, or t < 0)
+    const bool twinSide = own && tw0 >= 0;
+    // child 0 of g: twin = 4 next(t) + 3, so next(t) and t are depth-d faces
+    const int32_t tn = tw0 >> 2, t = qprev(tn);
+    const int32_t eB1 = e1 - (int32_t)f + t;               // edge of child 1 of t: 2 E(d-1) + t
+    // GRAND, lane j = 1: C = M_J of G's halfedge g.  (j, 3)'s twin is child 0
+    // of face 4 next(T) + 3; child 0 of face 4 T + 1 has the edge
+    // 2 (2 E(d-2) + T) + (T > next(T) ? 0 : 1), where 2 E(d-2) + g = e0 >> 1
+    const int32_t gT = qprev(tw3 >> 4);
+    const bool ownC = GRAND && j == 1 && (tw3 < 0 || g > gT);
+    const bool twinC = ownC && tw3 >= 0;
+    const int32_t eT1 = 2 * ((e0 >> 1) - g + gT) + ((gT & 3) == 3 ? 0 : 1);
+    f3 pM = zero3(), pZ = zero3(), pMp = zero3(), F = zero3(), E0 = zero3(), E1 = zero3(), E3 = zero3();
+    f3 FB1 = zero3(), FB2 = zero3(), EB1 = zero3();
+    float s0 = 0.0f, s0x = 0.0f, s1 = 0.0f, s2 = 0.0f, s3 = 0.0f, s3x = 0.0f;
     if (valid) {
-        if constexpr (RW == 4) {
-            const int4 r = __ldg(reinterpret_cast<const int4*>(L.he) + h);
-            tw = r.x; ed = r.y; vx = r.z;
-        } else {
-            tw = __ldg(L.he + 3 * h64 + 0);
-            ed = __ldg(L.he + 3 * h64 + 1);
-            vx = __ldg(L.he + 3 * h64 + 2);
-        }
-    }
-    // child 0 of g: twin = 4 next(t) + 3 (negative on a boundary), edge = 2 e + (g > t ? 0 : 1)
-    const int32_t tw0 = __shfl_sync(full, tw, qb);
-    const int32_t ed0 = __shfl_sync(full, ed, qb);
-    const int32_t ed0p = __shfl_sync(full, ed, gb | (((j + 3) & 3) << 2));   // child 0 of prev(g)
-    const bool ownG = (ed0 & 1) == 0, ownPrev = (ed0p & 1) == 0;
-    const bool need = k == 2 || (k == 3 ? ownPrev : ownG);
-    // the owner of an interior parent edge also reads the twin side's face
-    // and edge points (children 1 of t and 3 of next(t)), in the same round
-    const bool twinSide = k == 1 && ownG && tw0 >= 0;
-    const int32_t tn = tw0 >> 2, t = qprev(tn);        // next(t) and t = twin(g), depth d-1
-    const int32_t eB1 = ed - (h >> 2) + t;             // edge of child 1 of t: 2 E(d-1) + t
-    f3 p = zero3(), Fh = zero3(), Eh = zero3(), FB1 = zero3(), FB2 = zero3(), EB1 = zero3();
-    if (valid && need) {
-        Eh = ld3(ept + 3 * (int64_t)ed);              // k = 0: E of child 0, the twin side's or prev's edge point
-        if (k != 0) {
-            p = ld3(pin + 3 * (int64_t)vx);
-            Fh = ld3(fpt + 3 * (int64_t)(h >> 2));
+        pM = ld3(pin + 3 * (int64_t)Mj);
+        pZ = ld3(pin + 3 * (int64_t)Z);
+        pMp = ld3(pin + 3 * (int64_t)Mp);
+        F = ld3(fpt + 3 * f);
+        E0 = ld3(ept + 3 * (int64_t)e0);
+        E1 = ld3(ept + 3 * (int64_t)e1);
+        E3 = ld3(ept + 3 * (int64_t)e3);
+        if (CREASED) {
+            s0 = L.sharp(e0); s0x = L.sharp(e0 ^ 1); s1 = L.sharp(e1); s2 = L.sharp(e2);
+            s3 = L.sharp(e3); s3x = L.sharp(e3 ^ 1);
         }
         if (twinSide) {
             FB1 = ld3(fpt + 3 * (int64_t)t);
@@ -960,58 +977,108 @@ __device__ __forceinline__ void tile_level_b_exact(const QuadView<RW>& L, const 
             EB1 = ld3(ept + 3 * (int64_t)eB1);
         }
     }
-    const f3 Ep = shfl3(Eh, lp);                      // edge point of prev(h)'s edge
-    const int32_t ped = __shfl_sync(full, ed, lp);
-    const int32_t ptw = __shfl_sync(full, tw, lp);
-    f3 s = zero3();
-    float vpre = 4.0f, cpre = 0.0f, avgS = 0.0f;
-    bool bnd = false;
-    if (valid && need && k != 0) {
-        if (k != 2) {
-            const int32_t eh = k == 1 ? ped : ed;        // one half of the parent edge
-            const float sa = L.sharp(eh), sb = L.sharp(eh ^ 1);
-            bnd = (k == 1 ? ptw : tw) < 0;
-            vpre = bnd ? 2.0f : 4.0f;
-            const bool own = k == 3;                     // the walk from h skips its own edge
-            avgS = (bnd && own) ? sb : fadd(sa, sb);
-            cpre = (bnd && own) ? fsign(sb) : fadd(fsign(sa), fsign(sb));
-        }
-        s = quad_vertex_rule<CREASED>(p, Fh, Eh, Ep, vpre, cpre, avgS, bnd, fsign(L.sharp(ed)),
-                                      fsign(L.sharp(ped)));
-    }
-    // face centre: lanes 2, 6, 10, 14
-    const f3 s4 = shfl_down3(s, 4), s8 = shfl_down3(s, 8), s12 = shfl_down3(s, 12);
-    // edge midpoint: child 3 of next(g) sits in lanes 4 (j + 1 mod 4) + 3
-    const int partner = gb | (((j + 1) & 3) << 2) | 3;
-    f3 sA2 = shfl3(s, partner);
-    int32_t iA2 = __shfl_sync(full, h, partner);
-    if (!valid) return;
-    float* o = pout + 3 * (int64_t)vx;
-    if ((lane & 15) == 2) {
-        st3(o, add3(add3(add3(add3(zero3(), s), s4), s8), s12));
-    } else if (k == 1 && ownG) {
-        int32_t iA1 = h;
-        f3 sA1 = s;
+    const f3 E2 = shfl3(E1, lp);                           // inner edge j-1 is the previous lane's
+    // (j, 1) at M_j: the halves of its parent edge are e0 and e0 ^ 1
+    const bool bnd1 = tw0 < 0;
+    const float vpre1 = bnd1 ? 2.0f : 4.0f;
+    const float avgS1 = CREASED ? fadd(s0, s0x) : 0.0f;
+    const float cpre1 = CREASED ? fadd(fsign(s0), fsign(s0x)) : 0.0f;
+    const f3 sh1 = quad_vertex_rule<CREASED>(pM, F, E1, E0, vpre1, cpre1, avgS1, bnd1, fsign(s1), fsign(s0));
+    // (j, 2) at the centre
+    const f3 sh2 = quad_vertex_rule<CREASED>(pZ, F, E2, E1, 4.0f, 0.0f, 0.0f, false, fsign(s2), fsign(s1));
+    // (j, 3) at M_{j-1}: on a boundary the walk from it skips its own edge
+    const bool bnd3 = tw3 < 0;
+    const float avgS3 = CREASED ? (bnd3 ? s3x : fadd(s3, s3x)) : 0.0f;
+    const float cpre3 = CREASED ? (bnd3 ? fsign(s3x) : fadd(fsign(s3), fsign(s3x))) : 0.0f;
+    const f3 sh3 = quad_vertex_rule<CREASED>(pMp, F, E3, E2, bnd3 ? 2.0f : 4.0f, cpre3, avgS3, bnd3, fsign(s3),
+                                             fsign(s2));
+    const f3 c1 = shfl3(sh2, qb + 1), c2 = shfl3(sh2, qb + 2), c3 = shfl3(sh2, qb + 3);
+    f3 sA2 = shfl3(sh3, ln);                               // (j+1, 3), also at M_j
+    if (valid && j == 0) st3(pout + 3 * (int64_t)Z, add3(add3(add3(add3(zero3(), sh2), c1), c2), c3));
+    if (valid && own) {
+        int32_t iA1 = (int32_t)(4 * f + 1), iA2 = (int32_t)(4 * (f - j + ((j + 1) & 3)) + 3);
+        f3 sA1 = sh1;
         order2(iA1, sA1, iA2, sA2);
         f3 acc;
         if (!twinSide) {
             acc = add3(add3(zero3(), sA1), sA2);
         } else {
-            // child 3 of next(t) has edge 2 e = ed0, whose edge point is Ep
-            const f3 sB1 = quad_vertex_rule<CREASED>(p, FB1, EB1, zero3(), vpre, cpre, avgS, false,
-                                                     fsign(L.sharp(eB1)), 0.0f);
-            const f3 sB2 = quad_vertex_rule<CREASED>(p, FB2, Ep, zero3(), vpre, cpre, avgS, false,
-                                                     fsign(L.sharp(ed0)), 0.0f);
+            // child 1 of t, and child 3 of next(t), the twin of (j, 0) (edge e0, point E0)
+            f3 b1 = quad_vertex_rule<CREASED>(pM, FB1, EB1, zero3(), vpre1, cpre1, avgS1, false,
+                                              CREASED ? fsign(L.sharp(eB1)) : 0.0f, 0.0f);
+            f3 b2 = quad_vertex_rule<CREASED>(pM, FB2, E0, zero3(), vpre1, cpre1, avgS1, false, fsign(s0), 0.0f);
             int32_t iB1 = 4 * t + 1, iB2 = 4 * tn + 3;
-            f3 b1 = sB1, b2 = sB2;
             order2(iB1, b1, iB2, b2);
             // merge the two ordered pairs
-            order2(iA1, sA1, iB1, b1);                   // smallest in A1
-            order2(iA2, sA2, iB2, b2);                   // largest in B2
+            order2(iA1, sA1, iB1, b1);                    // smallest in A1
+            order2(iA2, sA2, iB2, b2);                    // largest in B2
             order2(iA2, sA2, iB1, b1);
             acc = add3(add3(add3(add3(zero3(), sA1), sA2), b1), b2);
         }
-        st3(o, acc);
+        st3(pout + 3 * (int64_t)Mj, acc);
+    }
+    if (GRAND) {
+        // a third round of gathers, after the midpoints' registers are free
+        f3 pC = zero3(), FT1 = zero3(), FT2 = zero3(), ET1 = zero3();
+        float sT1 = 0.0f;
+        if (valid && (j == 2 || ownC)) pC = ld3(pin + 3 * (int64_t)C);
+        if (valid && twinC) {
+            FT1 = ld3(fpt + 3 * (int64_t)(4 * gT + 1));
+            FT2 = ld3(fpt + 3 * (int64_t)(tw3 >> 2));
+            ET1 = ld3(ept + 3 * (int64_t)eT1);
+            if (CREASED) sT1 = L.sharp(eT1);
+        }
+        const int gl = lane & ~15, J = (lane >> 2) & 3;
+        // G's centre: members child 0 of the lanes j = 2, in quad order
+        const float z0 = __shfl_sync(0xffffffffu, s0, gl | 2), z1 = __shfl_sync(0xffffffffu, s0, gl | 6);
+        const float z2 = __shfl_sync(0xffffffffu, s0, gl | 10), z3 = __shfl_sync(0xffffffffu, s0, gl | 14);
+        const float totZ = CREASED ? fadd(fadd(fadd(fadd(0.0f, z0), z1), z2), z3) : 0.0f;
+        const float cntZ = CREASED ? fadd(fadd(fadd(fadd(0.0f, fsign(z0)), fsign(z1)), fsign(z2)), fsign(z3)) : 0.0f;
+        const f3 shZ = quad_vertex_rule<CREASED>(pC, F, E0, zero3(), 4.0f, cntZ, totZ, false, fsign(s0), 0.0f);
+        const f3 zs1 = shfl3(shZ, gl | 6), zs2 = shfl3(shZ, gl | 10), zs3 = shfl3(shZ, gl | 14);
+        // G's midpoint of edge J: the second local member is child 0 of the
+        // lane j = 3 of quad J+1 (face 4 next(g) + 3)
+        const int l2 = gl | (((J + 1) & 3) << 2) | 3;
+        const f3 F2 = shfl3(F, l2), E02 = shfl3(E0, l2);
+        const float s02 = __shfl_sync(0xffffffffu, s0, l2);
+        if (valid && j == 2 && J == 0)
+            st3(pout + 3 * (int64_t)C, add3(add3(add3(add3(zero3(), shZ), zs1), zs2), zs3));
+        if (ownC && valid) {
+            int32_t i1 = 4 * (int32_t)f, i2 = 4 * (4 * qnext(g) + 3);
+            f3 a1, a2, acc;
+            if (!twinC) {
+                // boundary: members child 0 of f and of face 4 next(g) + 3; the
+                // ring's edge without a member is (j, 3)'s, the prev edge of
+                // the second member is f's own (their twins share it)
+                const float cA = CREASED ? fadd(fsign(s3), fsign(s02)) : 0.0f;
+                const float aA = CREASED ? fadd(s3, s02) : 0.0f;
+                const float cB = CREASED ? fadd(fsign(s3), fsign(s0)) : 0.0f;
+                const float aB = CREASED ? fadd(s3, s0) : 0.0f;
+                a1 = quad_vertex_rule<CREASED>(pC, F, E0, CREASED ? E3 : zero3(), 2.0f, cA, aA, true, fsign(s0),
+                                               fsign(s3));
+                a2 = quad_vertex_rule<CREASED>(pC, F2, E02, CREASED ? E0 : zero3(), 2.0f, cB, aB, true,
+                                               fsign(s02), fsign(s0));
+                order2(i1, a1, i2, a2);
+                acc = add3(add3(zero3(), a1), a2);
+            } else {
+                // interior: the twin side's members child 0 of faces 4 T + 1
+                // (edge eT1) and 4 next(T) + 3 (the twin of (j, 3), edge e3)
+                const float tot = CREASED ? fadd(fadd(fadd(s0, s02), sT1), s3) : 0.0f;
+                const float cnt = CREASED ? fadd(fadd(fadd(fsign(s0), fsign(s02)), fsign(sT1)), fsign(s3)) : 0.0f;
+                a1 = quad_vertex_rule<CREASED>(pC, F, E0, zero3(), 4.0f, cnt, tot, false, fsign(s0), 0.0f);
+                a2 = quad_vertex_rule<CREASED>(pC, F2, E02, zero3(), 4.0f, cnt, tot, false, fsign(s02), 0.0f);
+                f3 b1 = quad_vertex_rule<CREASED>(pC, FT1, ET1, zero3(), 4.0f, cnt, tot, false, fsign(sT1), 0.0f);
+                f3 b2 = quad_vertex_rule<CREASED>(pC, FT2, E3, zero3(), 4.0f, cnt, tot, false, fsign(s3), 0.0f);
+                int32_t i3 = 4 * (4 * gT + 1), i4 = tw3;
+                order2(i1, a1, i2, a2);
+                order2(i3, b1, i4, b2);
+                order2(i1, a1, i3, b1);                    // smallest in a1
+                order2(i2, a2, i4, b2);                    // largest in b2
+                order2(i2, a2, i3, b1);
+                acc = add3(add3(add3(add3(zero3(), a1), a2), b1), b2);
+            }
+            st3(pout + 3 * (int64_t)C, acc);
+        }
     }
 }
 

@@ -38,7 +38,8 @@ def kernel_bytes(kernel: str, lv: dict, rec: int = 16, prev: dict | None = None,
     vertices at depth 1, where the quad-structure count below does not
     hold; `units` = the launch's own item count where it is not a level's:
     the statistics entries of every level for "cage_side" and the
-    every-level "ring_stats" launch)."""
+    every-level "ring_stats" launch; the older vertices of the ring walks for
+    "exact_points" and "old_vertices")."""
     H, V, F, E, C = lv["H"], lv["V"], lv["F"], lv["E"], lv["C"]
     if kernel == "cage_side":
         # cage records in, 4 child records out, cage creases in and their
@@ -91,14 +92,20 @@ def kernel_bytes(kernel: str, lv: dict, rec: int = 16, prev: dict | None = None,
         # crease half (k_crease_stats): the level's crease records in; the
         # atomics of its creased edges go to the statistics already written
         return int(12 * C)
+    # the exact pass: `units` = the older vertices the ring walks take (all
+    # V - nb, or from depth 3 only those of depth d-2, the per-face pass
+    # summing the centres and edge midpoints of depth d-2 as well)
+    older = max(V - nb, 0) if units is None else int(units)
     if kernel == "exact_points":
         # records + crease records + face and edge points in; the points of
         # its vertices in and out
-        return int(rec * H + 12 * C + 12 * F + 12 * E + 24 * nb)
+        return int(rec * H + 12 * C + 12 * F + 12 * E + 24 * (V - older))
     if kernel == "old_vertices":
         # records of children 0 and 3 (the ring walk), the ring's face and
-        # edge points (H / 4 members), the points in and out
-        return int(rec * H // 2 + 24 * (H // 4) + 24 * max(V - nb, 0))
+        # edge points (one member per halfedge of the walks' depth: H / 4,
+        # or H / 16 from depth d-2), the points in and out
+        members = H // 4 if older >= V - nb else H // 16
+        return int(2 * rec * members + 24 * members + 24 * older)
     if kernel == "adjoint":
         return int(rec * H + 12 * C + 12 * (V + F + E) + 12 * V)
     return 0
