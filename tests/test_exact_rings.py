@@ -1,6 +1,7 @@
-"""The index identities the exact vertex pass's per-face kernel relies on
-(`tile_face_exact` in csrc/ccs_tiles.cuh), checked on the oracle's refined
-levels of closed, open and non-quad cages.
+"""The index identities and the arithmetic of the exact vertex pass's
+per-face kernel (`tile_face_exact` in csrc/ccs_tiles.cuh) for the corners it
+sums without a ring walk, checked on the oracle's refined levels of closed,
+open and non-quad cages.
 
 At depth d >= 3 the kernel sums, besides the parent quads' centres and
 edge midpoints, the older vertices that are the centre and the edge
@@ -12,7 +13,10 @@ vertex, that the members the kernel derives are exactly the halfedges
 whose vertex it is, that the derived edge ids are the records' own, that
 each vertex is claimed by exactly one thread, and that the ring walks left
 to `old_vertex_item` (ids below V(d-2)) take exactly the other corners.
-The topology rules these follow are CatmullClark.h:2749-2796.
+The topology rules these follow are CatmullClark.h:2749-2796.  A float32
+restatement of the kernel's statistics, shares and summation order for
+those corners then reproduces the reference-order points bit for bit
+(the vertex rule of CatmullClark.h:2496-2615, with and without creases).
 """
 import numpy as np
 import pytest
@@ -104,3 +108,140 @@ def test_grandparent_corner_rings_follow_the_numbering(name, cage, depth):
                 assert tw[4 * f1[i]] >= 0 and tw[4 * f2[i]] < 0, (name, d, i)
                 assert ed[4 * f2[i] + 3] == ed[4 * f1[i]], (name, d, i)
             assert np.array_equal(ring(C[f1[i]]), np.sort(members)), (name, d, i)
+
+
+# ---------------------------------------------------------------------------
+# The kernel's arithmetic for those corners, restated in float32 numpy (every
+# operation an IEEE round-to-nearest float32 operation, no fused multiply-add,
+# as the kernels are built), against the reference-order points of the oracle.
+# ---------------------------------------------------------------------------
+f32 = np.float32
+
+
+def _fsign(x):
+    return np.where(x < 0, f32(-1), np.where(x > 0, f32(1), f32(0))).astype(f32)
+
+
+def _rule(p, F, E, Ep, vpre, cpre, avgS, bnd, cw, pcw, creased):
+    """quad_vertex_rule (CatmullClark.h:2496-2615): one halfedge's share."""
+    col = lambda x: np.asarray(x, f32)[:, None]
+    if not creased:
+        w = f32(1) / vpre
+        ws = w * np.where(bnd, f32(0), f32(1)).astype(f32)
+        return (col(w) * (p + col(ws) * ((f32(4) * E - F) - f32(3) * p))).astype(f32)
+    valence = np.where(bnd, vpre + f32(1), vpre).astype(f32)
+    count = np.where(bnd, cpre + cw, cpre).astype(f32)
+    corner = p * col(f32(1) / vpre)
+    smooth = (F * f32(-1) + E * f32(4)) + p * col(vpre - f32(3))
+    smooth = smooth * col(f32(1) / (vpre * vpre))
+    q = f32(0.25) * cw
+    crease = p * col(q) + E * col(q)
+    qp = f32(0.25) * pcw
+    crease = np.where(col(bnd), crease + (p * col(qp) + Ep * col(qp)), crease)
+    h = avgS * f32(0.5)
+    u = np.where(f32(0) > np.where(h < f32(1), h, f32(1)), f32(0), np.where(h < f32(1), h, f32(1))).astype(f32)
+    lerp = corner + col(u) * (crease - corner)
+    out = np.where(col((count >= 3) | (valence == 2)), corner, np.where(col(count <= 1), smooth, lerp))
+    return out.astype(f32)
+
+
+def _sum_sorted(ids, shares):
+    """Shares (k, n, 3) summed from zero in increasing id order (ids (k, n))."""
+    order = np.argsort(ids, axis=0, kind="stable")
+    acc = np.zeros(shares.shape[1:], f32)
+    for r in range(ids.shape[0]):
+        acc = (acc + np.take_along_axis(shares, order[r][None, :, None], 0)[0]).astype(f32)
+    return acc
+
+
+@pytest.mark.parametrize("mode", ["scatter", "nocreases_scatter"])
+@pytest.mark.parametrize("name,cage,depth", _cages(), ids=[c[0] for c in _cages()])
+def test_grandparent_corner_sums_match_the_reference_order(name, cage, depth, mode):
+    from oracle import oracle
+    creased = mode == "scatter"
+    cnt = oracle.counts(cage, depth)
+    he, cr, pts = oracle.refine(cage, depth, mode)
+    for d in range(3, depth):
+        tw, ed, vx = _level(he, cnt, d)
+        s0 = cnt["cumC"][d - 1]
+        sharp_d = cr["sharpness"][s0:s0 + cnt["C"][d]]
+
+        def sharp(e):
+            """Sharpness of level-d edges: 0 past the crease records, or without creases."""
+            e = np.asarray(e, np.int64)
+            if not creased:
+                return np.zeros(e.shape, f32)
+            ok = e < sharp_d.size
+            return np.where(ok, sharp_d[np.where(ok, e, 0)], f32(0)).astype(f32)
+
+        P = pts[oracle.level_slice(cage, depth, d, "V")]
+        Q = pts[oracle.level_slice(cage, depth, d + 1, "V")]
+        Vd, Fd = cnt["V"][d], cnt["F"][d]
+        Fp, Ep = Q[Vd:Vd + Fd], Q[Vd + Fd:]
+        nF = cnt["H"][d] // 4
+        f = np.arange(nF, dtype=np.int64)
+        j, g = f & 3, f >> 2
+        C = vx[4 * f]
+        # G's centres: the lanes j = 2 of quads 0..3, in quad order
+        cen = f[j == 2].reshape(-1, 4)
+        n = cen.shape[0]
+        sc = sharp(ed[4 * cen])                                   # (n, 4)
+        tot = np.zeros(n, f32)
+        cntz = np.zeros(n, f32)
+        for J in range(4):
+            tot = (tot + sc[:, J]).astype(f32)
+            cntz = (cntz + _fsign(sc[:, J])).astype(f32)
+        four = np.full(n, f32(4))
+        shares = np.stack([_rule(P[C[cen[:, J]]], Fp[cen[:, J]], Ep[ed[4 * cen[:, J]]], np.zeros((n, 3), f32),
+                                 four, cntz, tot, np.zeros(n, bool), _fsign(sc[:, J]), np.zeros(n, f32),
+                                 creased) for J in range(4)])
+        got = _sum_sorted(np.stack([4 * cen[:, J] for J in range(4)]), shares)
+        want = Q[C[cen[:, 0]]]
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), (name, mode, d, "centres")
+        # G's edge midpoints, summed by the owner of G's halfedge J (lane j = 1)
+        f1 = f[j == 1]
+        g1 = g[j == 1]
+        t3 = tw[4 * f1 + 3]
+        gT = _qprev(t3 >> 4)
+        own = (t3 < 0) | (g1 > gT)
+        f1, g1, t3, gT = f1[own], g1[own], t3[own], gT[own]
+        f2 = 4 * _qnext(g1) + 3
+        pC = P[C[f1]]
+        sa, sb, s3 = sharp(ed[4 * f1]), sharp(ed[4 * f2]), sharp(ed[4 * f1 + 3])
+        inner = t3 >= 0
+        # interior: four members, the ring's statistics shared by all
+        i = inner
+        m1 = 4 * (4 * gT[i] + 1)
+        eT1 = 2 * ((ed[4 * f1[i]] >> 1) - g1[i] + gT[i]) + np.where((gT[i] & 3) == 3, 0, 1)
+        sT = sharp(eT1)
+        tot = (((sa[i] + sb[i]).astype(f32) + sT).astype(f32) + s3[i]).astype(f32)
+        cn = (((_fsign(sa[i]) + _fsign(sb[i])).astype(f32) + _fsign(sT)).astype(f32) + _fsign(s3[i])).astype(f32)
+        k = int(i.sum())
+        z3, four, no = np.zeros((k, 3), f32), np.full(k, f32(4)), np.zeros(k, bool)
+        zk = np.zeros(k, f32)
+        sh = np.stack([
+            _rule(pC[i], Fp[f1[i]], Ep[ed[4 * f1[i]]], z3, four, cn, tot, no, _fsign(sa[i]), zk, creased),
+            _rule(pC[i], Fp[f2[i]], Ep[ed[4 * f2[i]]], z3, four, cn, tot, no, _fsign(sb[i]), zk, creased),
+            _rule(pC[i], Fp[4 * gT[i] + 1], Ep[eT1], z3, four, cn, tot, no, _fsign(sT), zk, creased),
+            _rule(pC[i], Fp[t3[i] >> 2], Ep[ed[4 * f1[i] + 3]], z3, four, cn, tot, no, _fsign(s3[i]), zk,
+                  creased)])
+        got = _sum_sorted(np.stack([4 * f1[i], 4 * f2[i], m1, t3[i]]), sh)
+        want = Q[C[f1[i]]]
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), (name, mode, d, "inner midpoints")
+        # boundary: two members; the ring's edge without a member is (j, 3)'s
+        b = ~inner
+        k = int(b.sum())
+        if k:
+            two, yes = np.full(k, f32(2)), np.ones(k, bool)
+            aA = (s3[b] + sb[b]).astype(f32)
+            cA = (_fsign(s3[b]) + _fsign(sb[b])).astype(f32)
+            aB = (s3[b] + sa[b]).astype(f32)
+            cB = (_fsign(s3[b]) + _fsign(sa[b])).astype(f32)
+            sh = np.stack([
+                _rule(pC[b], Fp[f1[b]], Ep[ed[4 * f1[b]]], Ep[ed[4 * f1[b] + 3]], two, cA, aA, yes,
+                      _fsign(sa[b]), _fsign(s3[b]), creased),
+                _rule(pC[b], Fp[f2[b]], Ep[ed[4 * f2[b]]], Ep[ed[4 * f1[b]]], two, cB, aB, yes,
+                      _fsign(sb[b]), _fsign(sa[b]), creased)])
+            got = _sum_sorted(np.stack([4 * f1[b], 4 * f2[b]]), sh)
+            want = Q[C[f1[b]]]
+            assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), (name, mode, d, "boundary midpoints")
