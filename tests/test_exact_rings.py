@@ -245,3 +245,79 @@ def test_grandparent_corner_sums_match_the_reference_order(name, cage, depth, mo
             got = _sum_sorted(np.stack([4 * f1[b], 4 * f2[b]]), sh)
             want = Q[C[f1[b]]]
             assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), (name, mode, d, "boundary midpoints")
+
+
+@pytest.mark.parametrize("mode", ["scatter", "nocreases_scatter"])
+@pytest.mark.parametrize("name,cage,depth", _cages(), ids=[c[0] for c in _cages()])
+def test_parent_centre_and_midpoint_sums_match_the_reference_order(name, cage, depth, mode):
+    """The rest of the kernel's sums, from depth 2: the parent quad's centre
+    from the quad's four (j, 2) shares, and the parent edge's midpoint at the
+    pair's owner from (j, 1), (j+1, 3) and the twin side's two shares rebuilt
+    from its face and edge points."""
+    from oracle import oracle
+    creased = mode == "scatter"
+    cnt = oracle.counts(cage, depth)
+    he, cr, pts = oracle.refine(cage, depth, mode)
+    for d in range(2, depth):
+        tw, ed, vx = _level(he, cnt, d)
+        s0 = cnt["cumC"][d - 1]
+        sharp_d = cr["sharpness"][s0:s0 + cnt["C"][d]]
+
+        def sharp(e):
+            e = np.asarray(e, np.int64)
+            if not creased:
+                return np.zeros(e.shape, f32)
+            ok = e < sharp_d.size
+            return np.where(ok, sharp_d[np.where(ok, e, 0)], f32(0)).astype(f32)
+
+        P = pts[oracle.level_slice(cage, depth, d, "V")]
+        Q = pts[oracle.level_slice(cage, depth, d + 1, "V")]
+        Vd, Fd = cnt["V"][d], cnt["F"][d]
+        Fp, Ep = Q[Vd:Vd + Fd], Q[Vd + Fd:]
+        nF = cnt["H"][d] // 4
+        f = np.arange(nF, dtype=np.int64)
+        nxt = f - (f & 3) + ((f + 1) & 3)                          # the next face of the quad
+        zn, no, four = np.zeros(nF, f32), np.zeros(nF, bool), np.full(nF, f32(4))
+        e0, e1, e2, e3 = ed[4 * f], ed[4 * f + 1], ed[4 * f + 2], ed[4 * f + 3]
+        # the shares of (j, 2) at the centre and (j, 3) at M_{j-1}, every face
+        sh2 = _rule(P[vx[4 * f + 2]], Fp[f], Ep[e2], Ep[e1], four, zn, zn, no, _fsign(sharp(e2)),
+                    _fsign(sharp(e1)), creased)
+        bnd3 = tw[4 * f + 3] < 0
+        s3, s3x = sharp(e3), sharp(e3 ^ 1)
+        avg3 = np.where(bnd3, s3x, (s3 + s3x).astype(f32)).astype(f32)
+        cp3 = np.where(bnd3, _fsign(s3x), (_fsign(s3) + _fsign(s3x)).astype(f32)).astype(f32)
+        sh3 = _rule(P[vx[4 * f + 3]], Fp[f], Ep[e3], Ep[e2], np.where(bnd3, f32(2), f32(4)).astype(f32), cp3,
+                    avg3, bnd3, _fsign(s3), _fsign(sharp(e2)), creased)
+        # centres: the quad's four (j, 2) in face order
+        q = f[(f & 3) == 0]
+        got = _sum_sorted(np.stack([4 * (q + k) + 2 for k in range(4)]), np.stack([sh2[q + k] for k in range(4)]))
+        assert np.array_equal(got.view(np.uint32), Q[vx[4 * q + 2]].view(np.uint32)), (name, mode, d, "centres")
+        # midpoints of the parent edges, at the owner of each pair
+        tw0 = tw[4 * f]
+        own = (e0 & 1) == 0
+        o = f[own]
+        bnd1 = tw0[own] < 0
+        sa, sx = sharp(e0[own]), sharp(e0[own] ^ 1)
+        vp1 = np.where(bnd1, f32(2), f32(4)).astype(f32)
+        av1 = (sa + sx).astype(f32)
+        cp1 = (_fsign(sa) + _fsign(sx)).astype(f32)
+        pM = P[vx[4 * o + 1]]
+        a1 = _rule(pM, Fp[o], Ep[e1[own]], Ep[e0[own]], vp1, cp1, av1, bnd1, _fsign(sharp(e1[own])), _fsign(sa),
+                   creased)
+        a2 = sh3[nxt[own]]
+        tn = tw0[own] >> 2
+        t = _qprev(tn)
+        eB1 = e1[own] - o + t
+        k = o.size
+        z3, zk, nk = np.zeros((k, 3), f32), np.zeros(k, f32), np.zeros(k, bool)
+        ts = np.where(bnd1, 0, t)
+        tns = np.where(bnd1, 0, tn)
+        eBs = np.where(bnd1, 0, eB1)
+        b1 = _rule(pM, Fp[ts], Ep[eBs], z3, vp1, cp1, av1, nk, _fsign(sharp(eBs)), zk, creased)
+        b2 = _rule(pM, Fp[tns], Ep[e0[own]], z3, vp1, cp1, av1, nk, _fsign(sa), zk, creased)
+        ids_a = np.stack([4 * o + 1, 4 * nxt[own] + 3])
+        pair = _sum_sorted(ids_a, np.stack([a1, a2]))
+        quad4 = _sum_sorted(np.concatenate([ids_a, np.stack([4 * t + 1, 4 * tn + 3])]),
+                            np.stack([a1, a2, b1, b2]))
+        got = np.where(bnd1[:, None], pair, quad4)
+        assert np.array_equal(got.view(np.uint32), Q[vx[4 * o + 1]].view(np.uint32)), (name, mode, d, "midpoints")
