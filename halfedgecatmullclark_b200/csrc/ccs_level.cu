@@ -30,11 +30,13 @@
 //   default (k_level_b): the vertex shares as above, read back from memory;
 //   deterministic (CCS_FLAG_DETERMINISTIC): every vertex summed by one thread
 //      in increasing halfedge order, the reference's one-thread order --
-//      bit-identical points.  Depth >= 2: k_level_v (one thread per older
-//      vertex, one ring walk, on a second stream) beside k_level_fq_exact
-//      (one thread per face: face centres summed in the quad of lanes, edge
-//      midpoints by the parent pair's owner with the twin side's shares
-//      rebuilt).  Depth 1: k_vertex_det.
+//      bit-identical points.  Depth >= 2: k_level_fq_exact (one thread per
+//      face: face centres summed in the quad of lanes, edge midpoints by the
+//      parent pair's owner with the twin side's shares rebuilt; from depth 3
+//      also the grandparent's centre and edge midpoints) beside k_level_v
+//      (one ring walk per remaining older vertex -- of depth d-1, or of
+//      depth d-2 from depth 3 -- on a second stream).  Depth 1:
+//      k_vertex_det.
 //
 // Face and edge points are evaluated in the reference's operation order in
 // every kernel; topology, creases, UVs, face and edge points are
@@ -337,8 +339,8 @@ k_level_fq_exact(QuadView<RW> L, const float* __restrict__ pin, float* __restric
     tile_face_exact<RW, CREASED, GRAND>(L, pin, pout, (int64_t)blockIdx.x * kBlockF);
 }
 
-// exact vertex pass (d >= 2): one thread per older vertex (its own launch,
-// on a second stream beside k_level_fq_exact)
+// exact vertex pass (d >= 2): one thread per older vertex v < Vold (its own
+// launch, on a second stream beside k_level_fq_exact, which sums the rest)
 template <int RW, bool CREASED>
 __global__ void __launch_bounds__(kBlockL)
 k_level_v(QuadView<RW> L, const float* __restrict__ pin, float* __restrict__ pout, int32_t Vold) {
